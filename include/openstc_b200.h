@@ -1,0 +1,170 @@
+/*
+ * C ABI of the B200-native OpenSTC step engine (libopenstc_b200.so).
+ *
+ * The reference has no FFI: its boundary is the C++ class template
+ * cfd::Driver<MixtureModel, TurbMethod> (src/Driver.cuh:12-46) driven by
+ * main (src/main.cu:7-68).  These entry points are what a binding of that
+ * boundary needs: open a case directory laid out like the reference's
+ * (input_files/...), initialise, step, read and write fields, write the
+ * Tecplot file.  Plain pointers and sizes only.  Every function returns 0 on
+ * success or a negative ostc_status; ostc_last_error() describes the failure.
+ *
+ * Array layout for every field: the reference's column-major layout with
+ * ghost layers (src/gxl_lib/Array.hpp:71-130),
+ *   idx(i,j,k) = k*(mx+2g)*(my+2g) + j*(mx+2g) + i + ((mx+2g)*(my+2g)+(mx+2g)+1)*g,
+ * components of a vector field stacked with the stride of one component.
+ * g is the field's ghost count (ostc_field_layout).  The metric is nine
+ * components (xi_x, xi_y, xi_z, eta_x, ..., zeta_z) and the inviscid
+ * spectral radius three, both in this stacked form.
+ */
+#ifndef OPENSTC_B200_H
+#define OPENSTC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ostc_driver ostc_driver;
+
+typedef enum ostc_status {
+  OSTC_OK = 0,
+  OSTC_ERR_INPUT = -1,     /* bad argument, missing or malformed case file */
+  OSTC_ERR_CUDA = -2,      /* CUDA runtime error */
+  OSTC_ERR_STATE = -3,     /* call out of order (e.g. step before initialize) */
+  OSTC_ERR_NAN = -4,       /* NaN residual: the reference aborts here (src/Driver.cu:372-377) */
+  OSTC_ERR_INTERNAL = -5
+} ostc_status;
+
+/* Field identifiers (the DZone members of src/Field.h:13-57). */
+typedef enum ostc_field_id {
+  OSTC_X = 0, OSTC_Y, OSTC_Z, OSTC_JAC, OSTC_METRIC, OSTC_WALL_DIST,
+  OSTC_BV, OSTC_SV, OSTC_CV, OSTC_VEL, OSTC_ACOUSTIC, OSTC_MACH, OSTC_MUL, OSTC_CONDUCTIVITY,
+  OSTC_RHO_D, OSTC_GAMMA, OSTC_CP, OSTC_MUT, OSTC_TURB_COND, OSTC_CHEM_JAC, OSTC_TURB_SRC_JAC,
+  OSTC_DQ, OSTC_DQ0, OSTC_DQK, OSTC_INV_SPEC, OSTC_VISC_SPEC, OSTC_DT_LOCAL, OSTC_BV_LAST,
+  OSTC_N_FIELDS
+} ostc_field_id;
+
+/* Step phases for per-kernel parity checks (see ostc_driver_run_phase). */
+typedef enum ostc_phase {
+  OSTC_PHASE_RESIDUAL = 0, /* dq = source + inviscid + viscous; local dt (src/Driver.cu:234-243) */
+  OSTC_PHASE_IMPLICIT = 1, /* point-implicit / DPLUR (src/ImplicitTreatmentHPP.cuh:10-59) */
+  OSTC_PHASE_UPDATE = 2,   /* update_cv_and_bv + limit_flow (src/Driver.cu:248-251) */
+  OSTC_PHASE_BC = 3,       /* boundary conditions (src/BoundCond.cuh:321-412) */
+  OSTC_PHASE_EXCHANGE = 4, /* inner faces, 2-D k copy, properties (src/Driver.cu:257-272) */
+  OSTC_PHASE_STORE = 5     /* store_last_step (src/TimeAdvanceFunc.cu:5-16) */
+} ostc_phase;
+
+typedef struct ostc_options {
+  int device; /* CUDA device ordinal */
+  int quiet;  /* suppress the reference's screen output */
+} ostc_options;
+
+typedef struct ostc_info {
+  int n_block, ngg, dimension;
+  int n_spec, n_reac, n_var, n_scalar;
+  int mix;       /* 0 air, 1 mixture, 2 finite-rate chemistry */
+  int rans;      /* 1 if k-omega SST */
+  int implicit_method, dplur_inner_step, chem_src_method;
+  int step;      /* current step number */
+  int64_t n_grid_total;
+  int n_bc, n_inner;
+} ostc_info;
+
+/* Model constants and mechanism tables as the engine sees them (the
+   reference's DParameter, src/DParameter.h:11-58).  Arrays are row-major:
+   [species][7] for NASA-7 coefficients, [reaction][species] for
+   stoichiometry and third-body efficiencies. */
+#define OSTC_MAX_SPEC 20
+#define OSTC_MAX_REAC 50
+typedef struct ostc_params {
+  int ns, nr, n_var, n_scalar;
+  int mix, turb, rans_model, turb_implicit, chem_src_method, implicit_method, dplur_inner_step;
+  int reconstruction, limiter, viscous_order, dim, output_screen;
+  double cfl, Pr, Prt, Sct, Sc;
+  double ll[7], ul[7];
+  double sv_inf[OSTC_MAX_SPEC + 2];
+  double mw[OSTC_MAX_SPEC], t_low[OSTC_MAX_SPEC], t_mid[OSTC_MAX_SPEC];
+  double low_coeff[OSTC_MAX_SPEC * 7], high_coeff[OSTC_MAX_SPEC * 7];
+  double lj_inv[OSTC_MAX_SPEC], vis_coeff[OSTC_MAX_SPEC];
+  double w_quarter[OSTC_MAX_SPEC * OSTC_MAX_SPEC], w_sqrt8[OSTC_MAX_SPEC * OSTC_MAX_SPEC];
+  int label[OSTC_MAX_REAC], order[OSTC_MAX_REAC];
+  int stoi_f[OSTC_MAX_REAC * OSTC_MAX_SPEC], stoi_b[OSTC_MAX_REAC * OSTC_MAX_SPEC];
+  double A[OSTC_MAX_REAC], b[OSTC_MAX_REAC], Ea[OSTC_MAX_REAC];
+  double A2[OSTC_MAX_REAC], b2[OSTC_MAX_REAC], Ea2[OSTC_MAX_REAC];
+  double third_body[OSTC_MAX_REAC * OSTC_MAX_SPEC];
+  double troe_alpha[OSTC_MAX_REAC], troe_t3[OSTC_MAX_REAC], troe_t1[OSTC_MAX_REAC], troe_t2[OSTC_MAX_REAC];
+} ostc_params;
+
+/* One boundary face in application order (outflow 6, inflow 5, symmetry 3,
+   wall 2), ranges after registration and wall trimming
+   (src/Mesh.cpp:18-35, src/BoundCond.cu:215-229). */
+typedef struct ostc_bc {
+  int block, type, face, direction;
+  int start[3], end[3];
+  double density, u, v, w, pressure, temperature, mut;
+  double sv[OSTC_MAX_SPEC + 2];
+  int isothermal;
+  double t_wall;
+} ostc_bc;
+
+/* One block-to-block face after registration (src/Mesh.cpp:47-177). */
+typedef struct ostc_inner {
+  int block, target_block, face, direction;
+  int start[3], end[3], loop_dir[3], tstart[3], tloop_dir[3], src_tar[3], n_point[3];
+} ostc_inner;
+
+/* Reads <case_dir>/input_files (setup, grid, boundary, chemistry), builds the
+   ghost geometry and metric and the initial field (fresh start or restart
+   from output/field/flowfield.plt).  Host only; replaces src/main.cu:7-28 and
+   the constructor Driver(Parameter&, Mesh&) (src/Driver.cu:14-40). */
+int ostc_driver_create(const char *case_dir, const ostc_options *opt, ostc_driver **out);
+void ostc_driver_destroy(ostc_driver *d);
+const char *ostc_last_error(void);
+
+int ostc_driver_info(const ostc_driver *d, ostc_info *info);
+int ostc_driver_params(const ostc_driver *d, ostc_params *params);
+int ostc_driver_bc(const ostc_driver *d, int index, ostc_bc *bc);
+int ostc_driver_inner(const ostc_driver *d, int index, ostc_inner *face);
+/* Block dimensions mx, my, mz. */
+int ostc_driver_block_dims(const ostc_driver *d, int block, int dims[3]);
+/* Ghost layers and component count of a field in this configuration
+   (components 0 = not allocated). */
+int ostc_field_layout(const ostc_driver *d, int field, int *ghost, int *components);
+
+/* Host copies made while reading the case, before initialisation:
+   OSTC_X/Y/Z, OSTC_JAC, OSTC_METRIC, OSTC_BV, OSTC_SV. */
+int ostc_driver_get_host_field(const ostc_driver *d, int block, int field, double *out, int64_t count);
+
+/* Driver::initialize_computation (src/Driver.cu:44-104) on the GPU. */
+int ostc_driver_initialize(ostc_driver *d);
+/* Driver::simulate (src/Driver.cu:107-120, 192-289): the steady loop with
+   history.dat, residual_scale.txt, step.txt and flowfield.plt output. */
+int ostc_driver_simulate(ostc_driver *d);
+/* n iterations of the steady loop body, no file output.  *err_max receives
+   the last normalised residual (or -1 if none was due). */
+int ostc_driver_step(ostc_driver *d, int n_steps, double *err_max);
+/* Normalised residuals of rho, |V|, p, T from the last residual step. */
+int ostc_driver_residual(const ostc_driver *d, double res[4]);
+int ostc_driver_run_phase(ostc_driver *d, int phase);
+/* Device field of a block (count = values of the field, see layout). */
+int ostc_driver_get_field(ostc_driver *d, int block, int field, double *out, int64_t count);
+int ostc_driver_set_field(ostc_driver *d, int block, int field, const double *in, int64_t count);
+/* MPIIO::print_field (src/MPIIO.hpp:420-546) to an explicit path. */
+int ostc_driver_write_plt(ostc_driver *d, const char *path);
+/* Kernel launches of one step of the cached CUDA graph. */
+int ostc_driver_launches_per_step(const ostc_driver *d, int store_last, int residual);
+/* Device time of the last step that computed a residual, in ms. */
+int ostc_driver_last_step_ms(const ostc_driver *d, double *ms);
+/* Runs one step eagerly with an event after every kernel and writes one line
+   "name launches total_ms" per kernel into buf.  Advances the solution
+   without counting a step.  Returns the number of lines. */
+int ostc_driver_profile_step(ostc_driver *d, char *buf, int buflen);
+/* The CUDA stream the engine launches on (cudaStream_t). */
+void *ostc_driver_stream(ostc_driver *d);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

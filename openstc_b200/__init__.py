@@ -1,0 +1,284 @@
+"""B200-native OpenSTC step engine: Python binding of the C ABI.
+
+The compute path is the in-tree library ``libopenstc_b200.so`` (C++ host
+code and sm_100a CUDA kernels, declared in include/openstc_b200.h).  This
+module only loads it and wraps its entry points; there is no Python or CPU
+fallback: if the library is missing, importing the binding raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libopenstc_b200.so"
+
+MAX_SPEC = 20
+MAX_REAC = 50
+
+# ostc_field_id
+FIELDS = [
+    "x", "y", "z", "jac", "metric", "wall_dist", "bv", "sv", "cv", "vel", "acoustic", "mach", "mul",
+    "conductivity", "rho_d", "gamma", "cp", "mut", "turb_cond", "chem_jac", "turb_src_jac", "dq", "dq0", "dqk",
+    "inv_spec", "visc_spec", "dt_local", "bv_last",
+]
+FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
+PHASES = {"residual": 0, "implicit": 1, "update": 2, "bc": 3, "exchange": 4, "store": 5}
+
+
+class OstcError(RuntimeError):
+    pass
+
+
+class Options(C.Structure):
+    _fields_ = [("device", C.c_int), ("quiet", C.c_int)]
+
+
+class Info(C.Structure):
+    _fields_ = [
+        ("n_block", C.c_int), ("ngg", C.c_int), ("dimension", C.c_int), ("n_spec", C.c_int), ("n_reac", C.c_int),
+        ("n_var", C.c_int), ("n_scalar", C.c_int), ("mix", C.c_int), ("rans", C.c_int),
+        ("implicit_method", C.c_int), ("dplur_inner_step", C.c_int), ("chem_src_method", C.c_int),
+        ("step", C.c_int), ("n_grid_total", C.c_int64), ("n_bc", C.c_int), ("n_inner", C.c_int),
+    ]
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("ns", C.c_int), ("nr", C.c_int), ("n_var", C.c_int), ("n_scalar", C.c_int),
+        ("mix", C.c_int), ("turb", C.c_int), ("rans_model", C.c_int), ("turb_implicit", C.c_int),
+        ("chem_src_method", C.c_int), ("implicit_method", C.c_int), ("dplur_inner_step", C.c_int),
+        ("reconstruction", C.c_int), ("limiter", C.c_int), ("viscous_order", C.c_int), ("dim", C.c_int),
+        ("output_screen", C.c_int),
+        ("cfl", C.c_double), ("Pr", C.c_double), ("Prt", C.c_double), ("Sct", C.c_double), ("Sc", C.c_double),
+        ("ll", C.c_double * 7), ("ul", C.c_double * 7), ("sv_inf", C.c_double * (MAX_SPEC + 2)),
+        ("mw", C.c_double * MAX_SPEC), ("t_low", C.c_double * MAX_SPEC), ("t_mid", C.c_double * MAX_SPEC),
+        ("low_coeff", C.c_double * (MAX_SPEC * 7)), ("high_coeff", C.c_double * (MAX_SPEC * 7)),
+        ("lj_inv", C.c_double * MAX_SPEC), ("vis_coeff", C.c_double * MAX_SPEC),
+        ("w_quarter", C.c_double * (MAX_SPEC * MAX_SPEC)), ("w_sqrt8", C.c_double * (MAX_SPEC * MAX_SPEC)),
+        ("label", C.c_int * MAX_REAC), ("order", C.c_int * MAX_REAC),
+        ("stoi_f", C.c_int * (MAX_REAC * MAX_SPEC)), ("stoi_b", C.c_int * (MAX_REAC * MAX_SPEC)),
+        ("A", C.c_double * MAX_REAC), ("b", C.c_double * MAX_REAC), ("Ea", C.c_double * MAX_REAC),
+        ("A2", C.c_double * MAX_REAC), ("b2", C.c_double * MAX_REAC), ("Ea2", C.c_double * MAX_REAC),
+        ("third_body", C.c_double * (MAX_REAC * MAX_SPEC)),
+        ("troe_alpha", C.c_double * MAX_REAC), ("troe_t3", C.c_double * MAX_REAC),
+        ("troe_t1", C.c_double * MAX_REAC), ("troe_t2", C.c_double * MAX_REAC),
+    ]
+
+
+class Bc(C.Structure):
+    _fields_ = [
+        ("block", C.c_int), ("type", C.c_int), ("face", C.c_int), ("direction", C.c_int),
+        ("start", C.c_int * 3), ("end", C.c_int * 3),
+        ("density", C.c_double), ("u", C.c_double), ("v", C.c_double), ("w", C.c_double),
+        ("pressure", C.c_double), ("temperature", C.c_double), ("mut", C.c_double),
+        ("sv", C.c_double * (MAX_SPEC + 2)), ("isothermal", C.c_int), ("t_wall", C.c_double),
+    ]
+
+
+class Inner(C.Structure):
+    _fields_ = [
+        ("block", C.c_int), ("target_block", C.c_int), ("face", C.c_int), ("direction", C.c_int),
+        ("start", C.c_int * 3), ("end", C.c_int * 3), ("loop_dir", C.c_int * 3), ("tstart", C.c_int * 3),
+        ("tloop_dir", C.c_int * 3), ("src_tar", C.c_int * 3), ("n_point", C.c_int * 3),
+    ]
+
+
+_lib = None
+
+
+def library() -> C.CDLL:
+    """Load libopenstc_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise OstcError(f"{LIB_PATH} is missing: build it with `python -m openstc_b200.build`")
+    lib = C.CDLL(str(LIB_PATH))
+    P, I64, D = C.c_void_p, C.c_int64, C.POINTER(C.c_double)
+    sig = {
+        "ostc_driver_create": ([C.c_char_p, C.POINTER(Options), C.POINTER(P)], C.c_int),
+        "ostc_driver_destroy": ([P], None),
+        "ostc_last_error": ([], C.c_char_p),
+        "ostc_driver_info": ([P, C.POINTER(Info)], C.c_int),
+        "ostc_driver_params": ([P, C.POINTER(Params)], C.c_int),
+        "ostc_driver_bc": ([P, C.c_int, C.POINTER(Bc)], C.c_int),
+        "ostc_driver_inner": ([P, C.c_int, C.POINTER(Inner)], C.c_int),
+        "ostc_driver_block_dims": ([P, C.c_int, C.POINTER(C.c_int)], C.c_int),
+        "ostc_field_layout": ([P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+        "ostc_driver_get_host_field": ([P, C.c_int, C.c_int, D, I64], C.c_int),
+        "ostc_driver_initialize": ([P], C.c_int),
+        "ostc_driver_simulate": ([P], C.c_int),
+        "ostc_driver_step": ([P, C.c_int, D], C.c_int),
+        "ostc_driver_residual": ([P, D], C.c_int),
+        "ostc_driver_run_phase": ([P, C.c_int], C.c_int),
+        "ostc_driver_get_field": ([P, C.c_int, C.c_int, D, I64], C.c_int),
+        "ostc_driver_set_field": ([P, C.c_int, C.c_int, D, I64], C.c_int),
+        "ostc_driver_write_plt": ([P, C.c_char_p], C.c_int),
+        "ostc_driver_launches_per_step": ([P, C.c_int, C.c_int], C.c_int),
+        "ostc_driver_last_step_ms": ([P, D], C.c_int),
+        "ostc_driver_stream": ([P], C.c_void_p),
+        "ostc_driver_profile_step": ([P, C.c_char_p, C.c_int], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        msg = library().ostc_last_error().decode(errors="replace")
+        raise OstcError(f"openstc_b200 call failed ({rc}): {msg}")
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Driver:
+    """Python face of the reference's Driver<mix, turb> (src/Driver.cuh:12-46).
+
+    ``Driver(case_dir)`` reads the case (host only); ``initialize()`` runs
+    Driver::initialize_computation on the GPU; ``simulate()`` the steady loop;
+    ``step(n)`` n loop iterations without file output.
+    """
+
+    def __init__(self, case_dir: str | Path, device: int = 0, quiet: bool = True):
+        lib = library()
+        self._h = C.c_void_p()
+        opt = Options(device, 1 if quiet else 0)
+        _check(lib.ostc_driver_create(str(case_dir).encode(), C.byref(opt), C.byref(self._h)))
+        self.case_dir = Path(case_dir)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            library().ostc_driver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---------------------------------------------------------- description
+    def info(self) -> Info:
+        inf = Info()
+        _check(library().ostc_driver_info(self._h, C.byref(inf)))
+        return inf
+
+    def params(self) -> Params:
+        p = Params()
+        _check(library().ostc_driver_params(self._h, C.byref(p)))
+        return p
+
+    def bcs(self) -> list[Bc]:
+        out = []
+        for q in range(self.info().n_bc):
+            b = Bc()
+            _check(library().ostc_driver_bc(self._h, q, C.byref(b)))
+            out.append(b)
+        return out
+
+    def inner_faces(self) -> list[Inner]:
+        out = []
+        for q in range(self.info().n_inner):
+            f = Inner()
+            _check(library().ostc_driver_inner(self._h, q, C.byref(f)))
+            out.append(f)
+        return out
+
+    def dims(self, block: int) -> tuple[int, int, int]:
+        d = (C.c_int * 3)()
+        _check(library().ostc_driver_block_dims(self._h, block, d))
+        return d[0], d[1], d[2]
+
+    def layout(self, field: str) -> tuple[int, int]:
+        g, n = C.c_int(), C.c_int()
+        _check(library().ostc_field_layout(self._h, FIELD_ID[field], C.byref(g), C.byref(n)))
+        return g.value, n.value
+
+    def field_shape(self, block: int, field: str) -> tuple[int, int, int, int]:
+        """(components, nz, ny, nx) of the ghosted array in C order."""
+        g, n = self.layout(field)
+        mx, my, mz = self.dims(block)
+        return n, mz + 2 * g, my + 2 * g, mx + 2 * g
+
+    def host_field(self, block: int, field: str) -> np.ndarray:
+        shape = self.field_shape(block, field)
+        out = np.empty(shape, dtype=np.float64)
+        _check(library().ostc_driver_get_host_field(self._h, block, FIELD_ID[field], _dptr(out), out.size))
+        return out
+
+    # ---------------------------------------------------------- device
+    def initialize(self) -> None:
+        _check(library().ostc_driver_initialize(self._h))
+
+    def simulate(self) -> None:
+        _check(library().ostc_driver_simulate(self._h))
+
+    def step(self, n: int = 1) -> float:
+        err = C.c_double(-1.0)
+        _check(library().ostc_driver_step(self._h, n, C.byref(err)))
+        return err.value
+
+    def residual(self) -> np.ndarray:
+        r = np.zeros(4)
+        _check(library().ostc_driver_residual(self._h, _dptr(r)))
+        return r
+
+    def run_phase(self, phase: str) -> None:
+        _check(library().ostc_driver_run_phase(self._h, PHASES[phase]))
+
+    def get(self, block: int, field: str) -> np.ndarray:
+        shape = self.field_shape(block, field)
+        out = np.empty(shape, dtype=np.float64)
+        _check(library().ostc_driver_get_field(self._h, block, FIELD_ID[field], _dptr(out), out.size))
+        return out
+
+    def get_into(self, block: int, field: str, out: np.ndarray) -> None:
+        _check(library().ostc_driver_get_field(self._h, block, FIELD_ID[field], _dptr(out), out.size))
+
+    def set(self, block: int, field: str, values: np.ndarray) -> None:
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        _check(library().ostc_driver_set_field(self._h, block, FIELD_ID[field], _dptr(a), a.size))
+
+    def write_plt(self, path: str | Path) -> None:
+        _check(library().ostc_driver_write_plt(self._h, str(path).encode()))
+
+    def launches_per_step(self, store_last: bool = False, residual: bool = False) -> int:
+        n = library().ostc_driver_launches_per_step(self._h, int(store_last), int(residual))
+        if n < 0:
+            _check(n)
+        return n
+
+    def last_step_ms(self) -> float:
+        v = C.c_double()
+        _check(library().ostc_driver_last_step_ms(self._h, C.byref(v)))
+        return v.value
+
+    def profile_step(self) -> list[tuple[str, int, float]]:
+        """One eager step with per-kernel CUDA events: [(kernel, launches, ms)]."""
+        buf = C.create_string_buffer(1 << 16)
+        n = library().ostc_driver_profile_step(self._h, buf, len(buf))
+        if n < 0:
+            _check(n)
+        rows = []
+        for line in buf.value.decode().splitlines():
+            name, cnt, ms = line.split()
+            rows.append((name, int(cnt), float(ms)))
+        return rows
+
+    def stream(self) -> int:
+        return library().ostc_driver_stream(self._h) or 0

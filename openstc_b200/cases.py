@@ -1,0 +1,359 @@
+"""Case directories in the reference's input format.
+
+A case directory holds ``input_files/setup/*.txt`` (the nine setup files of
+src/Parameter.h:64-74), ``input_files/grid/grid   0.grd`` (src/Mesh.cpp:598-685),
+``input_files/boundary_condition/{boundary,inner}   0.txt`` and
+``input_files/chemistry/*``.  Both this library and the reference build read
+these files unchanged.
+
+Workloads:
+* ``ramp_case``           - 2-D laminar air, Mach 3 over a 15 degree ramp
+                            (256 x 128 x 1 by default, explicit, CFL 0.5).
+* ``mixing_layer_case``   - 3-D reacting H2 / vitiated-air mixing layer,
+                            9 species, k-omega SST, DPLUR 4 sweeps, EPI
+                            (384 x 192 x 64 by default); starts from a tanh
+                            blend of the two streams written as a restart file.
+* ``multiblock_case``     - the mixing-layer physics on several blocks tiled
+                            along x with 1:1 inner faces.
+"""
+from __future__ import annotations
+
+import math
+import shutil
+from pathlib import Path
+
+import numpy as np
+
+_DATA = Path(__file__).resolve().parent / "data" / "chemistry"
+
+
+def _fmt(v) -> str:
+    if isinstance(v, bool):
+        return "1" if v else "0"
+    return repr(v) if isinstance(v, float) else str(v)
+
+
+def write_setup(case: Path, files: dict[str, list[str]]) -> None:
+    d = Path(case) / "input_files" / "setup"
+    d.mkdir(parents=True, exist_ok=True)
+    for name, lines in files.items():
+        (d / name).write_text("\n".join(lines) + "\n")
+
+
+def setup_files(*, dimension: int, total_step: int, output_file: int, output_screen: int, cfl: float,
+                implicit_method: int, dplur_inner_step: int, species: bool, reaction: bool, turbulence: bool,
+                chem_src_method: int = 1, initial: int = 0, convergence: float = 1e-30, reconstruction: int = 2,
+                grid_scale: float = 1.0, inflows: list[dict] | None = None, walls: list[dict] | None = None,
+                default_init: str = "freestream", schmidt: float = 0.5) -> dict[str, list[str]]:
+    """The nine setup files with the keys the reference reads."""
+    inflows = inflows or []
+    walls = walls or []
+    names = [f["name"] for f in inflows] + [w["name"] for w in walls]
+    bc = ["array   string  boundary_conditions {", "    " + " ".join(names), "}", ""]
+    for f in inflows:
+        bc.append(f"struct  {f['name']} {{")
+        bc.append("    string  type            =   inflow")
+        bc.append(f"    int     label           =   {f['label']}")
+        for k in ("temperature", "mach", "pressure", "u", "v", "w"):
+            bc.append(f"    real    {k} = {_fmt(float(f[k]))}")
+        if species:
+            bc.append("    int     mole_or_mass    =   1")
+            for sp, y in f.get("Y", {}).items():
+                bc.append(f"    real    {sp} = {_fmt(float(y))}")
+        if turbulence:
+            bc.append(f"    real    turbulence_intensity = {_fmt(float(f.get('ti', 0.01)))}")
+            bc.append(f"    real    turb_viscosity_ratio = {_fmt(float(f.get('mut_ratio', 1.0)))}")
+        bc += ["}", ""]
+    for w in walls:
+        bc.append(f"struct  {w['name']} {{")
+        bc.append("    string  type            =   wall")
+        bc.append(f"    int     label           =   {w['label']}")
+        bc.append(f"    string  thermal_type    =   {w.get('thermal', 'isothermal')}")
+        bc.append(f"    real    temperature     =   {_fmt(float(w.get('temperature', 300.0)))}")
+        bc += ["}", ""]
+    return {
+        "0_global_control.txt": [
+            "bool parallel = 0", f"int initial = {initial}", f"int total_step = {total_step}",
+            f"int output_file = {output_file}", f"int output_screen = {output_screen}"],
+        "1_grid_information.txt": [
+            f"int dimension = {dimension}", f"real gridScale = {_fmt(float(grid_scale))}",
+            "real referenceLength = 1.0", "int wall_distance = 0"],
+        "2_scheme.txt": [
+            "bool    steady = 1", f"real    cfl = {_fmt(float(cfl))}", f"int     implicit_method = {implicit_method}",
+            f"int     DPLUR_inner_step = {dplur_inner_step}", f"real convergence_criteria = {_fmt(float(convergence))}",
+            "int	 temporal_scheme = 0", "real dt = 1e-9", "real total_simulation_time = 7e-3",
+            "int     inner_iteration = 20", "int  inviscid_scheme = 3", f"int  reconstruction = {reconstruction}",
+            "int  limiter = 0", "real entropy_fix_factor = 0.125", "int viscous_order = 2"],
+        "3_species_reactions.txt": [
+            f"bool species = {int(species)}", f"bool reaction = {int(reaction)}",
+            "string mechanism_file = chemistry/combustion_mechanism.inp", "string therm_file = chemistry/therm.dat",
+            "string transport_file = chemistry/tran.dat", f"int chemSrcMethod = {chem_src_method}",
+            "string mix_frac_elem = C", "real hcst_tolerance = 1e-4"],
+        "4_laminar_turbulent.txt": [
+            f"bool    turbulence = {int(turbulence)}", f"int     turbulence_method = {1 if turbulence else 0}",
+            "int     fluctuate_method = 0", "int     RANS_model = 2", "int     turb_implicit   =   1"],
+        "5_boundary_condition.txt": bc,
+        "6_post_process.txt": ["array   int post_process {", "}"],
+        "8_initialization.txt": ["int groups_init = 1", f"string  default_init    =   {default_init}"],
+        "9_transport_property.txt": [
+            "int diffusivity_method = 1", f"real schmidt_number = {_fmt(float(schmidt))}",
+            "real prandtl_number = 0.72", "real turbulent_prandtl_number = 0.9",
+            "real turbulent_schmidt_number = 0.9"],
+    }
+
+
+def write_grid(case: Path, blocks: list[tuple[np.ndarray, np.ndarray, np.ndarray]]) -> None:
+    """blocks: (x, y, z) arrays of shape (mz, my, mx) each."""
+    d = Path(case) / "input_files" / "grid"
+    d.mkdir(parents=True, exist_ok=True)
+    with open(d / "grid   0.grd", "w") as f:
+        f.write(f"{len(blocks)}\n")
+        for x, _, _ in blocks:
+            mz, my, mx = x.shape
+            f.write(f"{mx} {my} {mz}\n")
+        for x, y, z in blocks:
+            for a in (x, y, z):
+                f.write("\n".join(map(repr, np.asarray(a, dtype=np.float64).ravel().tolist())))
+                f.write("\n")
+
+
+def write_boundary(case: Path, faces: list[list[tuple[int, ...]]], inner: list[list[tuple]] | None = None) -> None:
+    """faces[b]: rows (i1, i2, j1, j2, k1, k2, label), 0-based inclusive.
+    inner[b]: pairs ((7 ints of this face), (7 ints of the target face))
+    in the 1-based convention of src/Mesh.cpp:709-741."""
+    d = Path(case) / "input_files" / "boundary_condition"
+    d.mkdir(parents=True, exist_ok=True)
+    lines = []
+    for fl in faces:
+        lines.append(f"{len(fl):12d}")
+        lines += ["".join(f"{v:6d}" for v in row) for row in fl]
+    (d / "boundary   0.txt").write_text("\n".join(lines) + "\n")
+    inner = inner or [[] for _ in faces]
+    il = [f"{len(faces):12d}", "".join(f"{len(fl):12d}" for fl in inner), " imin  imax  jmin  jmax  kmin  kmax   id"]
+    for fl in inner:
+        for src, tar in fl:
+            il.append("".join(f"{v:9d}" for v in src))
+            il.append("".join(f"{v:9d}" for v in tar))
+    (d / "inner   0.txt").write_text("\n".join(il) + "\n")
+    (d / "parallel   0.txt").write_text(f"{len(faces):12d}{0:12d}\n" + "".join(f"{0:12d}" for _ in faces) + "\n")
+
+
+def copy_chemistry(case: Path) -> None:
+    d = Path(case) / "input_files" / "chemistry"
+    d.mkdir(parents=True, exist_ok=True)
+    for f in ("combustion_mechanism.inp", "therm.dat", "tran.dat"):
+        shutil.copyfile(_DATA / f, d / f)
+
+
+def _tanh_wall(n: int, first: float, height: float) -> np.ndarray:
+    """n points on [0, height], one-sided tanh stretching with first spacing
+    close to `first` (the stretching factor is found by bisection)."""
+    s = np.linspace(0.0, 1.0, n)
+
+    def spacing(beta):
+        y = height * (1.0 + np.tanh(beta * (s - 1.0)) / np.tanh(beta))
+        return y[1] - y[0]
+
+    lo, hi = 1e-3, 20.0
+    if spacing(lo) < first:
+        return height * s
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if spacing(mid) > first:
+            lo = mid
+        else:
+            hi = mid
+    beta = 0.5 * (lo + hi)
+    return height * (1.0 + np.tanh(beta * (s - 1.0)) / np.tanh(beta))
+
+
+def ramp_case(case: str | Path, mx: int = 256, my: int = 128, total_step: int = 5000, output_screen: int = 100,
+              output_file: int | None = None) -> Path:
+    """2-D laminar air, Mach 3, p = 2.5 kPa, T = 220 K over a 15 degree
+    compression ramp (corner at x = 0.05 m, x in [0, 0.1] m, top at y = 0.03 m),
+    first cell 1e-5 m at the isothermal 300 K wall; inflow i = 0, outflow
+    i = max, symmetry on top.  AUSM+ / MUSCL-minmod, explicit, CFL 0.5."""
+    case = Path(case)
+    xs = np.linspace(0.0, 0.1, mx)
+    ywall = np.where(xs < 0.05, 0.0, (xs - 0.05) * math.tan(math.radians(15.0)))
+    x = np.empty((1, my, mx))
+    y = np.empty((1, my, mx))
+    for i in range(mx):
+        y[0, :, i] = ywall[i] + _tanh_wall(my, 1e-5, 0.03 - ywall[i])
+        x[0, :, i] = xs[i]
+    z = np.zeros((1, my, mx))
+    write_grid(case, [(x, y, z)])
+    write_boundary(case, [[
+        (0, mx - 1, 0, 0, 0, 0, 2),
+        (0, 0, 0, my - 1, 0, 0, 5),
+        (mx - 1, mx - 1, 0, my - 1, 0, 0, 6),
+        (0, mx - 1, my - 1, my - 1, 0, 0, 3),
+    ]])
+    write_setup(case, setup_files(
+        dimension=2, total_step=total_step, output_file=output_file or total_step, output_screen=output_screen,
+        cfl=0.5, implicit_method=0, dplur_inner_step=3, species=False, reaction=False, turbulence=False,
+        inflows=[dict(name="freestream", label=5, temperature=220.0, mach=3.0, pressure=2500.0, u=1.0, v=0.0,
+                      w=0.0)],
+        walls=[dict(name="wall", label=2, temperature=300.0)]))
+    copy_chemistry(case)
+    return case
+
+
+UPPER = dict(name="freestream", label=5, temperature=1250.0, mach=2.4, pressure=101325.0, u=1.0, v=0.0, w=0.0,
+             Y={"O2": 0.245, "H2O": 0.175, "N2": 0.58}, ti=0.01, mut_ratio=1.0)
+LOWER = dict(name="fuel", label=9, temperature=300.0, mach=1.2, pressure=101325.0, u=1.0, v=0.0, w=0.0,
+             Y={"H2": 0.4, "N2": 0.6}, ti=0.01, mut_ratio=1.0)
+
+
+def _mixing_layer_grid(mx, my, mz, x0=0.0, lx=0.3):
+    xs = np.linspace(x0, x0 + lx, mx)
+    s = np.linspace(-1.0, 1.0, my)
+    ys = 0.025 + 0.025 * np.sinh(3.0 * s) / math.sinh(3.0)
+    zs = np.linspace(0.0, 0.02, mz)
+    z, y, x = np.meshgrid(zs, ys, xs, indexing="ij")
+    return x, y, z
+
+
+def _mixing_setup(case, *, total_step, output_screen, output_file, initial, cfl, dplur, chem, implicit=1):
+    write_setup(case, setup_files(
+        dimension=3, total_step=total_step, output_file=output_file, output_screen=output_screen, cfl=cfl,
+        implicit_method=implicit, dplur_inner_step=dplur, species=True, reaction=True, turbulence=True,
+        chem_src_method=chem, initial=initial, inflows=[UPPER, LOWER]))
+
+
+def _blend_initial_field(case: Path, delta: float = 5e-4) -> None:
+    """Writes output/field/flowfield.plt with a tanh blend (thickness delta)
+    of the two inflow states across y = 0.025 m, plus step.txt and
+    residual_scale.txt, so that a run with initial = 1 starts from it."""
+    from . import Driver
+    from .plt import write_plt
+
+    drv = Driver(case)
+    try:
+        info = drv.info()
+        prm = drv.params()
+        # the two inflow states: the cold stream is the lower one
+        inflow = [b for b in drv.bcs() if b.type == 5]
+        ns, nsc = info.n_spec, info.n_scalar
+        species = _species_names(case)
+        by_t = sorted(inflow, key=lambda b: b.temperature)
+        lo, up = by_t[0], by_t[-1]
+        names = ["x", "y", "z", "density", "u", "v", "w", "pressure", "temperature", "mach"] + species + [
+            "tke", "omega", "mut"]
+        zones = []
+        for blk in range(info.n_block):
+            x = drv.host_field(blk, "x")[0]
+            y = drv.host_field(blk, "y")[0]
+            z = drv.host_field(blk, "z")[0]
+            g = info.ngg
+            x, y, z = x[g:-g, g:-g, g:-g], y[g:-g, g:-g, g:-g], z[g:-g, g:-g, g:-g]
+            phi = 0.5 * (1.0 + np.tanh((y - 0.025) / delta))
+            mix = lambda a, b: phi * b + (1.0 - phi) * a  # noqa: E731
+            zone = {"x": x, "y": y, "z": z}
+            zone["u"] = mix(lo.u, up.u)
+            zone["v"] = np.zeros_like(x)
+            zone["w"] = np.zeros_like(x)
+            zone["pressure"] = np.full_like(x, up.pressure)
+            zone["temperature"] = mix(lo.temperature, up.temperature)
+            Y = [mix(lo.sv[l], up.sv[l]) for l in range(ns)]
+            mw = 1.0 / sum(Y[l] / prm.mw[l] for l in range(ns))
+            zone["density"] = zone["pressure"] * mw / (8314.462618 * zone["temperature"])
+            zone["mach"] = np.zeros_like(x)
+            for l, n in enumerate(species):
+                zone[n] = Y[l]
+            zone["tke"] = mix(lo.sv[ns], up.sv[ns])
+            zone["omega"] = mix(lo.sv[ns + 1], up.sv[ns + 1])
+            zone["mut"] = mix(lo.mut, up.mut)
+            zones.append(zone)
+        write_plt(case / "output" / "field" / "flowfield.plt", names, zones)
+        msg = case / "output" / "message"
+        msg.mkdir(parents=True, exist_ok=True)
+        (msg / "step.txt").write_text("0")
+        (msg / "residual_scale.txt").write_text("1\n1\n1\n1\n")
+    finally:
+        drv.close()
+
+
+def _species_names(case: Path) -> list[str]:
+    text = (Path(case) / "input_files" / "chemistry" / "combustion_mechanism.inp").read_text().split()
+    i = text.index("SPECIES") + 1
+    out = []
+    while text[i].upper() != "END":
+        out.append(text[i].upper())
+        i += 1
+    return out
+
+
+def mixing_layer_case(case: str | Path, mx: int = 384, my: int = 192, mz: int = 64, total_step: int = 2000,
+                      output_screen: int = 100, output_file: int | None = None, cfl: float = 0.5,
+                      dplur: int = 4, chem: int = 1, implicit: int = 1) -> Path:
+    """3-D supersonic H2 / vitiated-air mixing layer (0.3 x 0.05 x 0.02 m,
+    y clustered at the splitter y = 0.025 m).  Upper stream Mach 2.4, 1250 K,
+    Y_O2 0.245, Y_H2O 0.175, N2; lower stream H2 / N2 (0.4 / 0.6) at
+    Mach 1.2, 300 K; 1 atm; 9 species / 19 reactions, k-omega SST with 1 %
+    inflow turbulence, DPLUR with `dplur` sweeps, EPI chemistry."""
+    case = Path(case)
+    x, y, z = _mixing_layer_grid(mx, my, mz)
+    write_grid(case, [(x, y, z)])
+    js = int(np.searchsorted(y[0, :, 0], 0.025))
+    write_boundary(case, [[
+        (0, 0, js, my - 1, 0, mz - 1, 5),
+        (0, 0, 0, js - 1, 0, mz - 1, 9),
+        (mx - 1, mx - 1, 0, my - 1, 0, mz - 1, 6),
+        (0, mx - 1, 0, 0, 0, mz - 1, 3),
+        (0, mx - 1, my - 1, my - 1, 0, mz - 1, 3),
+        (0, mx - 1, 0, my - 1, 0, 0, 3),
+        (0, mx - 1, 0, my - 1, mz - 1, mz - 1, 3),
+    ]])
+    copy_chemistry(case)
+    _mixing_setup(case, total_step=total_step, output_screen=output_screen, output_file=output_file or 10 ** 9,
+                  initial=0, cfl=cfl, dplur=dplur, chem=chem, implicit=implicit)
+    _blend_initial_field(case)
+    _mixing_setup(case, total_step=total_step, output_screen=output_screen, output_file=output_file or 10 ** 9,
+                  initial=1, cfl=cfl, dplur=dplur, chem=chem, implicit=implicit)
+    return case
+
+
+def multiblock_case(case: str | Path, mxs: list[int], my: int = 64, mz: int = 32, total_step: int = 100,
+                    output_screen: int = 10, output_file: int | None = None, cfl: float = 0.5,
+                    dplur: int = 4) -> Path:
+    """Mixing-layer physics on len(mxs) blocks tiled along x (1:1 faces):
+    block b spans mxs[b] points and shares its first plane with the last
+    plane of block b-1."""
+    case = Path(case)
+    total = sum(mxs) - (len(mxs) - 1)
+    x_all, y_all, z_all = _mixing_layer_grid(total, my, mz)
+    blocks, faces, inner = [], [], []
+    i0 = 0
+    nb = len(mxs)
+    js = int(np.searchsorted(y_all[0, :, 0], 0.025))
+    for b, m in enumerate(mxs):
+        sl = slice(i0, i0 + m)
+        blocks.append((x_all[:, :, sl], y_all[:, :, sl], z_all[:, :, sl]))
+        fl = []
+        if b == 0:
+            fl += [(0, 0, js, my - 1, 0, mz - 1, 5), (0, 0, 0, js - 1, 0, mz - 1, 9)]
+        if b == nb - 1:
+            fl.append((m - 1, m - 1, 0, my - 1, 0, mz - 1, 6))
+        fl += [(0, m - 1, 0, 0, 0, mz - 1, 3), (0, m - 1, my - 1, my - 1, 0, mz - 1, 3),
+               (0, m - 1, 0, my - 1, 0, 0, 3), (0, m - 1, 0, my - 1, mz - 1, mz - 1, 3)]
+        faces.append(fl)
+        il = []
+        # 1-based ranges; the negative j range marks the first tangential
+        # direction of a 3-D face (src/Mesh.cpp:84-106).
+        if b > 0:
+            prev = mxs[b - 1]
+            il.append(((1, 1, -1, -my, 1, mz, b + 1), (prev, prev, -1, -my, 1, mz, b)))
+        if b < nb - 1:
+            il.append(((m, m, -1, -my, 1, mz, b + 1), (1, 1, -1, -my, 1, mz, b + 2)))
+        inner.append(il)
+        i0 += m - 1
+    write_grid(case, blocks)
+    write_boundary(case, faces, inner)
+    copy_chemistry(case)
+    _mixing_setup(case, total_step=total_step, output_screen=output_screen, output_file=output_file or 10 ** 9,
+                  initial=0, cfl=cfl, dplur=dplur, chem=1)
+    _blend_initial_field(case)
+    _mixing_setup(case, total_step=total_step, output_screen=output_screen, output_file=output_file or 10 ** 9,
+                  initial=1, cfl=cfl, dplur=dplur, chem=1)
+    return case

@@ -1,0 +1,338 @@
+// extern "C" boundary of libopenstc_b200.so (declared in include/openstc_b200.h).
+#include "../../include/openstc_b200.h"
+
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <string>
+
+#include "host/driver.hpp"
+
+struct ostc_driver {
+  ostc::Driver drv;
+  ostc_driver(const std::string &dir, const ostc::DriverOptions &o) : drv(dir, o) {}
+};
+
+namespace {
+thread_local std::string g_error;
+
+int fail(int code, const std::string &msg) {
+  g_error = msg;
+  return code;
+}
+
+template <typename F>
+int guarded(F &&f) {
+  try {
+    return f();
+  } catch (const ostc::ParameterError &e) {
+    const std::string m = e.what();
+    return fail(m.rfind("Nan occurred", 0) == 0 ? OSTC_ERR_NAN : OSTC_ERR_INPUT, m);
+  } catch (const std::exception &e) {
+    const std::string m = e.what();
+    return fail(m.rfind("CUDA error", 0) == 0 ? OSTC_ERR_CUDA : OSTC_ERR_INTERNAL, m);
+  }
+}
+
+// Ghost layers / components of a field for a configuration; mirrors the
+// engine's allocation (0 components: not allocated).
+void field_layout(const ostc::DevParams &p, int ngg, int field, int &ghost, int &nc) {
+  const bool dplur = p.implicit_method == 1;
+  ghost = ngg;
+  nc = 1;
+  switch (field) {
+    case OSTC_METRIC: nc = 9; break;
+    case OSTC_WALL_DIST: case OSTC_MUT: case OSTC_TURB_COND: nc = p.turb ? 1 : 0; break;
+    case OSTC_BV: nc = 6; break;
+    case OSTC_SV: nc = p.n_scalar; break;
+    case OSTC_CV: nc = p.n_var; break;
+    case OSTC_RHO_D: nc = p.ns; break;
+    case OSTC_CHEM_JAC:
+      ghost = 0;
+      nc = (p.mix == 2 && p.chem_src_method != 0) ? (p.chem_src_method == 2 ? p.ns : p.ns * p.ns) : 0;
+      break;
+    case OSTC_TURB_SRC_JAC: ghost = 0; nc = p.turb ? 2 : 0; break;
+    case OSTC_DQ: ghost = dplur ? 1 : 0; nc = p.n_var; break;
+    case OSTC_DQ0: case OSTC_DQK: ghost = dplur ? 1 : 0; nc = dplur ? p.n_var : 0; break;
+    case OSTC_INV_SPEC: ghost = dplur ? 1 : 0; nc = 3; break;
+    case OSTC_VISC_SPEC: ghost = dplur ? 1 : 0; break;
+    case OSTC_DT_LOCAL: ghost = 0; break;
+    case OSTC_BV_LAST: ghost = 0; nc = 4; break;
+    default: break;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+const char *ostc_last_error(void) { return g_error.c_str(); }
+
+int ostc_driver_create(const char *case_dir, const ostc_options *opt, ostc_driver **out) {
+  if (!case_dir || !out) return fail(OSTC_ERR_INPUT, "null argument");
+  *out = nullptr;
+  return guarded([&] {
+    ostc::DriverOptions o;
+    if (opt) {
+      o.device = opt->device;
+      o.quiet = opt->quiet != 0;
+    }
+    *out = new ostc_driver(case_dir, o);
+    return OSTC_OK;
+  });
+}
+
+void ostc_driver_destroy(ostc_driver *d) { delete d; }
+
+int ostc_driver_info(const ostc_driver *d, ostc_info *info) {
+  if (!d || !info) return fail(OSTC_ERR_INPUT, "null argument");
+  const ostc::Driver &D = d->drv;
+  std::memset(info, 0, sizeof(*info));
+  info->n_block = D.mesh.n_block;
+  info->ngg = D.mesh.ngg;
+  info->dimension = D.mesh.dimension;
+  info->n_spec = D.spec.n_spec;
+  info->n_reac = D.reac.n_reac;
+  info->n_var = D.dev_params.n_var;
+  info->n_scalar = D.dev_params.n_scalar;
+  info->mix = D.mix;
+  info->rans = D.rans ? 1 : 0;
+  info->implicit_method = D.dev_params.implicit_method;
+  info->dplur_inner_step = D.dev_params.dplur_inner_step;
+  info->chem_src_method = D.dev_params.chem_src_method;
+  info->step = D.step;
+  info->n_grid_total = D.mesh.n_grid_total;
+  info->n_bc = static_cast<int>(D.host_bcs.size());
+  info->n_inner = static_cast<int>(D.host_inner.size());
+  return OSTC_OK;
+}
+
+int ostc_driver_params(const ostc_driver *d, ostc_params *o) {
+  if (!d || !o) return fail(OSTC_ERR_INPUT, "null argument");
+  const ostc::DevParams &p = d->drv.dev_params;
+  std::memset(o, 0, sizeof(*o));
+  o->ns = p.ns;
+  o->nr = p.nr;
+  o->n_var = p.n_var;
+  o->n_scalar = p.n_scalar;
+  o->mix = p.mix;
+  o->turb = p.turb;
+  o->rans_model = p.rans_model;
+  o->turb_implicit = p.turb_implicit;
+  o->chem_src_method = p.chem_src_method;
+  o->implicit_method = p.implicit_method;
+  o->dplur_inner_step = p.dplur_inner_step;
+  o->reconstruction = p.reconstruction;
+  o->limiter = p.limiter;
+  o->viscous_order = p.viscous_order;
+  o->dim = p.dim;
+  o->output_screen = d->drv.parameter.get_int("output_screen");
+  o->cfl = p.cfl;
+  o->Pr = p.Pr;
+  o->Prt = p.Prt;
+  o->Sct = p.Sct;
+  o->Sc = p.Sc;
+  std::memcpy(o->ll, p.ll, sizeof(p.ll));
+  std::memcpy(o->ul, p.ul, sizeof(p.ul));
+  std::memcpy(o->sv_inf, p.sv_inf, sizeof(p.sv_inf));
+  const int ns = p.ns;
+  for (int i = 0; i < ns; ++i) {
+    o->mw[i] = p.mw[i];
+    o->t_low[i] = p.t_low[i];
+    o->t_mid[i] = p.t_mid[i];
+    o->lj_inv[i] = p.lj_inv[i];
+    o->vis_coeff[i] = p.vis_coeff[i];
+  }
+  std::memcpy(o->low_coeff, p.low, sizeof(double) * 7 * ns);
+  std::memcpy(o->high_coeff, p.high, sizeof(double) * 7 * ns);
+  std::memcpy(o->w_quarter, p.wq, sizeof(double) * ns * ns);
+  std::memcpy(o->w_sqrt8, p.w8, sizeof(double) * ns * ns);
+  for (int r = 0; r < p.nr; ++r) {
+    o->label[r] = p.label[r];
+    o->order[r] = p.order[r];
+    o->A[r] = p.A[r];
+    o->b[r] = p.b[r];
+    o->Ea[r] = p.Ea[r];
+    o->A2[r] = p.A2[r];
+    o->b2[r] = p.b2[r];
+    o->Ea2[r] = p.Ea2[r];
+    o->troe_alpha[r] = p.troe_a[r];
+    o->troe_t3[r] = p.troe_t3[r];
+    o->troe_t1[r] = p.troe_t1[r];
+    o->troe_t2[r] = p.troe_t2[r];
+    for (int l = 0; l < ns; ++l) {
+      o->stoi_f[r * ns + l] = p.sf[r * ns + l];
+      o->stoi_b[r * ns + l] = p.sb[r * ns + l];
+      o->third_body[r * ns + l] = p.tb[r * ns + l];
+    }
+  }
+  return OSTC_OK;
+}
+
+int ostc_driver_bc(const ostc_driver *d, int index, ostc_bc *bc) {
+  if (!d || !bc) return fail(OSTC_ERR_INPUT, "null argument");
+  if (index < 0 || index >= static_cast<int>(d->drv.host_bcs.size())) return fail(OSTC_ERR_INPUT, "bc index");
+  static_assert(sizeof(ostc_bc) == sizeof(ostc::HostBc), "ostc_bc layout");
+  std::memcpy(bc, &d->drv.host_bcs[index], sizeof(ostc_bc));
+  return OSTC_OK;
+}
+
+int ostc_driver_inner(const ostc_driver *d, int index, ostc_inner *f) {
+  if (!d || !f) return fail(OSTC_ERR_INPUT, "null argument");
+  if (index < 0 || index >= static_cast<int>(d->drv.host_inner.size())) return fail(OSTC_ERR_INPUT, "inner index");
+  static_assert(sizeof(ostc_inner) == sizeof(ostc::HostInner), "ostc_inner layout");
+  std::memcpy(f, &d->drv.host_inner[index], sizeof(ostc_inner));
+  return OSTC_OK;
+}
+
+int ostc_driver_block_dims(const ostc_driver *d, int block, int dims[3]) {
+  if (!d || !dims) return fail(OSTC_ERR_INPUT, "null argument");
+  if (block < 0 || block >= d->drv.mesh.n_block) return fail(OSTC_ERR_INPUT, "block index");
+  const ostc::Block &B = d->drv.mesh[block];
+  dims[0] = B.mx;
+  dims[1] = B.my;
+  dims[2] = B.mz;
+  return OSTC_OK;
+}
+
+int ostc_field_layout(const ostc_driver *d, int field, int *ghost, int *components) {
+  if (!d || !ghost || !components) return fail(OSTC_ERR_INPUT, "null argument");
+  if (field < 0 || field >= OSTC_N_FIELDS) return fail(OSTC_ERR_INPUT, "field id");
+  field_layout(d->drv.dev_params, d->drv.mesh.ngg, field, *ghost, *components);
+  return OSTC_OK;
+}
+
+int ostc_driver_get_host_field(const ostc_driver *d, int block, int field, double *out, int64_t count) {
+  if (!d || !out) return fail(OSTC_ERR_INPUT, "null argument");
+  return guarded([&] {
+    const ostc::Driver &D = d->drv;
+    if (block < 0 || block >= D.mesh.n_block) return fail(OSTC_ERR_INPUT, "block index");
+    const ostc::Block &B = D.mesh[block];
+    const ostc::HostField &F = D.field[block];
+    const int64_t n = B.x.e.size();
+    auto put = [&](const double *src, int64_t want) {
+      if (count != want) return fail(OSTC_ERR_INPUT, "count mismatch: expected " + std::to_string(want));
+      std::memcpy(out, src, sizeof(double) * want);
+      return static_cast<int>(OSTC_OK);
+    };
+    switch (field) {
+      case OSTC_X: return put(B.x.v.data(), n);
+      case OSTC_Y: return put(B.y.v.data(), n);
+      case OSTC_Z: return put(B.z.v.data(), n);
+      case OSTC_JAC: return put(B.jac.v.data(), n);
+      case OSTC_METRIC: {
+        if (count != 9 * n) return fail(OSTC_ERR_INPUT, "count mismatch: expected " + std::to_string(9 * n));
+        for (int q = 0; q < 9; ++q) std::memcpy(out + q * n, B.metric[q].v.data(), sizeof(double) * n);
+        return static_cast<int>(OSTC_OK);
+      }
+      case OSTC_BV: return put(F.bv.data(), static_cast<int64_t>(F.bv.size()));
+      case OSTC_SV: return put(F.sv.data(), static_cast<int64_t>(F.sv.size()));
+      default: return fail(OSTC_ERR_INPUT, "field has no host copy");
+    }
+  });
+}
+
+int ostc_driver_initialize(ostc_driver *d) {
+  if (!d) return fail(OSTC_ERR_INPUT, "null argument");
+  return guarded([&] {
+    d->drv.initialize_computation();
+    return OSTC_OK;
+  });
+}
+
+int ostc_driver_simulate(ostc_driver *d) {
+  if (!d) return fail(OSTC_ERR_INPUT, "null argument");
+  if (!d->drv.initialized()) return fail(OSTC_ERR_STATE, "initialize first");
+  return guarded([&] {
+    d->drv.simulate();
+    return OSTC_OK;
+  });
+}
+
+int ostc_driver_step(ostc_driver *d, int n_steps, double *err_max) {
+  if (!d || n_steps < 0) return fail(OSTC_ERR_INPUT, "bad argument");
+  if (!d->drv.initialized()) return fail(OSTC_ERR_STATE, "initialize first");
+  return guarded([&] {
+    const double e = d->drv.advance(n_steps);
+    if (err_max) *err_max = e;
+    return OSTC_OK;
+  });
+}
+
+int ostc_driver_residual(const ostc_driver *d, double res[4]) {
+  if (!d || !res) return fail(OSTC_ERR_INPUT, "null argument");
+  for (int l = 0; l < 4; ++l) res[l] = d->drv.res[l];
+  return OSTC_OK;
+}
+
+int ostc_driver_run_phase(ostc_driver *d, int phase) {
+  if (!d) return fail(OSTC_ERR_INPUT, "null argument");
+  if (!d->drv.initialized()) return fail(OSTC_ERR_STATE, "initialize first");
+  return guarded([&] {
+    d->drv.engine().phase(phase);
+    return OSTC_OK;
+  });
+}
+
+int ostc_driver_get_field(ostc_driver *d, int block, int field, double *out, int64_t count) {
+  if (!d || !out) return fail(OSTC_ERR_INPUT, "null argument");
+  if (!d->drv.initialized()) return fail(OSTC_ERR_STATE, "initialize first");
+  return guarded([&] {
+    d->drv.engine().get_field(block, field, out, count);
+    return OSTC_OK;
+  });
+}
+
+int ostc_driver_set_field(ostc_driver *d, int block, int field, const double *in, int64_t count) {
+  if (!d || !in) return fail(OSTC_ERR_INPUT, "null argument");
+  if (!d->drv.initialized()) return fail(OSTC_ERR_STATE, "initialize first");
+  return guarded([&] {
+    d->drv.engine().set_field(block, field, in, count);
+    return OSTC_OK;
+  });
+}
+
+int ostc_driver_write_plt(ostc_driver *d, const char *path) {
+  if (!d || !path) return fail(OSTC_ERR_INPUT, "null argument");
+  if (!d->drv.initialized()) return fail(OSTC_ERR_STATE, "initialize first");
+  return guarded([&] {
+    d->drv.write_field(path);
+    return OSTC_OK;
+  });
+}
+
+int ostc_driver_launches_per_step(const ostc_driver *d, int store_last, int residual) {
+  if (!d) return fail(OSTC_ERR_INPUT, "null argument");
+  if (!d->drv.initialized()) return fail(OSTC_ERR_STATE, "initialize first");
+  return const_cast<ostc_driver *>(d)->drv.engine().launches_per_step(store_last != 0, residual != 0);
+}
+
+int ostc_driver_last_step_ms(const ostc_driver *d, double *ms) {
+  if (!d || !ms) return fail(OSTC_ERR_INPUT, "null argument");
+  if (!d->drv.initialized()) return fail(OSTC_ERR_STATE, "initialize first");
+  *ms = const_cast<ostc_driver *>(d)->drv.engine().last_step_ms();
+  return OSTC_OK;
+}
+
+int ostc_driver_profile_step(ostc_driver *d, char *buf, int buflen) {
+  if (!d || !buf || buflen <= 0) return fail(OSTC_ERR_INPUT, "bad argument");
+  if (!d->drv.initialized()) return fail(OSTC_ERR_STATE, "initialize first");
+  return guarded([&] {
+    const auto rows = d->drv.engine().profile_step();
+    std::string text;
+    for (const auto &[name, n, ms] : rows) {
+      char line[160];
+      std::snprintf(line, sizeof(line), "%s %d %.6f\n", name.c_str(), n, ms);
+      text += line;
+    }
+    if (static_cast<int>(text.size()) + 1 > buflen) return fail(OSTC_ERR_INPUT, "buffer too small");
+    std::memcpy(buf, text.c_str(), text.size() + 1);
+    return static_cast<int>(rows.size());
+  });
+}
+
+void *ostc_driver_stream(ostc_driver *d) {
+  if (!d || !d->drv.initialized()) return nullptr;
+  return d->drv.engine().stream();
+}
+
+}  // extern "C"

@@ -1,0 +1,81 @@
+// Device-side data layout and parameters of the sm_100a engine.
+//
+// State arrays keep the reference's column-major layout with ghost layers
+// (src/gxl_lib/Array.hpp:71-130) so that the C ABI can copy the host fields
+// of the reference unchanged; the metric is stored as nine arrays instead of
+// a 3x3 struct per point, and the inviscid spectral radius as three arrays.
+#pragma once
+
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define OSTC_HD __host__ __device__
+#else
+#define OSTC_HD
+#endif
+
+namespace ostc {
+
+constexpr int kMaxSpec = 20;
+constexpr int kMaxReac = 50;
+constexpr int kMaxBlocks = 16;
+
+constexpr double kDR_u = 8314.462618;
+constexpr double kDP_atm = 101325.0;
+constexpr double kDGammaAir = 1.4;
+constexpr double kDMwAir = 28.9647;
+
+// Physics constants and mechanism tables; lives in __constant__ memory.
+struct DevParams {
+  int ns, nr, n_var, n_scalar;
+  int mix, turb, rans_model, turb_implicit, chem_src_method, implicit_method, dplur_inner_step;
+  int reconstruction, limiter, viscous_order, dim;
+  double cfl, Pr, Prt, Sct, Sc;
+  double ll[7], ul[7];
+  double sv_inf[kMaxSpec + 2];
+  double mw[kMaxSpec], t_low[kMaxSpec], t_mid[kMaxSpec];
+  double low[kMaxSpec * 7], high[kMaxSpec * 7];
+  double lj_inv[kMaxSpec], vis_coeff[kMaxSpec];
+  double wq[kMaxSpec * kMaxSpec], w8[kMaxSpec * kMaxSpec];
+  int label[kMaxReac], order[kMaxReac];
+  signed char sf[kMaxReac * kMaxSpec], sb[kMaxReac * kMaxSpec];
+  double A[kMaxReac], b[kMaxReac], Ea[kMaxReac], A2[kMaxReac], b2[kMaxReac], Ea2[kMaxReac];
+  double tb[kMaxReac * kMaxSpec];
+  double troe_a[kMaxReac], troe_t3[kMaxReac], troe_t1[kMaxReac], troe_t2[kMaxReac];
+};
+
+// Strides of a 3-D array with a given number of ghost layers.
+struct Lay {
+  int64_t sx = 0, sxy = 0, size = 0, off = 0;
+  OSTC_HD int64_t at(int i, int j, int k) const { return k * sxy + j * sx + i + off; }
+  static Lay make(int mx, int my, int mz, int g) {
+    Lay l;
+    l.sx = mx + 2 * g;
+    l.sxy = l.sx * (my + 2 * g);
+    l.size = l.sxy * (mz + 2 * g);
+    l.off = (l.sxy + l.sx + 1) * g;
+    return l;
+  }
+};
+
+// One grid block's device arrays.  G: ngg ghost layers; D: layout of the
+// dq family (one ghost layer under DPLUR, none otherwise); Z: no ghosts.
+struct DevBlock {
+  int mx, my, mz, ngg;
+  Lay G, D, Z;
+  double *x, *y, *z, *jac, *metric, *wall_dist;
+  double *bv, *sv, *cv, *vel, *acoustic, *mach, *mul, *cond, *rho_d, *gamma, *cp, *mut, *turb_cond;
+  double *chem_jac, *turb_src_jac;
+  unsigned char *lu_piv;
+  double *dq, *dq0, *dqk, *inv_spec, *visc_spec, *dt_local, *bv_last;
+};
+
+// Work table of a launch: CTA-tiles of every block, in block order.
+struct Tiles {
+  int nblk = 0;
+  int begin[kMaxBlocks + 1] = {};
+  int ntx[kMaxBlocks] = {}, nty[kMaxBlocks] = {};
+  int halo = 0;  // cells [-halo, m+halo) in every direction
+};
+
+}  // namespace ostc

@@ -1,0 +1,83 @@
+// Host-side interface of the device engine: device memory for all grid
+// blocks, the launch sequence of one pseudo-time step and its CUDA graph.
+#pragma once
+
+#include <array>
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "common.cuh"
+
+namespace ostc {
+
+// Field identifiers of the C ABI (ostc_field_id in include/openstc_b200.h).
+enum FieldId : int {
+  F_X = 0, F_Y, F_Z, F_JAC, F_METRIC, F_WALL_DIST, F_BV, F_SV, F_CV, F_VEL, F_ACOUSTIC, F_MACH, F_MUL,
+  F_CONDUCTIVITY, F_RHO_D, F_GAMMA, F_CP, F_MUT, F_TURB_COND, F_CHEM_JAC, F_TURB_SRC_JAC, F_DQ, F_DQ0, F_DQK,
+  F_INV_SPEC, F_VISC_SPEC, F_DT_LOCAL, F_BV_LAST, F_N_FIELDS
+};
+
+struct HostBc {
+  int block, type, face, direction;
+  int start[3], end[3];
+  double density, u, v, w, pressure, temperature, mut;
+  double sv[kMaxSpec + 2];
+  int isothermal;
+  double t_wall;
+};
+
+struct HostInner {
+  int block, target_block, face, direction;
+  int start[3], end[3], loop_dir[3], tstart[3], tloop_dir[3], src_tar[3], n_point[3];
+};
+
+struct EngineSetup {
+  DevParams params;
+  int ngg = 2;
+  std::vector<std::array<int, 3>> dims;
+  std::vector<HostBc> bcs;        // application order
+  std::vector<HostInner> inner;   // application order
+  std::vector<double> wall_points;  // x,y,z triples for the wall distance
+  int device = 0;
+};
+
+class Engine {
+ public:
+  virtual ~Engine() = default;
+  // Copy a host array (reference layout) into a device field of block b.
+  virtual void set_field(int b, int field, const double *host, int64_t count) = 0;
+  virtual void get_field(int b, int field, double *host, int64_t count) = 0;
+  virtual int64_t field_count(int b, int field) const = 0;
+  // Driver::initialize_computation, src/Driver.cu:44-104.
+  virtual void initialize() = 0;
+  // One pass of the steady loop body; res receives the raw RMS sums when
+  // `residual` is set.  Uses a cached CUDA graph per (store, residual).
+  virtual void step(bool store_last, bool residual, double res[4]) = 0;
+  // Phases for per-kernel parity tests.
+  virtual void phase(int which) = 0;
+  virtual void synchronize() = 0;
+  virtual void *stream() = 0;
+  virtual const std::vector<DevBlock> &blocks() const = 0;
+  virtual int launches_per_step(bool store_last, bool residual) const = 0;
+  // Runs one step eagerly (no graph) with an event after every launch and
+  // returns (kernel name, launches, total ms).  Advances the solution.
+  virtual std::vector<std::tuple<std::string, int, double>> profile_step() = 0;
+  virtual double last_step_ms() const = 0;
+};
+
+std::unique_ptr<Engine> make_engine(const EngineSetup &setup);
+
+// Per-configuration factories (one translation unit each).
+std::unique_ptr<Engine> make_engine_air_lam(const EngineSetup &);
+std::unique_ptr<Engine> make_engine_air_sst(const EngineSetup &);
+std::unique_ptr<Engine> make_engine_mix9_lam(const EngineSetup &);
+std::unique_ptr<Engine> make_engine_mix9_sst(const EngineSetup &);
+std::unique_ptr<Engine> make_engine_fr9_lam(const EngineSetup &);
+std::unique_ptr<Engine> make_engine_fr9_sst(const EngineSetup &);
+
+void cuda_check(int err, const char *what);
+
+}  // namespace ostc

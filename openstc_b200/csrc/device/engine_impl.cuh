@@ -1,0 +1,493 @@
+// Templated engine implementation; included by one .cu file per model
+// configuration.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <stdexcept>
+#include <string>
+
+#include "engine.hpp"
+#include "kernels_step.cuh"
+
+namespace ostc {
+
+template <class C>
+class EngineT final : public Engine {
+ public:
+  explicit EngineT(const EngineSetup &s) : setup_(s) {
+    cuda_check(cudaSetDevice(s.device), "cudaSetDevice");
+    cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (s.params.ns != C::ns) throw std::runtime_error("engine instantiated for another species count");
+    if (static_cast<int>(s.dims.size()) > kMaxBlocks)
+      throw std::runtime_error("at most " + std::to_string(kMaxBlocks) + " grid blocks per engine");
+    upload_params();
+    const bool dplur = s.params.implicit_method == 1;
+    const int ngg = s.ngg;
+    for (const auto &d : s.dims) {
+      DevBlock B{};
+      B.mx = d[0];
+      B.my = d[1];
+      B.mz = d[2];
+      B.ngg = ngg;
+      B.G = Lay::make(d[0], d[1], d[2], ngg);
+      B.D = Lay::make(d[0], d[1], d[2], dplur ? 1 : 0);
+      B.Z = Lay::make(d[0], d[1], d[2], 0);
+      blocks_.push_back(B);
+    }
+    for (int b = 0; b < static_cast<int>(blocks_.size()); ++b) allocate(blocks_[b]);
+    cuda_check(cudaMalloc(&d_blocks_, sizeof(DevBlock) * blocks_.size()), "cudaMalloc blocks");
+    cuda_check(cudaMemcpy(d_blocks_, blocks_.data(), sizeof(DevBlock) * blocks_.size(), cudaMemcpyHostToDevice),
+               "copy blocks");
+    // boundary and inner faces
+    std::vector<DevBc> bcs;
+    for (const auto &h : s.bcs) {
+      DevBc d{};
+      std::memcpy(&d, &h, sizeof(DevBc));
+      bcs.push_back(d);
+    }
+    static_assert(sizeof(DevBc) == sizeof(HostBc), "DevBc / HostBc layouts differ");
+    if (!bcs.empty()) {
+      cuda_check(cudaMalloc(&d_bcs_, sizeof(DevBc) * bcs.size()), "cudaMalloc bcs");
+      cuda_check(cudaMemcpy(d_bcs_, bcs.data(), sizeof(DevBc) * bcs.size(), cudaMemcpyHostToDevice), "copy bcs");
+    }
+    static_assert(sizeof(DevInner) == sizeof(HostInner), "DevInner / HostInner layouts differ");
+    if (!s.inner.empty()) {
+      cuda_check(cudaMalloc(&d_inner_, sizeof(DevInner) * s.inner.size()), "cudaMalloc inner");
+      cuda_check(cudaMemcpy(d_inner_, s.inner.data(), sizeof(DevInner) * s.inner.size(), cudaMemcpyHostToDevice),
+                 "copy inner");
+    }
+    tiles0_ = make_tiles(0);
+    tiles1_ = make_tiles(1);
+    tilesg_ = make_tiles(ngg);
+    cuda_check(cudaMalloc(&d_partial_, sizeof(double) * 4 * tiles0_.begin[tiles0_.nblk]), "cudaMalloc partial");
+    cuda_check(cudaMalloc(&d_res_, sizeof(double) * 4), "cudaMalloc res");
+    cuda_check(cudaMalloc(&d_bad_, sizeof(unsigned int)), "cudaMalloc bad");
+    cuda_check(cudaMemset(d_bad_, 0, sizeof(unsigned int)), "memset bad");
+    cuda_check(cudaMallocHost(&h_res_, sizeof(double) * 4), "cudaMallocHost res");
+    if (!s.wall_points.empty()) {
+      cuda_check(cudaMalloc(&d_wall_, sizeof(double) * s.wall_points.size()), "cudaMalloc wall");
+      cuda_check(cudaMemcpy(d_wall_, s.wall_points.data(), sizeof(double) * s.wall_points.size(),
+                            cudaMemcpyHostToDevice),
+                 "copy wall");
+    }
+    source_smem_ = C::mix == 2 ? 2 * std::max(1, s.params.nr) * kCta * sizeof(double) : 0;
+    flux_smem_ = C::nv * kCta * sizeof(double);
+    if (source_smem_ > 48 * 1024)
+      cuda_check(cudaFuncSetAttribute(k_source<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(source_smem_)),
+                 "smem attribute");
+    cuda_check(cudaEventCreate(&ev0_), "event");
+    cuda_check(cudaEventCreate(&ev1_), "event");
+  }
+
+  ~EngineT() override {
+    for (auto &g : graphs_)
+      if (g) cudaGraphExecDestroy(g);
+    for (void *p : allocations_) cudaFree(p);
+    cudaFree(d_blocks_);
+    cudaFree(d_bcs_);
+    cudaFree(d_inner_);
+    cudaFree(d_partial_);
+    cudaFree(d_res_);
+    cudaFree(d_bad_);
+    cudaFree(d_wall_);
+    cudaFreeHost(h_res_);
+    cudaEventDestroy(ev0_);
+    cudaEventDestroy(ev1_);
+    cudaStreamDestroy(stream_);
+  }
+
+  void set_field(int b, int field, const double *host, int64_t count) override {
+    double *p = field_ptr(b, field);
+    check_count(b, field, count);
+    upload_params();
+    cuda_check(cudaMemcpyAsync(p, host, sizeof(double) * count, cudaMemcpyHostToDevice, stream_), "set_field");
+    cuda_check(cudaStreamSynchronize(stream_), "set_field sync");
+  }
+
+  void get_field(int b, int field, double *host, int64_t count) override {
+    double *p = field_ptr(b, field);
+    check_count(b, field, count);
+    cuda_check(cudaMemcpyAsync(host, p, sizeof(double) * count, cudaMemcpyDeviceToHost, stream_), "get_field");
+    cuda_check(cudaStreamSynchronize(stream_), "get_field sync");
+  }
+
+  int64_t field_count(int b, int field) const override {
+    const DevBlock &B = blocks_.at(b);
+    int nc = 0;
+    const Lay &L = layout_of(B, field, nc);
+    return field_pointer(B, field) ? L.size * nc : 0;
+  }
+
+  void initialize() override {
+    upload_params();
+    const auto &p = setup_.params;
+    if (C::turb && p.rans_model == 2)
+      k_wall_distance<<<grid(tilesg_), block3(), 0, stream_>>>(d_blocks_, tilesg_, d_wall_,
+                                                              static_cast<int>(setup_.wall_points.size() / 3));
+    if (p.dim == 2) launch_kcopy();
+    launch_bcs();
+    k_cv_from_bv<C><<<grid(tilesg_), block3(), 0, stream_>>>(d_blocks_, tilesg_);
+    if constexpr (C::turb) k_init_mut<C><<<grid(tiles1_), block3(), 0, stream_>>>(d_blocks_, tiles1_);
+    launch_inner();
+    k_props<C><<<grid(tiles1_), block3(), 0, stream_>>>(d_blocks_, tiles1_);
+    cuda_check(cudaGetLastError(), "initialize launch");
+    cuda_check(cudaStreamSynchronize(stream_), "initialize");
+  }
+
+  void step(bool store_last, bool residual, double res[4]) override {
+    upload_params();
+    const int key = (store_last ? 1 : 0) + (residual ? 2 : 0);
+    if (!graphs_[key]) {
+      cudaGraph_t g;
+      cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+      enqueue_step(store_last, residual);
+      cuda_check(cudaStreamEndCapture(stream_, &g), "end capture");
+      cuda_check(cudaGraphInstantiate(&graphs_[key], g, 0), "graph instantiate");
+      cudaGraphDestroy(g);
+    }
+    cuda_check(cudaEventRecord(ev0_, stream_), "event");
+    cuda_check(cudaGraphLaunch(graphs_[key], stream_), "graph launch");
+    cuda_check(cudaEventRecord(ev1_, stream_), "event");
+    if (residual) {
+      cuda_check(cudaStreamSynchronize(stream_), "step sync");
+      for (int l = 0; l < 4; ++l) res[l] = h_res_[l];
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev0_, ev1_);
+      last_ms_ = ms;
+    }
+  }
+
+  void phase(int which) override {
+    upload_params();
+    switch (which) {
+      case 0:
+        launch_residual();
+        break;
+      case 1:
+        launch_implicit();
+        break;
+      case 2:
+        launch_update();
+        break;
+      case 3:
+        launch_bcs();
+        break;
+      case 4:
+        launch_exchange();
+        break;
+      case 5:
+        k_store_last<<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_);
+        break;
+      default:
+        throw std::runtime_error("unknown phase");
+    }
+    cuda_check(cudaGetLastError(), "phase launch");
+    cuda_check(cudaStreamSynchronize(stream_), "phase");
+  }
+
+  void synchronize() override { cuda_check(cudaStreamSynchronize(stream_), "synchronize"); }
+
+  std::vector<std::tuple<std::string, int, double>> profile_step() override {
+    upload_params();
+    std::vector<std::pair<const char *, cudaEvent_t>> marks;
+    cudaEvent_t start;
+    cuda_check(cudaEventCreate(&start), "event");
+    cuda_check(cudaEventRecord(start, stream_), "event");
+    marks_ = &marks;
+    enqueue_step(false, false);
+    marks_ = nullptr;
+    cuda_check(cudaStreamSynchronize(stream_), "profile sync");
+    std::map<std::string, std::pair<int, double>> agg;
+    std::vector<std::string> order;
+    cudaEvent_t prev = start;
+    for (auto &[name, ev] : marks) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, prev, ev);
+      if (!agg.count(name)) order.push_back(name);
+      agg[name].first += 1;
+      agg[name].second += ms;
+      prev = ev;
+    }
+    for (auto &m : marks) cudaEventDestroy(m.second);
+    cudaEventDestroy(start);
+    std::vector<std::tuple<std::string, int, double>> out;
+    for (const auto &n : order) out.emplace_back(n, agg[n].first, agg[n].second);
+    return out;
+  }
+  void *stream() override { return stream_; }
+  const std::vector<DevBlock> &blocks() const override { return blocks_; }
+  double last_step_ms() const override { return last_ms_; }
+
+  int launches_per_step(bool store_last, bool residual) const override {
+    const auto &p = setup_.params;
+    int n = 2;  // source, flux
+    if (p.implicit_method == 1) {
+      n += 1 + p.dplur_inner_step;
+    } else if ((C::mix == 2 && p.chem_src_method != 0) || (C::turb && p.turb_implicit == 1)) {
+      n += 1;
+    }
+    n += 2;  // update, limiter
+    n += static_cast<int>(setup_.bcs.size());
+    n += static_cast<int>(setup_.inner.size());
+    if (p.dim == 2) n += static_cast<int>(blocks_.size());
+    n += 1;  // properties
+    if (store_last) n += 1;
+    if (residual) n += 2;
+    return n;
+  }
+
+ private:
+  void upload_params() {
+    // The __constant__ parameter block is per translation unit and per
+    // device; re-upload when another engine of this configuration ran last.
+    static const void *owner = nullptr;
+    if (owner != this) {
+      cuda_check(cudaMemcpyToSymbol(cP, &setup_.params, sizeof(DevParams)), "upload params");
+      owner = this;
+    }
+  }
+
+  double *&field_pointer(DevBlock &B, int f) const {
+    switch (f) {
+      case F_X: return B.x;
+      case F_Y: return B.y;
+      case F_Z: return B.z;
+      case F_JAC: return B.jac;
+      case F_METRIC: return B.metric;
+      case F_WALL_DIST: return B.wall_dist;
+      case F_BV: return B.bv;
+      case F_SV: return B.sv;
+      case F_CV: return B.cv;
+      case F_VEL: return B.vel;
+      case F_ACOUSTIC: return B.acoustic;
+      case F_MACH: return B.mach;
+      case F_MUL: return B.mul;
+      case F_CONDUCTIVITY: return B.cond;
+      case F_RHO_D: return B.rho_d;
+      case F_GAMMA: return B.gamma;
+      case F_CP: return B.cp;
+      case F_MUT: return B.mut;
+      case F_TURB_COND: return B.turb_cond;
+      case F_CHEM_JAC: return B.chem_jac;
+      case F_TURB_SRC_JAC: return B.turb_src_jac;
+      case F_DQ: return B.dq;
+      case F_DQ0: return B.dq0;
+      case F_DQK: return B.dqk;
+      case F_INV_SPEC: return B.inv_spec;
+      case F_VISC_SPEC: return B.visc_spec;
+      case F_DT_LOCAL: return B.dt_local;
+      case F_BV_LAST: return B.bv_last;
+      default: throw std::runtime_error("unknown field id " + std::to_string(f));
+    }
+  }
+  double *field_pointer(const DevBlock &B, int f) const { return field_pointer(const_cast<DevBlock &>(B), f); }
+
+  const Lay &layout_of(const DevBlock &B, int f, int &nc) const {
+    const auto &p = setup_.params;
+    nc = 1;
+    switch (f) {
+      case F_METRIC: nc = 9; return B.G;
+      case F_BV: nc = 6; return B.G;
+      case F_SV: nc = C::nsc; return B.G;
+      case F_CV: nc = C::nv; return B.G;
+      case F_RHO_D: nc = C::ns; return B.G;
+      case F_CHEM_JAC: nc = p.chem_src_method == 2 ? C::ns : C::ns * C::ns; return B.Z;
+      case F_TURB_SRC_JAC: nc = 2; return B.Z;
+      case F_DQ: case F_DQ0: case F_DQK: nc = C::nv; return B.D;
+      case F_INV_SPEC: nc = 3; return B.D;
+      case F_VISC_SPEC: return B.D;
+      case F_DT_LOCAL: return B.Z;
+      case F_BV_LAST: nc = 4; return B.Z;
+      default: return B.G;
+    }
+  }
+
+  void allocate(DevBlock &B) {
+    const auto &p = setup_.params;
+    for (int f = 0; f < F_N_FIELDS; ++f) {
+      int nc = 1;
+      const Lay &L = layout_of(B, f, nc);
+      bool need = nc > 0;
+      if (f == F_RHO_D || f == F_GAMMA || f == F_CP) need = need && (C::ns > 0 || f != F_RHO_D);
+      if (f == F_CHEM_JAC) need = C::mix == 2 && p.chem_src_method != 0;
+      if (f == F_TURB_SRC_JAC || f == F_MUT || f == F_TURB_COND || f == F_WALL_DIST) need = C::turb;
+      if (f == F_DQ0 || f == F_DQK) need = p.implicit_method == 1;
+      double *&ptr = field_pointer(B, f);
+      ptr = nullptr;
+      if (!need) continue;
+      const size_t bytes = sizeof(double) * static_cast<size_t>(L.size) * nc;
+      void *q = nullptr;
+      cuda_check(cudaMalloc(&q, bytes), "cudaMalloc field");
+      cuda_check(cudaMemset(q, 0, bytes), "memset field");
+      allocations_.push_back(q);
+      ptr = static_cast<double *>(q);
+    }
+    B.lu_piv = nullptr;
+    if (C::mix == 2 && p.chem_src_method == 1) {
+      void *q = nullptr;
+      const size_t bytes = static_cast<size_t>(B.Z.size) * C::ns;
+      cuda_check(cudaMalloc(&q, bytes), "cudaMalloc piv");
+      cuda_check(cudaMemset(q, 0, bytes), "memset piv");
+      allocations_.push_back(q);
+      B.lu_piv = static_cast<unsigned char *>(q);
+    }
+  }
+
+  double *field_ptr(int b, int f) {
+    if (b < 0 || b >= static_cast<int>(blocks_.size())) throw std::runtime_error("block index out of range");
+    double *p = field_pointer(blocks_[b], f);
+    if (!p) throw std::runtime_error("field " + std::to_string(f) + " is not allocated in this configuration");
+    return p;
+  }
+
+  void check_count(int b, int f, int64_t count) const {
+    if (count != field_count(b, f))
+      throw std::runtime_error("field " + std::to_string(f) + " holds " + std::to_string(field_count(b, f)) +
+                               " values, caller passed " + std::to_string(count));
+  }
+
+  Tiles make_tiles(int halo) const {
+    Tiles t{};
+    t.nblk = static_cast<int>(blocks_.size());
+    t.halo = halo;
+    int acc = 0;
+    for (int b = 0; b < t.nblk; ++b) {
+      const DevBlock &B = blocks_[b];
+      t.begin[b] = acc;
+      t.ntx[b] = (B.mx + 2 * halo + kTX - 1) / kTX;
+      t.nty[b] = (B.my + 2 * halo + kTY - 1) / kTY;
+      const int ntz = (B.mz + 2 * halo + kTZ - 1) / kTZ;
+      acc += t.ntx[b] * t.nty[b] * ntz;
+    }
+    t.begin[t.nblk] = acc;
+    return t;
+  }
+
+  static dim3 grid(const Tiles &t) { return dim3(static_cast<unsigned>(t.begin[t.nblk])); }
+  static dim3 block3() { return dim3(kTX, kTY, kTZ); }
+
+  void launch_residual() {
+    k_source<C><<<grid(tiles0_), block3(), source_smem_, stream_>>>(d_blocks_, tiles0_);
+    mark("source");
+    k_flux<C><<<grid(tiles0_), block3(), flux_smem_, stream_>>>(d_blocks_, tiles0_);
+    mark("flux");
+  }
+
+  // returns the dq buffer holding the final increment (0 dq, 1 dq0, 2 dqk)
+  int launch_implicit() {
+    const auto &p = setup_.params;
+    if (p.implicit_method == 1) {
+      k_dq0<C><<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_);
+      mark("dq0");
+      int in = 1;
+      for (int s = 0; s < p.dplur_inner_step; ++s) {
+        const int out = (s % 2 == 0) ? 2 : 0;
+        k_sweep<C><<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_, in, out);
+        mark("dplur_sweep");
+        in = out;
+      }
+      final_dq_ = in;
+    } else {
+      if ((C::mix == 2 && p.chem_src_method != 0) || (C::turb && p.turb_implicit == 1))
+        k_point_implicit<C><<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_);
+        mark("point_implicit");
+      final_dq_ = 0;
+    }
+    return final_dq_;
+  }
+
+  void launch_update() {
+    cuda_check(cudaMemsetAsync(d_bad_, 0, sizeof(unsigned int), stream_), "memset bad");
+    mark("memset");
+    k_update<C><<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_, final_dq_, d_bad_);
+    mark("update");
+    k_limit<C><<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_, d_bad_);
+    mark("limit_flow");
+  }
+
+  void launch_bcs() {
+    for (int q = 0; q < static_cast<int>(setup_.bcs.size()); ++q) {
+      const HostBc &f = setup_.bcs[q];
+      const int np = (f.end[0] - f.start[0] + 1) * (f.end[1] - f.start[1] + 1) * (f.end[2] - f.start[2] + 1);
+      if (np <= 0) continue;
+      k_bc<C><<<(np + 127) / 128, 128, 0, stream_>>>(d_blocks_, d_bcs_, q);
+      mark("boundary");
+    }
+  }
+
+  void launch_inner() {
+    for (int q = 0; q < static_cast<int>(setup_.inner.size()); ++q) {
+      const HostInner &f = setup_.inner[q];
+      const int np = f.n_point[0] * f.n_point[1] * f.n_point[2];
+      if (np <= 0) continue;
+      k_inner<C><<<(np + 127) / 128, 128, 0, stream_>>>(d_blocks_, d_inner_, q);
+      mark("inner_face");
+    }
+  }
+
+  void launch_kcopy() {
+    for (int b = 0; b < static_cast<int>(blocks_.size()); ++b) {
+      const DevBlock &B = blocks_[b];
+      const int np = (B.mx + 2 * B.ngg) * (B.my + 2 * B.ngg);
+      k_kcopy<C><<<(np + 127) / 128, 128, 0, stream_>>>(d_blocks_, b);
+      mark("k_copy");
+    }
+  }
+
+  void launch_exchange() {
+    launch_inner();
+    if (setup_.params.dim == 2) launch_kcopy();
+    k_props<C><<<grid(tiles1_), block3(), 0, stream_>>>(d_blocks_, tiles1_);
+    mark("properties");
+  }
+
+  void enqueue_step(bool store_last, bool residual) {
+    if (store_last) {
+      k_store_last<<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_);
+      mark("store_last");
+    }
+    launch_residual();
+    launch_implicit();
+    launch_update();
+    launch_bcs();
+    launch_exchange();
+    if (residual) {
+      k_res_partial<<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_, d_partial_);
+      k_res_final<<<1, 128, 0, stream_>>>(d_partial_, tiles0_.begin[tiles0_.nblk], d_res_);
+      cuda_check(cudaMemcpyAsync(h_res_, d_res_, sizeof(double) * 4, cudaMemcpyDeviceToHost, stream_), "res copy");
+    }
+    cuda_check(cudaGetLastError(), "step launch");
+  }
+
+  void mark(const char *name) {
+    if (!marks_) return;
+    cudaEvent_t e;
+    cuda_check(cudaEventCreate(&e), "event");
+    cuda_check(cudaEventRecord(e, stream_), "event");
+    marks_->emplace_back(name, e);
+  }
+
+  std::vector<std::pair<const char *, cudaEvent_t>> *marks_ = nullptr;
+  EngineSetup setup_;
+  cudaStream_t stream_{};
+  std::vector<DevBlock> blocks_;
+  DevBlock *d_blocks_ = nullptr;
+  DevBc *d_bcs_ = nullptr;
+  DevInner *d_inner_ = nullptr;
+  double *d_partial_ = nullptr, *d_res_ = nullptr, *h_res_ = nullptr, *d_wall_ = nullptr;
+  unsigned int *d_bad_ = nullptr;
+  std::vector<void *> allocations_;
+  Tiles tiles0_, tiles1_, tilesg_;
+  size_t source_smem_ = 0, flux_smem_ = 0;
+  int final_dq_ = 0;
+  cudaGraphExec_t graphs_[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev0_{}, ev1_{};
+  double last_ms_ = 0;
+};
+
+}  // namespace ostc

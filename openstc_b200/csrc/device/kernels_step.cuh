@@ -1,0 +1,1064 @@
+// Kernels of one pseudo-time step, instantiated per model configuration.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace ostc {
+
+constexpr int kTX = 32, kTY = 4, kTZ = 1;  // per-cell tile (threads)
+constexpr int kCta = kTX * kTY * kTZ;
+
+// ---------------------------------------------------------------- source
+// compute_source (src/SourceTerm.cuh:11-40) fused with the reset of dq:
+// writes every dq component of an interior cell (zero + source).
+template <class C>
+__global__ void __launch_bounds__(kCta) k_source(const DevBlock *__restrict__ blks, Tiles T) {
+  constexpr int NS = C::ns, NV = C::nv;
+  extern __shared__ double sq[];  // q1, q2: 2 * n_reac * kCta doubles
+  int b, i, j, k;
+  if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
+  const DevBlock &B = blks[b];
+  const int64_t n = B.G.at(i, j, k), nd = B.D.at(i, j, k), nz = B.Z.at(i, j, k);
+  const int64_t sz = B.G.size, szd = B.D.size, sz0 = B.Z.size;
+  double dq[NV];
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] = 0;
+  if constexpr (C::turb) {
+    double sk, sw, mut, jk, jw;
+    sst_source<C>(B, n, sk, sw, mut, jk, jw);
+    B.mut[n] = mut;
+    dq[NS + 5] = sk;
+    dq[NS + 6] = sw;
+    if (cP.turb_implicit == 1) {
+      B.turb_src_jac[nz] = jk;
+      B.turb_src_jac[sz0 + nz] = jw;
+    }
+    if constexpr (C::mix != 0) {
+      B.turb_cond[n] = mut * ld(B.cp + n) / cP.Prt;
+    } else {
+      constexpr double cp = kDGammaAir * kDR_u / kDMwAir / (kDGammaAir - 1);
+      B.turb_cond[n] = mut * cp / cP.Prt;
+    }
+  }
+  if constexpr (C::mix == 2) {
+    const int tid = threadIdx.x + kTX * (threadIdx.y + kTY * threadIdx.z);
+    double *q1 = sq + tid, *q2 = sq + cP.nr * kCta + tid;
+    double Y[NS], omega[NS], omega_d[NS];
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) Y[l] = ld(B.sv + l * sz + n);
+    const double density = ld(B.bv + n), t = ld(B.bv + 5 * sz + n);
+    chemistry<NS>(density, t, Y, omega, omega_d, q1, q2, kCta);
+    const double jac = ld(B.jac + n);
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) dq[l + 5] = 0.0 + jac * omega[l];
+    const int method = cP.chem_src_method;
+    if (method == 1) {
+      // compute_chem_src_jacobian, src/FiniteRateChem.cu:173-194
+      const int nr = cP.nr;
+      OSTC_UNROLL for (int m = 0; m < NS; ++m) {
+        OSTC_UNROLL for (int q = 0; q < NS; ++q) {
+          double zz = 0;
+          if (Y[q] > 1e-25) {
+            for (int r = 0; r < nr; ++r) {
+              const int dn = cP.sb[r * NS + m] - cP.sf[r * NS + m];
+              if (dn == 0) continue;  // adds an exact zero in the reference
+              zz += dn * (cP.sf[r * NS + q] * q1[r * kCta] - cP.sb[r * NS + q] * q2[r * kCta]);
+            }
+            zz /= density * Y[q];
+          }
+          B.chem_jac[(m * NS + q) * sz0 + nz] = cP.mw[m] * zz * 1e+3;
+        }
+      }
+    } else if (method == 2) {
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) {
+        double v = 0;
+        if (Y[l] > 1e-25) v = -omega_d[l] / (Y[l] * density);
+        B.chem_jac[l * sz0 + nz] = v;
+      }
+    }
+  }
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq[l * szd + nd] = dq[l];
+}
+
+// ---------------------------------------------------------------- fluxes
+// Inviscid (AUSM+/MUSCL) then viscous (central) flux differences in the
+// reference's accumulation order, plus local_time_step
+// (src/TimeAdvanceFunc.cuh:21-71).
+template <class C>
+__global__ void __launch_bounds__(kCta) k_flux(const DevBlock *__restrict__ blks, Tiles T) {
+  constexpr int NV = C::nv;
+  extern __shared__ double sf[];
+  int b, i, j, k;
+  if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
+  const DevBlock &B = blks[b];
+  const int tid = threadIdx.x + kTX * (threadIdx.y + kTY * threadIdx.z);
+  double *fm = sf + tid;  // stride kCta
+  const int64_t n = B.G.at(i, j, k), nd = B.D.at(i, j, k), szd = B.D.size;
+  const int64_t sx = B.G.sx, sxy = B.G.sxy;
+  const bool three_d = B.mz > 1;
+  double dq[NV];
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] = B.dq[l * szd + nd];
+  double fp[NV];
+  // inviscid, i / j / k
+  {
+    double t[NV];
+    inviscid_face<C, 0>(B, n - 1, t);
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) fm[l * kCta] = t[l];
+  }
+  inviscid_face<C, 0>(B, n, fp);
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] -= fp[l] - fm[l * kCta];
+  {
+    double t[NV];
+    inviscid_face<C, 1>(B, n - sx, t);
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) fm[l * kCta] = t[l];
+  }
+  inviscid_face<C, 1>(B, n, fp);
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] -= fp[l] - fm[l * kCta];
+  if (three_d) {
+    {
+      double t[NV];
+      inviscid_face<C, 2>(B, n - sxy, t);
+      OSTC_UNROLL for (int l = 0; l < NV; ++l) fm[l * kCta] = t[l];
+    }
+    inviscid_face<C, 2>(B, n, fp);
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] -= fp[l] - fm[l * kCta];
+  }
+  if (cP.viscous_order != 0) {
+    {
+      double t[NV];
+      viscous_face<C, 0>(B, n - 1, t);
+      OSTC_UNROLL for (int l = 0; l < NV; ++l) fm[l * kCta] = t[l];
+    }
+    viscous_face<C, 0>(B, n, fp);
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] += fp[l] - fm[l * kCta];
+    {
+      double t[NV];
+      viscous_face<C, 1>(B, n - sx, t);
+      OSTC_UNROLL for (int l = 0; l < NV; ++l) fm[l * kCta] = t[l];
+    }
+    viscous_face<C, 1>(B, n, fp);
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] += fp[l] - fm[l * kCta];
+    if (three_d) {
+      {
+        double t[NV];
+        viscous_face<C, 2>(B, n - sxy, t);
+        OSTC_UNROLL for (int l = 0; l < NV; ++l) fm[l * kCta] = t[l];
+      }
+      viscous_face<C, 2>(B, n, fp);
+      OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] += fp[l] - fm[l * kCta];
+    }
+  }
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq[l * szd + nd] = dq[l];
+
+  // local time step
+  const int64_t sz = B.G.size;
+  const double *m = B.metric;
+  const double m11 = ld(m + n), m12 = ld(m + sz + n), m13 = ld(m + 2 * sz + n);
+  const double m21 = ld(m + 3 * sz + n), m22 = ld(m + 4 * sz + n), m23 = ld(m + 5 * sz + n);
+  const double m31 = ld(m + 6 * sz + n), m32 = ld(m + 7 * sz + n), m33 = ld(m + 8 * sz + n);
+  const double grad_xi = sqrt(m11 * m11 + m12 * m12 + m13 * m13);
+  const double grad_eta = sqrt(m21 * m21 + m22 * m22 + m23 * m23);
+  const double grad_zeta = sqrt(m31 * m31 + m32 * m32 + m33 * m33);
+  const double u = ld(B.bv + sz + n), v = ld(B.bv + 2 * sz + n), w = ld(B.bv + 3 * sz + n);
+  const double U = u * m11 + v * m12 + w * m13;
+  const double V = u * m21 + v * m22 + w * m23;
+  const double W = u * m31 + v * m32 + w * m33;
+  const double a = ld(B.acoustic + n);
+  const double s0 = fabs(U) + a * grad_xi, s1 = fabs(V) + a * grad_eta;
+  double s2 = 0;
+  if (three_d) s2 = fabs(W) + a * grad_zeta;
+  B.inv_spec[nd] = s0;
+  B.inv_spec[szd + nd] = s1;
+  B.inv_spec[2 * szd + nd] = s2;
+  const double sri = s0 + s1 + s2;
+  double gamma = kDGammaAir;
+  if constexpr (C::mix != 0) gamma = ld(B.gamma + n);
+  const double coeff_1 = fmax(gamma, 4.0 / 3.0) / ld(B.bv + n);
+  double coeff_2 = ld(B.mul + n) / cP.Pr;
+  if constexpr (C::turb) coeff_2 += ld(B.mut + n) / cP.Prt;
+  double srv = grad_xi * grad_xi + grad_eta * grad_eta;
+  if (three_d) srv += grad_zeta * grad_zeta;
+  srv *= coeff_1 * coeff_2;
+  B.visc_spec[nd] = srv;
+  B.dt_local[B.Z.at(i, j, k)] = cP.cfl / (sri + srv);
+}
+
+// ---------------------------------------------------------------- implicit
+// Column-pivoted Doolittle LU of the ns x ns point-implicit matrix,
+// src/FiniteRateChem.cu:286-342.  Factor and permutation are stored so that
+// the DPLUR sweeps reuse them: the reference re-factors the identical matrix
+// in every sweep, which yields the same factor bit for bit.
+template <int NS>
+__device__ __forceinline__ void lu_factor(double *lhs, int *ipiv) {
+  OSTC_UNROLL for (int n = 0; n < NS; ++n) {
+    int ik = n;
+    double amax = 0;  // |lhs[ik][n]|: entries of column n above row m are final
+    OSTC_UNROLL for (int m = n; m < NS; ++m) {
+      OSTC_UNROLL for (int t = 0; t < n; ++t) lhs[m * NS + n] -= lhs[m * NS + t] * lhs[t * NS + n];
+      const double a = fabs(lhs[m * NS + n]);
+      if (m == n) {
+        amax = a;
+      } else if (a > amax) {
+        ik = m;
+        amax = a;
+      }
+    }
+    ipiv[n] = ik;
+    if (ik != n) {
+      OSTC_UNROLL for (int t = 0; t < NS; ++t) {
+        // swap rows n and ik; ik is data dependent, so select row by row
+        double rowk = lhs[n * NS + t];
+        double other = 0;
+        OSTC_UNROLL for (int q = n + 1; q < NS; ++q)
+          if (q == ik) other = lhs[q * NS + t];
+        OSTC_UNROLL for (int q = n + 1; q < NS; ++q)
+          if (q == ik) lhs[q * NS + t] = rowk;
+        lhs[n * NS + t] = other;
+      }
+    }
+    OSTC_UNROLL for (int p = n + 1; p < NS; ++p)
+      OSTC_UNROLL for (int t = 0; t < n; ++t) lhs[n * NS + p] -= lhs[n * NS + t] * lhs[t * NS + p];
+    OSTC_UNROLL for (int m = n + 1; m < NS; ++m) lhs[m * NS + n] /= lhs[n * NS + n];
+  }
+}
+
+template <int NS>
+__device__ __forceinline__ void lu_solve(const double *lhs, const int *ipiv, double *rhs) {
+  OSTC_UNROLL for (int m = 0; m < NS; ++m) {
+    const int t = ipiv[m];
+    if (t != m) {
+      double a = rhs[m], other = 0;
+      OSTC_UNROLL for (int q = m + 1; q < NS; ++q)
+        if (q == t) other = rhs[q];
+      OSTC_UNROLL for (int q = m + 1; q < NS; ++q)
+        if (q == t) rhs[q] = a;
+      rhs[m] = other;
+    }
+  }
+  OSTC_UNROLL for (int m = 1; m < NS; ++m)
+    OSTC_UNROLL for (int t = 0; t < m; ++t) rhs[m] -= lhs[m * NS + t] * rhs[t];
+  rhs[NS - 1] /= lhs[NS * NS - 1];
+  OSTC_UNROLL for (int m = NS - 2; m >= 0; --m) {
+    OSTC_UNROLL for (int t = m + 1; t < NS; ++t) rhs[m] -= lhs[m * NS + t] * rhs[t];
+    rhs[m] /= lhs[m * NS + m];
+  }
+}
+
+// Explicit-mode point-implicit treatment: EPI / DA and the SST diagonal,
+// src/ImplicitTreatmentHPP.cuh:14-54, src/FiniteRateChem.cu:211-234, 400-412,
+// src/SST.cu:180-194.
+template <class C>
+__global__ void __launch_bounds__(kCta) k_point_implicit(const DevBlock *__restrict__ blks, Tiles T) {
+  constexpr int NS = C::ns;
+  int b, i, j, k;
+  if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
+  const DevBlock &B = blks[b];
+  const int64_t nd = B.D.at(i, j, k), nz = B.Z.at(i, j, k), szd = B.D.size, sz0 = B.Z.size;
+  const double dt = B.dt_local[nz];
+  if constexpr (C::mix == 2) {
+    if (cP.chem_src_method == 1) {
+      double lhs[NS * NS];
+      int piv[NS];
+      OSTC_UNROLL for (int m = 0; m < NS; ++m)
+        OSTC_UNROLL for (int q = 0; q < NS; ++q) {
+          const double J = B.chem_jac[(m * NS + q) * sz0 + nz];
+          lhs[m * NS + q] = (m == q) ? 1.0 - dt * J : -dt * J;
+        }
+      lu_factor<NS>(lhs, piv);
+      double rhs[NS];
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) rhs[l] = B.dq[(5 + l) * szd + nd];
+      lu_solve<NS>(lhs, piv, rhs);
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) B.dq[(5 + l) * szd + nd] = rhs[l];
+    } else if (cP.chem_src_method == 2) {
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) B.dq[(5 + l) * szd + nd] /= 1 - dt * B.chem_jac[l * sz0 + nz];
+    }
+  }
+  if constexpr (C::turb) {
+    if (cP.turb_implicit == 1) {
+      B.dq[(NS + 5) * szd + nd] /= 1 - dt * B.turb_src_jac[nz];
+      B.dq[(NS + 6) * szd + nd] /= 1 - dt * B.turb_src_jac[sz0 + nz];
+    }
+  }
+}
+
+// compute_DQ_0, src/DPLURHPP.cuh:13-76.  Writes dq0; with EPI the factored
+// matrix replaces the Jacobian in chem_jac and the pivots go to lu_piv.
+template <class C>
+__global__ void __launch_bounds__(kCta) k_dq0(const DevBlock *__restrict__ blks, Tiles T) {
+  constexpr int NS = C::ns, NV = C::nv;
+  int b, i, j, k;
+  if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
+  const DevBlock &B = blks[b];
+  const int64_t nd = B.D.at(i, j, k), nz = B.Z.at(i, j, k), szd = B.D.size, sz0 = B.Z.size;
+  const double dt = B.dt_local[nz];
+  const double diag = 1 + dt * (B.inv_spec[nd] + B.inv_spec[szd + nd] + B.inv_spec[2 * szd + nd]);
+  double dq[NV];
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] = B.dq[l * szd + nd];
+  if constexpr (C::mix != 2) {
+    OSTC_UNROLL for (int l = 0; l < 5 + NS; ++l) dq[l] /= diag;
+  } else {
+    OSTC_UNROLL for (int l = 0; l < 5; ++l) dq[l] /= diag;
+    const int method = cP.chem_src_method;
+    if (method == 1) {
+      double lhs[NS * NS];
+      int piv[NS];
+      OSTC_UNROLL for (int m = 0; m < NS; ++m)
+        OSTC_UNROLL for (int q = 0; q < NS; ++q) {
+          const double J = B.chem_jac[(m * NS + q) * sz0 + nz];
+          lhs[m * NS + q] = (m == q) ? diag - dt * J : -dt * J;
+        }
+      lu_factor<NS>(lhs, piv);
+      lu_solve<NS>(lhs, piv, dq + 5);
+      OSTC_UNROLL for (int q = 0; q < NS * NS; ++q) B.chem_jac[q * sz0 + nz] = lhs[q];
+      OSTC_UNROLL for (int q = 0; q < NS; ++q) B.lu_piv[q * sz0 + nz] = static_cast<unsigned char>(piv[q]);
+    } else if (method == 2) {
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) dq[5 + l] /= diag - dt * B.chem_jac[l * sz0 + nz];
+    } else {
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) dq[5 + l] /= diag;
+    }
+  }
+  if constexpr (C::turb) {
+    if (cP.turb_implicit == 1) {
+      dq[NS + 5] /= diag - dt * B.turb_src_jac[nz];
+      dq[NS + 6] /= diag - dt * B.turb_src_jac[sz0 + nz];
+    } else {
+      dq[NS + 5] /= diag;
+      dq[NS + 6] /= diag;
+    }
+  }
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq0[l * szd + nd] = dq[l];
+}
+
+// compute_jacobian_times_dq, src/DPLURHPP.cuh:78-125, accumulated into tot
+// with weight +-0.5 (sign < 0 subtracts).
+template <class C, int D>
+__device__ __forceinline__ void add_jac_dq(const DevBlock &B, const double *__restrict__ dqin, int64_t n,
+                                           int64_t nd, double pm_sr, bool subtract, double *tot) {
+  constexpr int NS = C::ns, NV = C::nv;
+  const int64_t sz = B.G.size, szd = B.D.size;
+  const double *mr = B.metric + 3 * D * sz;
+  const double xi_x = ld(mr + n), xi_y = ld(mr + sz + n), xi_z = ld(mr + 2 * sz + n);
+  const double u = ld(B.bv + sz + n), v = ld(B.bv + 2 * sz + n), w = ld(B.bv + 3 * sz + n);
+  const double U = xi_x * u + xi_y * v + xi_z * w;
+  const double lmd1 = U + pm_sr;
+  const double vel = ld(B.vel + n);
+  const double e = 0.5 * vel * vel;
+  double gamma = kDGammaAir, b3 = 0, b4 = 0, h = 0;
+  double d[NV];
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) d[l] = ld(dqin + l * szd + nd);
+  if constexpr (C::mix != 0) {
+    double hk[NS];
+    const double t = ld(B.bv + 5 * sz + n);
+    enthalpy<NS>(t, hk);
+    gamma = ld(B.gamma + n);
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) {
+      b3 += kDR_u * t / cP.mw[l] * d[5 + l];
+      b4 += hk[l] * d[5 + l];
+      h += ld(B.sv + l * sz + n) * hk[l];
+    }
+    b3 *= gamma;
+    b4 *= gamma - 1;
+    h += e;
+  } else {
+    h = gamma / (gamma - 1) * ld(B.bv + 4 * sz + n) / ld(B.bv + n) + e;
+  }
+  const double b1 = xi_x * d[1] + xi_y * d[2] + xi_z * d[3] - U * d[0];
+  const double b2 = (gamma - 1) * (e * d[0] - u * d[1] - v * d[2] - w * d[3] + d[4]);
+  double o[NV];
+  o[0] = b1 + lmd1 * d[0];
+  o[1] = u * b1 + xi_x * b2 + lmd1 * d[1] + xi_x * (b3 - b4);
+  o[2] = v * b1 + xi_y * b2 + lmd1 * d[2] + xi_y * (b3 - b4);
+  o[3] = w * b1 + xi_z * b2 + lmd1 * d[3] + xi_z * (b3 - b4);
+  o[4] = h * b1 + U * b2 + lmd1 * d[4] + U * (b3 - b4);
+  OSTC_UNROLL for (int l = 0; l < C::nsc; ++l) o[5 + l] = lmd1 * d[5 + l] + ld(B.sv + l * sz + n) * b1;
+  if (subtract) {
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) tot[l] -= 0.5 * o[l];
+  } else {
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) tot[l] += 0.5 * o[l];
+  }
+}
+
+// DPLUR_inner_iteration, src/DPLURHPP.cuh:127-249: dqout = dq0 + dt*sum/diag
+// with the neighbours' A(+-)*dqin; the point-implicit blocks reuse the LU.
+template <class C>
+__global__ void __launch_bounds__(kCta) k_sweep(const DevBlock *__restrict__ blks, Tiles T, int in_sel, int out_sel) {
+  constexpr int NS = C::ns, NV = C::nv;
+  int b, i, j, k;
+  if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
+  const DevBlock &B = blks[b];
+  const double *dqin = in_sel == 0 ? B.dq : (in_sel == 1 ? B.dq0 : B.dqk);
+  double *dqout = out_sel == 0 ? B.dq : B.dqk;
+  const int64_t szd = B.D.size, sz0 = B.Z.size;
+  const int64_t n = B.G.at(i, j, k), nd = B.D.at(i, j, k), nz = B.Z.at(i, j, k);
+  const int64_t sx = B.G.sx, sxy = B.G.sxy, dsx = B.D.sx, dsxy = B.D.sxy;
+  double tot[NV];
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) tot[l] = 0;
+  const double *isr = B.inv_spec;
+  if (i > 0) add_jac_dq<C, 0>(B, dqin, n - 1, nd - 1, isr[nd - 1], false, tot);
+  if (j > 0) add_jac_dq<C, 1>(B, dqin, n - sx, nd - dsx, isr[szd + nd - dsx], false, tot);
+  if (k > 0) add_jac_dq<C, 2>(B, dqin, n - sxy, nd - dsxy, isr[2 * szd + nd - dsxy], false, tot);
+  if (i != B.mx - 1) add_jac_dq<C, 0>(B, dqin, n + 1, nd + 1, -isr[nd + 1], true, tot);
+  if (j != B.my - 1) add_jac_dq<C, 1>(B, dqin, n + sx, nd + dsx, -isr[szd + nd + dsx], true, tot);
+  if (k != B.mz - 1) add_jac_dq<C, 2>(B, dqin, n + sxy, nd + dsxy, -isr[2 * szd + nd + dsxy], true, tot);
+  const double dt = B.dt_local[nz];
+  const double diag = 1 + dt * (isr[nd] + isr[szd + nd] + isr[2 * szd + nd]);
+  double out[NV];
+  if constexpr (C::mix != 2) {
+    OSTC_UNROLL for (int l = 0; l < 5 + NS; ++l) out[l] = B.dq0[l * szd + nd] + dt * tot[l] / diag;
+  } else {
+    OSTC_UNROLL for (int l = 0; l < 5; ++l) out[l] = B.dq0[l * szd + nd] + dt * tot[l] / diag;
+    const int method = cP.chem_src_method;
+    if (method == 1) {
+      double lhs[NS * NS];
+      int piv[NS];
+      OSTC_UNROLL for (int q = 0; q < NS * NS; ++q) lhs[q] = B.chem_jac[q * sz0 + nz];
+      OSTC_UNROLL for (int q = 0; q < NS; ++q) piv[q] = B.lu_piv[q * sz0 + nz];
+      double rhs[NS];
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) rhs[l] = tot[5 + l] * dt;
+      lu_solve<NS>(lhs, piv, rhs);
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) out[5 + l] = B.dq0[(5 + l) * szd + nd] + rhs[l];
+    } else if (method == 2) {
+      OSTC_UNROLL for (int l = 0; l < NS; ++l)
+        out[5 + l] = B.dq0[(5 + l) * szd + nd] + dt * tot[5 + l] / (diag - dt * B.chem_jac[l * sz0 + nz]);
+    } else {
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) out[5 + l] = B.dq0[(5 + l) * szd + nd] + dt * tot[5 + l] / diag;
+    }
+  }
+  if constexpr (C::turb) {
+    if (cP.turb_implicit == 1) {
+      out[NS + 5] = B.dq0[(NS + 5) * szd + nd] + dt * tot[5 + NS] / (diag - dt * B.turb_src_jac[nz]);
+      out[NS + 6] = B.dq0[(NS + 6) * szd + nd] + dt * tot[6 + NS] / (diag - dt * B.turb_src_jac[sz0 + nz]);
+    } else {
+      out[NS + 5] = B.dq0[(NS + 5) * szd + nd] + dt * tot[5 + NS] / diag;
+      out[NS + 6] = B.dq0[(NS + 6) * szd + nd] + dt * tot[6 + NS] / diag;
+    }
+  }
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) dqout[l * szd + nd] = out[l];
+}
+
+// ---------------------------------------------------------------- update
+// compute_temperature, src/FieldOperation.cu:3-40
+template <int NS>
+__device__ __forceinline__ void newton_temperature(const double *Y, double rho, double e, double &t, double &p) {
+  double mw = 0;
+  OSTC_UNROLL for (int l = 0; l < NS; ++l) mw += Y[l] / cP.mw[l];
+  mw = 1 / mw;
+  const double gas_const = kDR_u / mw;
+  double err = 1;
+  int iter = 0;
+  while (err > 1e-3 && iter++ < 1000) {
+    double hi[NS], cpi[NS];
+    enthalpy_cp<NS>(t, hi, cpi);
+    double cp_tot = 0, h = 0;
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) {
+      cp_tot += cpi[l] * Y[l];
+      h += hi[l] * Y[l];
+    }
+    const double e_t = h - gas_const * t;
+    const double cv = cp_tot - gas_const;
+    const double t1 = t - (e_t - e) / cv;
+    err = fabs(1 - t1 / t);
+    t = t1;
+  }
+  p = rho * t * gas_const;
+}
+
+// Primitive recovery from Q at one point (update_bv_1_point,
+// src/FieldOperation.cuh:185-215); cv must already hold the new Q.
+template <class C>
+__device__ __forceinline__ void primitives_from_q(const DevBlock &B, int64_t n) {
+  constexpr int NS = C::ns;
+  const int64_t sz = B.G.size;
+  const double rho = B.cv[n];
+  B.bv[n] = rho;
+  const double rinv = 1.0 / rho;
+  const double u = B.cv[sz + n] * rinv, v = B.cv[2 * sz + n] * rinv, w = B.cv[3 * sz + n] * rinv;
+  B.bv[sz + n] = u;
+  B.bv[2 * sz + n] = v;
+  B.bv[3 * sz + n] = w;
+  const double vel2 = u * u + v * v + w * w;
+  if constexpr (C::mix != 0 || C::turb) {
+    OSTC_UNROLL for (int l = 0; l < C::nsc; ++l) B.sv[l * sz + n] = B.cv[(5 + l) * sz + n] * rinv;
+  }
+  if constexpr (C::mix != 0) {
+    double Y[NS];
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) Y[l] = B.sv[l * sz + n];
+    const double e = B.cv[4 * sz + n] / rho - 0.5 * (u * u + v * v + w * w);
+    double t = B.bv[5 * sz + n], p;
+    newton_temperature<NS>(Y, rho, e, t, p);
+    B.bv[5 * sz + n] = t;
+    B.bv[4 * sz + n] = p;
+  } else {
+    const double p = (kDGammaAir - 1) * (B.cv[4 * sz + n] - 0.5 * rho * vel2);
+    B.bv[4 * sz + n] = p;
+    B.bv[5 * sz + n] = p * kDMwAir * rinv / kDR_u;
+  }
+  B.vel[n] = sqrt(vel2);
+}
+
+__device__ __forceinline__ bool flow_unphysical(const double *v) {
+  bool bad = false;
+  OSTC_UNROLL for (int l = 0; l < 5; ++l) bad |= isnan(v[l]) || v[l] < cP.ll[l] || v[l] > cP.ul[l];
+  return bad;
+}
+
+// update_cv_and_bv, src/FieldOperation.cuh:139-183.  Counts unphysical cells
+// so that the limiter pass can skip the block when there are none.
+template <class C>
+__global__ void __launch_bounds__(kCta) k_update(const DevBlock *__restrict__ blks, Tiles T, int dq_sel,
+                                                 unsigned int *bad_count) {
+  constexpr int NV = C::nv;
+  int b, i, j, k;
+  if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
+  const DevBlock &B = blks[b];
+  const double *dq = dq_sel == 0 ? B.dq : (dq_sel == 1 ? B.dq0 : B.dqk);
+  const int64_t n = B.G.at(i, j, k), nd = B.D.at(i, j, k), nz = B.Z.at(i, j, k);
+  const int64_t sz = B.G.size, szd = B.D.size;
+  const double dt_div_jac = B.dt_local[nz] / B.jac[n];
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) B.cv[l * sz + n] += dq[l * szd + nd] * dt_div_jac;
+  if (B.mz == 1) B.cv[3 * sz + n] = 0;
+  primitives_from_q<C>(B, n);
+  double v[5];
+  OSTC_UNROLL for (int l = 0; l < 5; ++l) v[l] = B.bv[l * sz + n];
+  bool bad = flow_unphysical(v);
+  if constexpr (C::turb) {
+    const double tk = B.sv[C::ns * sz + n], tw = B.sv[(C::ns + 1) * sz + n];
+    bad |= isnan(tk) || isnan(tw) || tk < 0 || tw < 0;
+  }
+  if (bad) atomicAdd(bad_count, 1u);
+}
+
+// limit_flow, src/TimeAdvanceFunc.cu:34-224 (neighbour loop bounded by mz
+// in i as in the reference).  Does nothing unless k_update counted a bad cell.
+template <class C>
+__global__ void __launch_bounds__(kCta) k_limit(const DevBlock *__restrict__ blks, Tiles T,
+                                                const unsigned int *bad_count) {
+  constexpr int NS = C::ns, NSC = C::nsc;
+  if (*bad_count == 0) return;
+  int b, i, j, k;
+  if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
+  const DevBlock &B = blks[b];
+  const int64_t sz = B.G.size;
+  const int64_t n = B.G.at(i, j, k);
+  const int mx = B.mx, my = B.my, mz = B.mz;
+  (void)mx;
+  double var[5];
+  OSTC_UNROLL for (int l = 0; l < 5; ++l) var[l] = B.bv[l * sz + n];
+  if (flow_unphysical(var)) {
+    double up[5 + NSC];
+    OSTC_UNROLL for (int l = 0; l < 5 + NSC; ++l) up[l] = 0;
+    int kn = 0;
+    for (int ka = -1; ka < 2; ++ka) {
+      const int k1 = k + ka;
+      if (k1 < 0 || k1 >= mz) continue;
+      for (int ja = -1; ja < 2; ++ja) {
+        const int j1 = j + ja;
+        if (j1 < 0 || j1 >= my) continue;
+        for (int ia = -1; ia < 2; ++ia) {
+          const int i1 = i + ia;
+          if (i1 < 0 || i1 >= mz) continue;
+          const int64_t q = B.G.at(i1, j1, k1);
+          double nv5[5];
+          OSTC_UNROLL for (int l = 0; l < 5; ++l) nv5[l] = B.bv[l * sz + q];
+          if (flow_unphysical(nv5)) continue;
+          OSTC_UNROLL for (int l = 0; l < 5; ++l) up[l] += nv5[l];
+          OSTC_UNROLL for (int l = 0; l < NSC; ++l) up[l + 5] += B.sv[l * sz + q];
+          ++kn;
+        }
+      }
+    }
+    if (kn > 0) {
+      const double kinv = 1.0 / kn;
+      OSTC_UNROLL for (int l = 0; l < 5 + NSC; ++l) up[l] *= kinv;
+    } else {
+      OSTC_UNROLL for (int l = 0; l < 5; ++l) up[l] = fmin(fmax(var[l], cP.ll[l]), cP.ul[l]);
+      OSTC_UNROLL for (int l = 0; l < NSC; ++l) up[l + 5] = cP.sv_inf[l];
+    }
+    OSTC_UNROLL for (int l = 0; l < 5; ++l) B.bv[l * sz + n] = up[l];
+    B.cv[n] = up[0];
+    B.cv[sz + n] = up[0] * up[1];
+    B.cv[2 * sz + n] = up[0] * up[2];
+    B.cv[3 * sz + n] = up[0] * up[3];
+    double e = 0.5 * up[0] * (up[1] * up[1] + up[2] * up[2] + up[3] * up[3]);
+    OSTC_UNROLL for (int l = 0; l < NSC; ++l) {
+      B.sv[l * sz + n] = up[5 + l];
+      B.cv[(5 + l) * sz + n] = up[0] * up[5 + l];
+    }
+    if constexpr (NS > 0) {
+      double mw = 0;
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) mw += up[5 + l] / cP.mw[l];
+      mw = 1 / mw;
+      const double t = up[4] * mw / (up[0] * kDR_u);
+      B.bv[5 * sz + n] = t;
+      double h[NS];
+      enthalpy<NS>(t, h);
+      OSTC_UNROLL for (int l = 0; l < NS; l++) e += h[l] * B.cv[(5 + l) * sz + n];
+      e -= up[4];
+    } else {
+      B.bv[5 * sz + n] = up[4] * kDMwAir / (up[0] * kDR_u);
+      e += up[4] / (kDGammaAir - 1);
+    }
+    B.cv[4 * sz + n] = e;
+  }
+  if constexpr (C::turb) {
+    const double t0 = B.sv[NS * sz + n], t1 = B.sv[(NS + 1) * sz + n];
+    if (isnan(t0) || isnan(t1) || t0 < 0 || t1 < 0) {
+      double up0 = 0, up1 = 0;
+      int kn = 0;
+      for (int ka = -1; ka < 2; ++ka) {
+        const int k1 = k + ka;
+        if (k1 < 0 || k1 >= mz) continue;
+        for (int ja = -1; ja < 2; ++ja) {
+          const int j1 = j + ja;
+          if (j1 < 0 || j1 >= my) continue;
+          for (int ia = -1; ia < 2; ++ia) {
+            const int i1 = i + ia;
+            if (i1 < 0 || i1 >= mz) continue;
+            const int64_t q = B.G.at(i1, j1, k1);
+            const double a0 = B.sv[NS * sz + q], a1 = B.sv[(NS + 1) * sz + q];
+            if (isnan(a0) || isnan(a1) || a0 < 0 || a1 < 0) continue;
+            up0 += a0;
+            up1 += a1;
+            ++kn;
+          }
+        }
+      }
+      if (kn > 0) {
+        const double kinv = 1.0 / kn;
+        up0 *= kinv;
+        up1 *= kinv;
+      } else {
+        up0 = t0 < 0 ? cP.sv_inf[NS] : t0;
+        up1 = t1 < 0 ? cP.sv_inf[NS + 1] : t1;
+      }
+      B.sv[NS * sz + n] = up0;
+      B.sv[(NS + 1) * sz + n] = up1;
+      B.cv[(NS + 5) * sz + n] = B.cv[n] * up0;
+      B.cv[(NS + 6) * sz + n] = B.cv[n] * up1;
+    }
+  }
+}
+
+// update_physical_properties + compute_transport_property,
+// src/FieldOperation.cuh:75-109, src/Transport.cu:40-84 (interior + one
+// ghost layer: launched with halo 1).
+template <class C>
+__global__ void __launch_bounds__(kCta) k_props(const DevBlock *__restrict__ blks, Tiles T) {
+  constexpr int NS = C::ns;
+  int b, i, j, k;
+  if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
+  const DevBlock &B = blks[b];
+  const int64_t n = B.G.at(i, j, k), sz = B.G.size;
+  const double t = B.bv[5 * sz + n];
+  if constexpr (C::mix != 0) {
+    double cp[NS], Y[NS];
+    heat_capacity<NS>(t, cp);
+    double mw = 0, cp_tot = 0, cv = 0;
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) {
+      Y[l] = B.sv[l * sz + n];
+      mw += Y[l] / cP.mw[l];
+      cp_tot += Y[l] * cp[l];
+      cv += Y[l] * (cp[l] - kDR_u / cP.mw[l]);
+    }
+    mw = 1 / mw;
+    const double gamma = cp_tot / cv;
+    B.cp[n] = cp_tot;
+    B.gamma[n] = gamma;
+    const double a = sqrt(gamma * kDR_u * t / mw);
+    B.acoustic[n] = a;
+    double X[NS], vis[NS];
+    species_viscosity<NS>(t, mw, Y, X, vis);
+    double viscosity = 0, conductivity = 0;
+    OSTC_UNROLL for (int m = 0; m < NS; ++m) {
+      const double vt = wilke_sum<NS>(vis, X, m);
+      const double cond_temp = 1.065 * vt - 0.065 * X[m];
+      viscosity += vis[m] * X[m] / vt;
+      const double lambda = vis[m] * (cp[m] + 1.25 * kDR_u / cP.mw[m]);
+      conductivity += lambda * X[m] / cond_temp;
+    }
+    B.mul[n] = viscosity;
+    B.cond[n] = conductivity;
+    const double sc = cP.Sc;
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) {
+      double d;
+      if (fabs(X[l] - 1) < 1e-3) {
+        d = viscosity / sc;
+      } else {
+        d = (1 - Y[l]) * viscosity / ((1 - X[l]) * sc);
+      }
+      B.rho_d[l * sz + n] = d;
+    }
+    B.mach[n] = B.vel[n] / a;
+  } else {
+    constexpr double c_temp = kDGammaAir * kDR_u / kDMwAir;
+    constexpr double cp = kDGammaAir * kDR_u / kDMwAir / (kDGammaAir - 1);
+    const double a = sqrt(c_temp * t);
+    B.acoustic[n] = a;
+    const double mul = sutherland(t);
+    B.mul[n] = mul;
+    B.cond[n] = mul * cp / cP.Pr;
+    B.mach[n] = B.vel[n] / a;
+  }
+}
+
+// ---------------------------------------------------------------- boundaries
+// One boundary face (src/BoundCond.cuh:45-319).
+struct DevBc {
+  int block, type, face, direction;
+  int start[3], end[3];
+  double density, u, v, w, pressure, temperature, mut;
+  double sv[kMaxSpec + 2];
+  int isothermal;
+  double t_wall;
+};
+
+// compute_total_energy, src/FieldOperation.cuh:15-35
+template <class C>
+__device__ __forceinline__ void total_energy(const DevBlock &B, int64_t n) {
+  constexpr int NS = C::ns;
+  const int64_t sz = B.G.size;
+  const double u = B.bv[sz + n], v = B.bv[2 * sz + n], w = B.bv[3 * sz + n];
+  const double vel = u * u + v * v + w * w;
+  double e = 0.5 * B.bv[n] * vel;
+  if constexpr (C::mix != 0) {
+    double h[NS];
+    enthalpy<NS>(B.bv[5 * sz + n], h);
+    OSTC_UNROLL for (int l = 0; l < NS; l++) e += h[l] * B.cv[(5 + l) * sz + n];
+    e -= B.bv[4 * sz + n];
+  } else {
+    e += B.bv[4 * sz + n] / (kDGammaAir - 1);
+  }
+  B.cv[4 * sz + n] = e;
+  B.vel[n] = sqrt(vel);
+}
+
+template <class C>
+__global__ void k_bc(const DevBlock *__restrict__ blks, const DevBc *__restrict__ bcs, int face) {
+  constexpr int NS = C::ns, NSC = C::nsc;
+  const DevBc &f = bcs[face];
+  const int e0 = f.end[0] - f.start[0] + 1, e1 = f.end[1] - f.start[1] + 1, e2 = f.end[2] - f.start[2] + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= e0 * e1 * e2) return;
+  const int i = f.start[0] + t % e0, j = f.start[1] + (t / e0) % e1, k = f.start[2] + t / (e0 * e1);
+  const DevBlock &B = blks[f.block];
+  const int64_t sz = B.G.size;
+  const int ngg = B.ngg;
+  int dir[3] = {0, 0, 0};
+  dir[f.face] = f.direction;
+  const int64_t step = dir[0] + dir[1] * B.G.sx + dir[2] * B.G.sxy;  // +1 layer outward
+  const int64_t n = B.G.at(i, j, k);
+  double *bv = B.bv, *sv = B.sv, *cv = B.cv;
+  if (f.type == 6) {  // apply_outflow
+    for (int g = 1; g <= ngg; ++g) {
+      const int64_t gn = n + g * step;
+      for (int l = 0; l < 6; ++l) bv[l * sz + gn] = bv[l * sz + n];
+      for (int l = 0; l < NSC; ++l) sv[l * sz + gn] = sv[l * sz + n];
+      if constexpr (C::turb) B.mut[gn] = B.mut[n];
+    }
+  } else if (f.type == 5) {  // apply_inflow
+    for (int g = 1; g <= ngg; ++g) {
+      const int64_t gn = n + g * step;
+      bv[gn] = f.density;
+      bv[sz + gn] = f.u;
+      bv[2 * sz + gn] = f.v;
+      bv[3 * sz + gn] = f.w;
+      bv[4 * sz + gn] = f.pressure;
+      bv[5 * sz + gn] = f.temperature;
+      for (int l = 0; l < NSC; ++l) sv[l * sz + gn] = f.sv[l];
+      if constexpr (C::turb) B.mut[gn] = f.mut;
+    }
+  } else if (f.type == 3) {  // apply_symmetry
+    const int64_t in = n - step;
+    const double *mr = B.metric + 3 * f.face * sz;
+    double k_x = mr[n], k_y = mr[sz + n], k_z = mr[2 * sz + n];
+    const double k_magnitude = sqrt(k_x * k_x + k_y * k_y + k_z * k_z);
+    k_x /= k_magnitude;
+    k_y /= k_magnitude;
+    k_z /= k_magnitude;
+    const double u1 = bv[sz + in], v1 = bv[2 * sz + in], w1 = bv[3 * sz + in];
+    double u_k = k_x * u1 + k_y * v1 + k_z * w1;
+    const double u_t = u1 - k_x * u_k, v_t = v1 - k_y * u_k, w_t = w1 - k_z * u_k;
+    bv[sz + n] = u_t;
+    bv[2 * sz + n] = v_t;
+    bv[3 * sz + n] = w_t;
+    B.vel[n] = sqrt(u_t * u_t + v_t * v_t + w_t * w_t);
+    bv[n] = bv[in];
+    bv[4 * sz + n] = bv[4 * sz + in];
+    bv[5 * sz + n] = bv[5 * sz + in];
+    for (int l = 0; l < NSC; ++l) sv[l * sz + n] = sv[l * sz + in];
+    const double rho = bv[n];
+    cv[n] = rho;
+    cv[sz + n] = rho * bv[sz + n];
+    cv[2 * sz + n] = rho * bv[2 * sz + n];
+    cv[3 * sz + n] = rho * bv[3 * sz + n];
+    cv[4 * sz + n] = cv[4 * sz + in] - 0.5 * bv[in] * (u1 * u1 + v1 * v1 + w1 * w1) +
+                     0.5 * rho * (u_t * u_t + v_t * v_t + w_t * w_t);
+    for (int l = 0; l < NSC; ++l) cv[(5 + l) * sz + n] = rho * sv[l * sz + n];
+    for (int g = 1; g <= ngg; ++g) {
+      const int64_t gn = n + g * step, ig = n - g * step;
+      bv[gn] = bv[ig];
+      const double u = bv[sz + ig], v = bv[2 * sz + ig], w = bv[3 * sz + ig];
+      u_k = k_x * u + k_y * v + k_z * w;
+      const double ug = u - 2 * u_k * k_x, vg = v - 2 * u_k * k_y, wg = w - 2 * u_k * k_z;
+      bv[sz + gn] = ug;
+      bv[2 * sz + gn] = vg;
+      bv[3 * sz + gn] = wg;
+      B.vel[gn] = sqrt(ug * ug + vg * vg + wg * wg);
+      bv[4 * sz + gn] = bv[4 * sz + ig];
+      bv[5 * sz + gn] = bv[5 * sz + ig];
+      for (int l = 0; l < NSC; ++l) sv[l * sz + gn] = sv[l * sz + ig];
+      if constexpr (C::turb) B.mut[gn] = B.mut[ig];
+    }
+  } else if (f.type == 2) {  // apply_wall
+    const int64_t in = n - step;
+    double t_wall = f.t_wall;
+    if (!f.isothermal) t_wall = bv[5 * sz + in];
+    const double p = bv[4 * sz + in];
+    double mw = kDMwAir;
+    if constexpr (C::mix != 0) {
+      mw = 0;
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) {
+        sv[l * sz + n] = sv[l * sz + in];
+        mw += sv[l * sz + n] / cP.mw[l];
+      }
+      mw = 1 / mw;
+    }
+    const double rho_wall = p * mw / (t_wall * kDR_u);
+    bv[n] = rho_wall;
+    bv[sz + n] = 0;
+    bv[2 * sz + n] = 0;
+    bv[3 * sz + n] = 0;
+    bv[4 * sz + n] = p;
+    bv[5 * sz + n] = t_wall;
+    cv[n] = rho_wall;
+    cv[sz + n] = 0;
+    cv[2 * sz + n] = 0;
+    cv[3 * sz + n] = 0;
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) cv[(l + 5) * sz + n] = sv[l * sz + n] * rho_wall;
+    total_energy<C>(B, n);
+    if constexpr (C::turb) {
+      double mu_wall;
+      if constexpr (C::mix != 0) {
+        double Y[NS];
+        OSTC_UNROLL for (int l = 0; l < NS; ++l) Y[l] = sv[l * sz + n];
+        mu_wall = mixture_viscosity<NS>(t_wall, mw, Y);
+      } else {
+        mu_wall = sutherland(t_wall);
+      }
+      const double dy = B.wall_dist[in];
+      sv[NS * sz + n] = 0;
+      cv[(NS + 5) * sz + n] = 0;
+      if (dy > 1e-25) {
+        sv[(NS + 1) * sz + n] = 60 * mu_wall / (rho_wall * sst::beta_1 * dy * dy);
+      } else {
+        sv[(NS + 1) * sz + n] = sv[(NS + 1) * sz + in];
+      }
+      cv[(NS + 6) * sz + n] = rho_wall * sv[(NS + 1) * sz + n];
+    }
+    for (int g = 1; g <= ngg; ++g) {
+      const int64_t ig = n - g * step, gn = n + g * step;
+      const double u_i = bv[sz + ig], v_i = bv[2 * sz + ig], w_i = bv[3 * sz + ig];
+      const double p_i = bv[4 * sz + ig], t_i = bv[5 * sz + ig];
+      double t_g = t_i;
+      if (f.isothermal) {
+        t_g = 2 * t_wall - t_i;
+        if (t_g <= 0.1 * t_wall) t_g = t_wall;
+      }
+      if constexpr (C::mix != 0) {
+        mw = 0;
+        OSTC_UNROLL for (int l = 0; l < NS; ++l) {
+          sv[l * sz + gn] = sv[l * sz + ig];
+          mw += sv[l * sz + gn] / cP.mw[l];
+        }
+        mw = 1 / mw;
+      }
+      const double rho_g = p_i * mw / (t_g * kDR_u);
+      bv[gn] = rho_g;
+      bv[sz + gn] = -u_i;
+      bv[2 * sz + gn] = -v_i;
+      bv[3 * sz + gn] = -w_i;
+      bv[4 * sz + gn] = p_i;
+      bv[5 * sz + gn] = t_g;
+      if constexpr (C::turb) {
+        sv[NS * sz + gn] = 0;
+        sv[(NS + 1) * sz + gn] = sv[(NS + 1) * sz + n];
+        B.mut[gn] = 0;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- block faces
+// inner_communication, src/DataCommunication.cuh:58-98: average Q on the
+// shared face and copy the neighbour's interior into the ghost layers.
+struct DevInner {
+  int block, target_block, face, direction;
+  int start[3], end[3], loop_dir[3], tstart[3], tloop_dir[3], src_tar[3], n_point[3];
+};
+
+template <class C>
+__global__ void k_inner(const DevBlock *__restrict__ blks, const DevInner *__restrict__ faces, int fi) {
+  const DevInner &f = faces[fi];
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int np = f.n_point[0] * f.n_point[1] * f.n_point[2];
+  if (t >= np) return;
+  const int nn[3] = {t % f.n_point[0], (t / f.n_point[0]) % f.n_point[1], t / (f.n_point[0] * f.n_point[1])};
+  int idx[3], it[3], d[3];
+  for (int q = 0; q < 3; ++q) {
+    d[q] = f.loop_dir[q] * nn[q];
+    idx[q] = f.start[q] + d[q];
+  }
+  for (int q = 0; q < 3; ++q) it[q] = f.tstart[q] + f.tloop_dir[q] * d[f.src_tar[q]];
+  const DevBlock &B = blks[f.block];
+  const DevBlock &Tb = blks[f.target_block];
+  const int64_t n = B.G.at(idx[0], idx[1], idx[2]), tn = Tb.G.at(it[0], it[1], it[2]);
+  const int64_t sz = B.G.size, tsz = Tb.G.size;
+  const int face_dir = f.direction > 0 ? f.start[f.face] : f.end[f.face];
+  if (idx[f.face] == face_dir) {
+    OSTC_UNROLL for (int l = 0; l < C::nv; ++l) {
+      const double ave = 0.5 * (Tb.cv[l * tsz + tn] + B.cv[l * sz + n]);
+      B.cv[l * sz + n] = ave;
+      Tb.cv[l * tsz + tn] = ave;
+    }
+    primitives_from_q<C>(B, n);
+  } else {
+    for (int l = 0; l < 6; ++l) B.bv[l * sz + n] = Tb.bv[l * tsz + tn];
+    OSTC_UNROLL for (int l = 0; l < C::nsc; ++l) B.sv[l * sz + n] = Tb.sv[l * tsz + tn];
+  }
+}
+
+// eliminate_k_gradient, src/FieldOperation.cu:42-62 (2-D cases)
+template <class C>
+__global__ void k_kcopy(const DevBlock *__restrict__ blks, int b) {
+  const DevBlock &B = blks[b];
+  const int g = B.ngg;
+  const int ex = B.mx + 2 * g, ey = B.my + 2 * g;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ex * ey) return;
+  const int i = t % ex - g, j = t / ex - g;
+  const int64_t sz = B.G.size, n0 = B.G.at(i, j, 0);
+  for (int k = 1; k <= g; ++k) {
+    const int64_t np = n0 + k * B.G.sxy, nm = n0 - k * B.G.sxy;
+    for (int l = 0; l < 6; ++l) {
+      B.bv[l * sz + np] = B.bv[l * sz + n0];
+      B.bv[l * sz + nm] = B.bv[l * sz + n0];
+    }
+    OSTC_UNROLL for (int l = 0; l < C::nsc; ++l) {
+      B.sv[l * sz + np] = B.sv[l * sz + n0];
+      B.sv[l * sz + nm] = B.sv[l * sz + n0];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- residual
+// store_last_step, src/TimeAdvanceFunc.cu:5-16
+static __global__ void __launch_bounds__(kCta) k_store_last(const DevBlock *__restrict__ blks, Tiles T) {
+  int b, i, j, k;
+  if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
+  const DevBlock &B = blks[b];
+  const int64_t n = B.G.at(i, j, k), nz = B.Z.at(i, j, k), sz = B.G.size, sz0 = B.Z.size;
+  B.bv_last[nz] = B.bv[n];
+  B.bv_last[sz0 + nz] = B.vel[n];
+  B.bv_last[2 * sz0 + nz] = B.bv[4 * sz + n];
+  B.bv_last[3 * sz0 + nz] = B.bv[5 * sz + n];
+}
+
+// compute_square_of_dbv + per-CTA partial sums (src/TimeAdvanceFunc.cu:18-32,
+// src/Driver.cu:418-459).  Partials are combined in a fixed order by
+// k_res_final, so the residual is reproducible run to run.
+static __global__ void __launch_bounds__(kCta) k_res_partial(const DevBlock *__restrict__ blks, Tiles T, double *partial) {
+  __shared__ double red[4][kCta / 32];
+  int b, i, j, k;
+  double s[4] = {0, 0, 0, 0};
+  if (tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) {
+    const DevBlock &B = blks[b];
+    const int64_t n = B.G.at(i, j, k), nz = B.Z.at(i, j, k), sz = B.G.size, sz0 = B.Z.size;
+    const double cur[4] = {B.bv[n], B.vel[n], B.bv[4 * sz + n], B.bv[5 * sz + n]};
+    for (int l = 0; l < 4; ++l) {
+      const double d = cur[l] - B.bv_last[l * sz0 + nz];
+      s[l] = d * d;
+    }
+  }
+  const int tid = threadIdx.x + kTX * (threadIdx.y + kTY * threadIdx.z);
+  for (int l = 0; l < 4; ++l) {
+    double v = s[l];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((tid & 31) == 0) red[l][tid >> 5] = v;
+  }
+  __syncthreads();
+  if (tid < 4) {
+    double v = 0;
+    for (int w = 0; w < kCta / 32; ++w) v += red[tid][w];
+    partial[static_cast<int64_t>(blockIdx.x) * 4 + tid] = v;
+  }
+}
+
+static __global__ void k_res_final(const double *partial, int n_part, double *out) {
+  __shared__ double red[4][32];
+  const int tid = threadIdx.x;  // 128 threads: 4 variables x 32 lanes
+  const int l = tid >> 5, lane = tid & 31;
+  double v = 0;
+  for (int q = lane; q < n_part; q += 32) v += partial[static_cast<int64_t>(q) * 4 + l];
+  red[l][lane] = v;
+  __syncthreads();
+  if (lane == 0) {
+    double s = 0;
+    for (int q = 0; q < 32; ++q) s += red[l][q];
+    out[l] = s;
+  }
+}
+
+// ---------------------------------------------------------------- initialisation
+// compute_cv_from_bv, src/FieldOperation.cuh:37-73 (launched with halo ngg)
+template <class C>
+__global__ void __launch_bounds__(kCta) k_cv_from_bv(const DevBlock *__restrict__ blks, Tiles T) {
+  int b, i, j, k;
+  if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
+  const DevBlock &B = blks[b];
+  const int64_t n = B.G.at(i, j, k), sz = B.G.size;
+  const double rho = B.bv[n];
+  B.cv[n] = rho;
+  B.cv[sz + n] = rho * B.bv[sz + n];
+  B.cv[2 * sz + n] = rho * B.bv[2 * sz + n];
+  B.cv[3 * sz + n] = rho * B.bv[3 * sz + n];
+  OSTC_UNROLL for (int l = 0; l < C::nsc; ++l) B.cv[(5 + l) * sz + n] = rho * B.sv[l * sz + n];
+  total_energy<C>(B, n);
+}
+
+// initialize_mut, src/FieldOperation.cuh:111-137 (launched with halo 1)
+template <class C>
+__global__ void __launch_bounds__(kCta) k_init_mut(const DevBlock *__restrict__ blks, Tiles T) {
+  constexpr int NS = C::ns;
+  int b, i, j, k;
+  if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
+  const DevBlock &B = blks[b];
+  const int64_t n = B.G.at(i, j, k), sz = B.G.size;
+  const double t = B.bv[5 * sz + n];
+  double mul = sutherland(t);
+  if constexpr (C::mix != 0) {
+    double mw = 0, Y[NS];
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) {
+      Y[l] = B.sv[l * sz + n];
+      mw += Y[l] / cP.mw[l];
+    }
+    mw = 1 / mw;
+    mul = mixture_viscosity<NS>(t, mw, Y);
+  }
+  B.mut[n] = sst_mut<C>(B, n, mul);
+}
+
+// compute_wall_distance, src/Driver.cu:461-482 (brute force; halo ngg)
+static __global__ void __launch_bounds__(kCta) k_wall_distance(const DevBlock *__restrict__ blks, Tiles T,
+                                                        const double *__restrict__ wall, int n_wall) {
+  int b, i, j, k;
+  if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
+  const DevBlock &B = blks[b];
+  const int64_t n = B.G.at(i, j, k);
+  const double x = B.x[n], y = B.y[n], z = B.z[n];
+  double wd = 1e+6;
+  for (int l = 0; l < n_wall; ++l) {
+    const double d = (x - wall[3 * l]) * (x - wall[3 * l]) + (y - wall[3 * l + 1]) * (y - wall[3 * l + 1]) +
+                     (z - wall[3 * l + 2]) * (z - wall[3 * l + 2]);
+    if (wd > d) wd = d;
+  }
+  B.wall_dist[n] = sqrt(wd);
+}
+
+}  // namespace ostc

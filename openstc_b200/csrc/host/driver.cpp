@@ -1,0 +1,334 @@
+#include "driver.hpp"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <limits>
+
+#include "plt_io.hpp"
+
+namespace ostc {
+
+Driver::Driver(const std::string &dir, const DriverOptions &o) : case_dir(dir), opt(o), parameter(dir) {
+  mesh = Mesh(parameter);
+  spec = Species(parameter);
+  reac = Reaction(parameter, spec);
+  const bool species = parameter.get_bool("species");
+  const bool reaction = parameter.get_bool("reaction");
+  int turb_method = parameter.get_int("turbulence_method");
+  if (!parameter.get_bool("turbulence")) turb_method = 0;
+  rans = turb_method == 1;
+  mix = species ? (reaction ? 2 : 1) : 0;
+  if (rans && parameter.get_int("RANS_model") != 2)
+    throw ParameterError("only the k-omega SST model (RANS_model = 2) is implemented");
+
+  // initialize_basic_variables, src/Initialize.cuh:37-55: the default inflow
+  // is always constructed first, which defines rho_inf / v_inf / p_inf.
+  Inflow default_inflow(parameter.get_string("default_init"), spec, parameter);
+  field.resize(mesh.n_block);
+  const int initial = parameter.get_int("initial");
+  if (initial == 1) {
+    const int n_scalar = parameter.get_int("n_scalar");
+    for (int b = 0; b < mesh.n_block; ++b) {
+      HostField &F = field[b];
+      F.e = Extent{mesh[b].mx, mesh[b].my, mesh[b].mz, mesh[b].ngg};
+      F.n_scalar = n_scalar;
+      F.bv.assign(static_cast<size_t>(6 * F.e.size()), 0.0);
+      F.sv.assign(static_cast<size_t>(n_scalar * F.e.size()), 0.0);
+    }
+    const std::string plt = case_dir + "/output/field/flowfield.plt";
+    if (!read_plt_restart(plt, mesh, spec, parameter, field))
+      throw ParameterError("restart requested but " + plt + " does not exist");
+    std::ifstream st(case_dir + "/output/message/step.txt");
+    int s = 0;
+    if (st >> s) parameter.set("step", s);
+    std::ifstream rs(case_dir + "/output/message/residual_scale.txt");
+    rs >> res_scale[0] >> res_scale[1] >> res_scale[2] >> res_scale[3];
+  } else {
+    initialize_from_start(parameter, mesh, spec, field);
+    std::ofstream history(case_dir + "/history.dat", std::ios::trunc);
+    history << "step\terror_max\n";
+  }
+  step = parameter.get_int("step");
+  bc.build(mesh, spec, parameter);
+  build_dev_params();
+  build_faces();
+}
+
+void Driver::build_dev_params() {
+  DevParams &p = dev_params;
+  std::memset(&p, 0, sizeof(p));
+  const Parameter &P = parameter;
+  p.ns = spec.n_spec;
+  p.nr = reac.n_reac;
+  if (p.nr > kMaxReac) throw ParameterError("at most 50 reactions are supported (MAX_REAC_NUMBER)");
+  p.n_var = P.get_int("n_var");
+  p.n_scalar = P.get_int("n_scalar");
+  p.mix = mix;
+  p.turb = rans ? 1 : 0;
+  p.rans_model = P.get_int("RANS_model");
+  p.turb_implicit = P.get_int("turb_implicit");
+  p.chem_src_method = P.get_int("chemSrcMethod");
+  p.implicit_method = P.get_int("implicit_method");
+  p.dplur_inner_step = p.implicit_method == 1 ? P.get_int("DPLUR_inner_step") : 0;
+  p.reconstruction = P.get_int("reconstruction");
+  p.limiter = P.get_int("limiter");
+  p.viscous_order = P.get_int("viscous_order");
+  p.dim = mesh.dimension;
+  p.cfl = P.get_real("cfl");
+  p.Pr = P.get_real("prandtl_number");
+  p.Prt = P.get_real("turbulent_prandtl_number");
+  p.Sct = P.get_real("turbulent_schmidt_number");
+  p.Sc = P.get_real("schmidt_number");
+  if (p.limiter != 0 && p.limiter != 1) throw ParameterError("only the minmod limiter (0) is implemented");
+  // DParameter::limit_flow, src/DParameter.cu:78-100
+  const double rho_inf = P.get_real("rho_inf"), v_inf = P.get_real("v_inf"), p_inf = P.get_real("p_inf");
+  p.ll[0] = 1e-6 * rho_inf;
+  p.ul[0] = 1e+3 * rho_inf;
+  for (int l = 1; l < 4; ++l) {
+    p.ll[l] = -1e+3 * v_inf;
+    p.ul[l] = 1e+3 * v_inf;
+  }
+  p.ll[4] = 1e-6 * p_inf;
+  p.ul[4] = 1e+3 * p_inf;
+  if (p.rans_model == 2) {
+    p.ul[5] = std::numeric_limits<double>::max();
+    p.ul[6] = std::numeric_limits<double>::max();
+  }
+  const auto &sv_inf = P.get_real_array("sv_inf");
+  for (int l = 0; l < p.n_scalar && l < static_cast<int>(sv_inf.size()); ++l) p.sv_inf[l] = sv_inf[l];
+  const int ns = p.ns;
+  for (int i = 0; i < ns; ++i) {
+    p.mw[i] = spec.mw[i];
+    p.t_low[i] = spec.t_low[i];
+    p.t_mid[i] = spec.t_mid[i];
+    for (int q = 0; q < 7; ++q) {
+      p.low[i * 7 + q] = spec.low_coeff[i * 7 + q];
+      p.high[i * 7 + q] = spec.high_coeff[i * 7 + q];
+    }
+    p.lj_inv[i] = spec.lj_potent_inv[i];
+    p.vis_coeff[i] = spec.vis_coeff[i];
+    for (int j = 0; j < ns; ++j) {
+      p.wq[i * ns + j] = spec.wj_div_wi_quarter[i * ns + j];
+      p.w8[i * ns + j] = spec.sqrt_wi_div_wj_8[i * ns + j];
+    }
+  }
+  for (int r = 0; r < p.nr; ++r) {
+    p.label[r] = reac.label[r];
+    p.order[r] = reac.order[r];
+    p.A[r] = reac.A[r];
+    p.b[r] = reac.b[r];
+    p.Ea[r] = reac.Ea[r];
+    p.A2[r] = reac.A2[r];
+    p.b2[r] = reac.b2[r];
+    p.Ea2[r] = reac.Ea2[r];
+    p.troe_a[r] = reac.troe_alpha[r];
+    p.troe_t3[r] = reac.troe_t3[r];
+    p.troe_t1[r] = reac.troe_t1[r];
+    p.troe_t2[r] = reac.troe_t2[r];
+    for (int l = 0; l < ns; ++l) {
+      p.sf[r * ns + l] = static_cast<signed char>(reac.stoi_f[r * ns + l]);
+      p.sb[r * ns + l] = static_cast<signed char>(reac.stoi_b[r * ns + l]);
+      p.tb[r * ns + l] = reac.third_body[r * ns + l];
+    }
+  }
+}
+
+void Driver::build_faces() {
+  host_bcs.clear();
+  for (const BcFace &f : bc.order) {
+    const Boundary &b = mesh[f.block].boundary[f.face_index];
+    HostBc h{};
+    h.block = f.block;
+    h.type = static_cast<int>(f.type);
+    h.face = b.face;
+    h.direction = b.direction;
+    for (int q = 0; q < 3; ++q) {
+      h.start[q] = b.start[q];
+      h.end[q] = b.end[q];
+    }
+    if (f.type == BcType::inflow) {
+      const Inflow &in = bc.inflow[f.cond];
+      h.density = in.density;
+      h.u = in.u;
+      h.v = in.v;
+      h.w = in.w;
+      h.pressure = in.pressure;
+      h.temperature = in.temperature;
+      h.mut = in.mut;
+      for (size_t l = 0; l < in.sv.size() && l < kMaxSpec + 2; ++l) h.sv[l] = in.sv[l];
+    } else if (f.type == BcType::wall) {
+      const Wall &w = bc.wall[f.cond];
+      h.isothermal = w.isothermal ? 1 : 0;
+      h.t_wall = w.temperature;
+    }
+    host_bcs.push_back(h);
+  }
+  host_inner.clear();
+  for (int b = 0; b < mesh.n_block; ++b)
+    for (const InnerFace &f : mesh[b].inner_face) {
+      HostInner h{};
+      h.block = b;
+      h.target_block = f.target_block;
+      h.face = f.face;
+      h.direction = f.direction;
+      for (int q = 0; q < 3; ++q) {
+        h.start[q] = f.start[q];
+        h.end[q] = f.end[q];
+        h.loop_dir[q] = f.loop_dir[q];
+        h.tstart[q] = f.tstart[q];
+        h.tloop_dir[q] = f.target_loop_dir[q];
+        h.src_tar[q] = f.src_tar[q];
+        h.n_point[q] = f.n_point[q];
+      }
+      host_inner.push_back(h);
+    }
+  // Wall points of the trimmed wall faces (Driver::acquire_wall_distance,
+  // src/Driver.cu:123-150).
+  wall_points.clear();
+  for (const HostBc &h : host_bcs) {
+    if (h.type != static_cast<int>(BcType::wall)) continue;
+    const Block &B = mesh[h.block];
+    for (int k = h.start[2]; k <= h.end[2]; ++k)
+      for (int j = h.start[1]; j <= h.end[1]; ++j)
+        for (int i = h.start[0]; i <= h.end[0]; ++i) {
+          wall_points.push_back(B.x(i, j, k));
+          wall_points.push_back(B.y(i, j, k));
+          wall_points.push_back(B.z(i, j, k));
+        }
+  }
+}
+
+Engine &Driver::engine() {
+  if (!engine_) throw ParameterError("the device engine is not initialised");
+  return *engine_;
+}
+
+void Driver::initialize_computation() {
+  EngineSetup s;
+  s.params = dev_params;
+  s.ngg = mesh.ngg;
+  for (const auto &b : mesh.block) s.dims.push_back({b.mx, b.my, b.mz});
+  s.bcs = host_bcs;
+  s.inner = host_inner;
+  s.wall_points = wall_points;
+  s.device = opt.device;
+  engine_ = make_engine(s);
+  for (int b = 0; b < mesh.n_block; ++b) {
+    const Block &B = mesh[b];
+    const int64_t n = B.x.e.size();
+    engine_->set_field(b, F_X, B.x.v.data(), n);
+    engine_->set_field(b, F_Y, B.y.v.data(), n);
+    engine_->set_field(b, F_Z, B.z.v.data(), n);
+    engine_->set_field(b, F_JAC, B.jac.v.data(), n);
+    std::vector<double> met(static_cast<size_t>(9 * n));
+    for (int q = 0; q < 9; ++q) std::copy(B.metric[q].v.begin(), B.metric[q].v.end(), met.begin() + q * n);
+    engine_->set_field(b, F_METRIC, met.data(), 9 * n);
+    engine_->set_field(b, F_BV, field[b].bv.data(), static_cast<int64_t>(field[b].bv.size()));
+    if (!field[b].sv.empty())
+      engine_->set_field(b, F_SV, field[b].sv.data(), static_cast<int64_t>(field[b].sv.size()));
+  }
+  engine_->initialize();
+  if (!opt.quiet) std::printf("The flowfield is completely initialized on GPU.\n");
+}
+
+double Driver::compute_residual(int step_no, const double raw[4]) {
+  // Driver::compute_residual, src/Driver.cu:292-380
+  for (int l = 0; l < 4; ++l) res[l] = std::sqrt(raw[l] / static_cast<double>(mesh.n_grid_total));
+  if (step_no == 1) {
+    for (int l = 0; l < 4; ++l) {
+      res_scale[l] = res[l];
+      if (res_scale[l] < 1e-20) res_scale[l] = 1e-20;
+    }
+    const std::filesystem::path dir = std::filesystem::path(case_dir) / "output" / "message";
+    std::filesystem::create_directories(dir);
+    std::ofstream out(dir / "residual_scale.txt");
+    out << res_scale[0] << '\n' << res_scale[1] << '\n' << res_scale[2] << '\n' << res_scale[3] << '\n';
+  }
+  for (int l = 0; l < 4; ++l) res[l] /= res_scale[l];
+  double err_max = res[0];
+  for (int l = 1; l < 4; ++l)
+    if (std::abs(res[l]) > err_max) err_max = res[l];
+  if (std::isnan(err_max)) throw ParameterError("Nan occurred in step " + std::to_string(step_no) + ". Stop simulation.");
+  return err_max;
+}
+
+double Driver::advance(int n) {
+  Engine &E = engine();
+  const int screen = parameter.get_int("output_screen");
+  double err = -1;
+  for (int q = 0; q < n; ++q) {
+    ++step;
+    const bool store = step % screen == 0;
+    const bool due = store || step == 1;
+    double raw[4] = {0, 0, 0, 0};
+    E.step(store, due, raw);
+    if (due) err = compute_residual(step, raw);
+  }
+  E.synchronize();
+  return err;
+}
+
+void Driver::simulate() {
+  if (!parameter.get_bool("steady")) throw ParameterError("Not implemented: only steady simulations are supported");
+  Engine &E = engine();
+  if (!opt.quiet) std::printf("Steady flow simulation.\n");
+  const int total = parameter.get_int("total_step") + step;
+  const int screen = parameter.get_int("output_screen");
+  const int out_file = parameter.get_int("output_file");
+  const double criteria = parameter.get_real("convergence_criteria");
+  bool converged = false;
+  while (!converged) {
+    ++step;
+    if (step > total) break;
+    const bool store = step % screen == 0;
+    const bool due = store || step == 1;
+    double raw[4] = {0, 0, 0, 0};
+    E.step(store, due, raw);
+    if (due) {
+      const double err_max = compute_residual(step, raw);
+      converged = err_max < criteria;
+      std::FILE *h = std::fopen((case_dir + "/history.dat").c_str(), "a");
+      if (h) {
+        std::fprintf(h, "%d\t%11.4e\n", step, err_max);
+        std::fclose(h);
+      }
+      if (!opt.quiet) {
+        std::printf("\n%38s    converged to: %11.4e\n", "rho", res[0]);
+        std::printf("  n=%8d,                       V     converged to: %11.4e   \n", step, res[1]);
+        std::printf("  n=%8d,                       p     converged to: %11.4e   \n", step, res[2]);
+        std::printf("%38s    converged to: %11.4e\n", "T ", res[3]);
+      }
+    }
+    if (step % out_file == 0 || converged) {
+      const std::filesystem::path dir = std::filesystem::path(case_dir) / "output" / "message";
+      std::filesystem::create_directories(dir);
+      std::ofstream(dir / "step.txt") << step;
+      write_field(case_dir + "/output/field/flowfield.plt");
+    }
+  }
+  E.synchronize();
+}
+
+void Driver::write_field(const std::string &path) {
+  Engine &E = engine();
+  std::vector<std::vector<double>> mach(mesh.n_block), mut(mesh.n_block);
+  std::vector<PltBlockData> blocks(mesh.n_block);
+  for (int b = 0; b < mesh.n_block; ++b) {
+    HostField &F = field[b];
+    E.get_field(b, F_BV, F.bv.data(), static_cast<int64_t>(F.bv.size()));
+    if (!F.sv.empty()) E.get_field(b, F_SV, F.sv.data(), static_cast<int64_t>(F.sv.size()));
+    mach[b].resize(static_cast<size_t>(F.e.size()));
+    E.get_field(b, F_MACH, mach[b].data(), F.e.size());
+    if (rans) {
+      mut[b].resize(static_cast<size_t>(F.e.size()));
+      E.get_field(b, F_MUT, mut[b].data(), F.e.size());
+    }
+    blocks[b] = PltBlockData{&mesh[b], &F, &mach[b], rans ? &mut[b] : nullptr};
+  }
+  write_plt(path, blocks, spec, rans);
+}
+
+}  // namespace ostc

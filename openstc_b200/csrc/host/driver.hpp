@@ -1,0 +1,68 @@
+// Driver of the steady pseudo-time loop: the host side of the reference's
+// cfd::Driver<mix, turb> (src/Driver.cuh:12-46, src/Driver.cu:14-415) on
+// top of the sm_100a engine.
+#pragma once
+
+#include <array>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../device/engine.hpp"
+#include "boundary.hpp"
+#include "chemdata.hpp"
+#include "mesh.hpp"
+#include "parameter.hpp"
+
+namespace ostc {
+
+struct DriverOptions {
+  int device = 0;
+  bool quiet = false;
+};
+
+class Driver {
+ public:
+  // Reads the case directory and prepares the initial field (the reference's
+  // main + Driver constructor, src/main.cu:7-28, src/Driver.cu:14-40).  No
+  // GPU work happens here.
+  Driver(const std::string &case_dir, const DriverOptions &opt);
+
+  // Driver::initialize_computation: creates the engine, uploads the grid and
+  // field and runs the initial boundary / exchange / property passes.
+  void initialize_computation();
+  // Driver::simulate: the steady loop with residual output and .plt output.
+  void simulate();
+  // Advances n loop iterations (residual cadence of the reference, no file
+  // output).  Returns the last err_max or -1 when no residual was due.
+  double advance(int n);
+
+  void write_field(const std::string &path);
+  bool initialized() const { return engine_ != nullptr; }
+  Engine &engine();
+
+  std::string case_dir;
+  DriverOptions opt;
+  Parameter parameter;
+  Mesh mesh;
+  Species spec;
+  Reaction reac;
+  BcRegistry bc;
+  std::vector<HostField> field;
+  DevParams dev_params{};
+  std::vector<HostBc> host_bcs;
+  std::vector<HostInner> host_inner;
+  std::vector<double> wall_points;
+  int step = 0;
+  std::array<double, 4> res{1, 1, 1, 1}, res_scale{1, 1, 1, 1};
+  bool rans = false;
+  int mix = 0;
+
+ private:
+  double compute_residual(int step_no, const double raw[4]);
+  void build_dev_params();
+  void build_faces();
+  std::unique_ptr<Engine> engine_;
+};
+
+}  // namespace ostc

@@ -1,0 +1,94 @@
+"""Generates the golden fixtures of tests/golden/ by running the reference
+program (Liangerty/OpenSTC built from its own sources by oracle/ref/Makefile
+into oracle/_ref/openstc_ref) on small cases written by openstc_b200.cases.
+
+The reference has no CPU path, so this runs on a GPU machine:
+
+    python tests/golden/make_golden.py --ref oracle/_ref/openstc_ref --out tests/golden
+
+Each fixture ``<case>_s<steps>.npz`` holds every variable of the reference's
+output/field/flowfield.plt after <steps> steps (x, y, z dropped) plus the
+history.dat residuals and residual_scale.txt of that run.
+"""
+from __future__ import annotations
+
+import argparse
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from openstc_b200 import cases  # noqa: E402
+from openstc_b200.plt import read_plt  # noqa: E402
+
+# name -> (builder, kwargs, steps recorded)
+CASES = {
+    "ramp": (cases.ramp_case, dict(mx=48, my=24), (1, 10, 100)),
+    "ml": (cases.mixing_layer_case, dict(mx=16, my=12, mz=6), (1, 10, 100)),
+    "ml_explicit": (cases.mixing_layer_case, dict(mx=16, my=12, mz=6, implicit=0), (1, 10)),
+    "mb": (cases.multiblock_case, dict(mxs=[10, 8], my=12, mz=6), (1, 10)),
+}
+
+
+def build_case(name: str, where: Path, steps: int) -> Path:
+    fn, kw, _ = CASES[name]
+    case = where / f"{name}_s{steps}"
+    if case.exists():
+        shutil.rmtree(case)
+    fn(case, **dict(kw, total_step=steps, output_screen=1, output_file=steps))
+    return case
+
+
+def run_reference(ref: Path, case: Path) -> None:
+    res = subprocess.run([str(ref.resolve())], cwd=case, capture_output=True, text=True, timeout=1800)
+    if res.returncode != 0:
+        raise RuntimeError(f"reference run failed in {case}:\n{res.stdout[-2000:]}\n{res.stderr[-2000:]}")
+
+
+def collect(case: Path) -> dict[str, np.ndarray]:
+    names, zones = read_plt(case / "output" / "field" / "flowfield.plt")
+    out: dict[str, np.ndarray] = {}
+    for z, zone in enumerate(zones):
+        for n in names:
+            if n in ("x", "y", "z"):
+                continue
+            out[f"b{z}/{n}"] = zone[n]
+    rows = []
+    for line in (case / "history.dat").read_text().splitlines():
+        parts = line.split()
+        if len(parts) == 2 and parts[0].isdigit():  # restart runs have no header line
+            rows.append([float(parts[0]), float(parts[1])])
+    out["history"] = np.array(rows) if rows else np.zeros((0, 2))
+    out["residual_scale"] = np.array([float(v) for v in (case / "output" / "message" / "residual_scale.txt")
+                                      .read_text().split()])
+    return out
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default=str(ROOT / "oracle" / "_ref" / "openstc_ref"))
+    ap.add_argument("--out", default=str(ROOT / "tests" / "golden"))
+    ap.add_argument("--work", default=str(ROOT / "cases" / "golden_runs"))
+    ap.add_argument("--only", nargs="*")
+    a = ap.parse_args()
+    work = Path(a.work)
+    work.mkdir(parents=True, exist_ok=True)
+    out = Path(a.out)
+    out.mkdir(parents=True, exist_ok=True)
+    for name, (_, _, steps_list) in CASES.items():
+        if a.only and name not in a.only:
+            continue
+        for steps in steps_list:
+            case = build_case(name, work, steps)
+            run_reference(Path(a.ref), case)
+            np.savez_compressed(out / f"{name}_s{steps}.npz", **collect(case))
+            print(f"{name} {steps} steps: ok", flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,66 @@
+"""The C ABI library loads, exports every declared entry point and reads
+cases on the host (no GPU needed)."""
+import ctypes
+import re
+
+import numpy as np
+import pytest
+
+import openstc_b200 as ostc
+from openstc_b200 import cases
+from conftest import ROOT
+
+
+def declared_symbols():
+    text = (ROOT / "include" / "openstc_b200.h").read_text()
+    return sorted(set(re.findall(r"\b(ostc_[a-z_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(str(ostc.LIB_PATH))
+    names = declared_symbols()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_missing_case_reports_input_error(tmp_path):
+    with pytest.raises(ostc.OstcError, match="cannot open setup file"):
+        ostc.Driver(tmp_path / "nope")
+
+
+def test_device_calls_need_initialize(case_factory):
+    case = case_factory("ramp", cases.ramp_case, mx=16, my=12, total_step=2, output_screen=1)
+    d = ostc.Driver(case)
+    with pytest.raises(ostc.OstcError, match="initialize first"):
+        d.step(1)
+
+
+def test_ramp_case_description(case_factory):
+    case = case_factory("ramp", cases.ramp_case, mx=16, my=12, total_step=2, output_screen=1)
+    d = ostc.Driver(case)
+    i = d.info()
+    assert (i.n_block, i.dimension, i.n_var, i.n_scalar, i.mix, i.rans) == (1, 2, 5, 0, 0, 0)
+    assert i.n_grid_total == 16 * 12
+    types = [b.type for b in d.bcs()]
+    assert types == [6, 5, 3, 2]  # outflow, inflow, symmetry, wall: application order
+    wall = d.bcs()[-1]
+    assert list(wall.start) == [0, 0, 0] and list(wall.end) == [15, 0, 0]  # trimmed by ngg, k range [0, 0]
+    inflow = d.bcs()[1]
+    assert list(inflow.start) == [0, -2, -2] and list(inflow.end) == [0, 13, 2]
+    # Mach 3 at 220 K, 2.5 kPa: velocity = 3 sqrt(1.4 R T / W)
+    c = np.sqrt(1.4 * 8314.462618 / 28.9647 * 220.0)
+    assert inflow.u == pytest.approx(3 * c, rel=1e-14)
+    assert inflow.density == pytest.approx(2500.0 * 28.9647 / (8314.462618 * 220.0), rel=1e-14)
+
+
+def test_layouts_follow_reference_ghosts(case_factory):
+    case = case_factory("ml", cases.mixing_layer_case, mx=12, my=10, mz=6, total_step=2, output_screen=1)
+    d = ostc.Driver(case)
+    assert d.layout("bv") == (2, 6)
+    assert d.layout("sv") == (2, 11)
+    assert d.layout("cv") == (2, 16)
+    assert d.layout("dq") == (1, 16)        # one ghost layer under DPLUR
+    assert d.layout("chem_jac") == (0, 81)  # EPI Jacobian, no ghosts
+    assert d.layout("bv_last") == (0, 4)
+    assert d.field_shape(0, "metric") == (9, 10, 14, 16)

@@ -1,0 +1,134 @@
+"""FP64 parity of the sm_100a path (through the C ABI) with the CPU oracle and
+with the reference program's own outputs (tests/golden).
+
+Tolerances, relative to each field's magnitude (max|gpu - ref| / max|ref|):
+  * one phase from identical inputs: 1e-12 (CUDA vs glibc libm differ by ulps)
+  * after N steps vs the oracle: 1e-9
+  * vs the reference's CUDA build after N steps: 1e-10 (same compiler and math
+    library on both sides).
+"""
+import numpy as np
+import pytest
+
+import openstc_b200 as ostc
+from openstc_b200 import cases
+from conftest import GOLDEN, rel_err
+from oracle_bridge import OracleSolver, interior
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "ramp": (cases.ramp_case, dict(mx=48, my=24)),
+    "ml": (cases.mixing_layer_case, dict(mx=16, my=12, mz=6)),
+    "ml_explicit": (cases.mixing_layer_case, dict(mx=16, my=12, mz=6, implicit=0)),
+    "mb": (cases.multiblock_case, dict(mxs=[10, 8], my=12, mz=6)),
+}
+
+STATE = ["bv", "sv", "cv", "vel", "acoustic", "mach", "mul", "conductivity", "mut", "turb_cond", "rho_d", "gamma",
+         "cp", "wall_dist"]
+
+
+def make_case(case_factory, name, steps=10):
+    fn, kw = CASES[name]
+    return case_factory(name, fn, **dict(kw, total_step=steps, output_screen=1, output_file=steps))
+
+
+def pair(case):
+    gpu = ostc.Driver(case)
+    gpu.initialize()
+    orc = OracleSolver(ostc.Driver(case), threads=4)
+    orc.initialize()
+    return gpu, orc
+
+
+def compare(gpu, orc, fields, tol, ghosts=True):
+    worst = {}
+    for b in range(gpu.info().n_block):
+        for f in fields:
+            g, n = gpu.layout(f)
+            if n == 0:
+                continue
+            a = gpu.get(b, f)
+            o = orc.get(b, f, a.shape)
+            if not ghosts:
+                a, o = interior(a, g), interior(o, g)
+            worst[f"b{b}/{f}"] = rel_err(a, o)
+    bad = {k: v for k, v in worst.items() if not v <= tol}
+    assert not bad, f"fields beyond {tol}: {bad}"
+    return worst
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_initialization_matches_oracle(case_factory, name):
+    gpu, orc = pair(make_case(case_factory, name))
+    compare(gpu, orc, STATE, 1e-12)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_each_phase_matches_oracle(case_factory, name):
+    gpu, orc = pair(make_case(case_factory, name))
+    nb = gpu.info().n_block
+    gpu.run_phase("residual")
+    for b in range(nb):
+        orc.phase("residual", b)
+    compare(gpu, orc, ["dq", "dt_local", "inv_spec", "visc_spec", "mut", "turb_cond", "chem_jac", "turb_src_jac"],
+            1e-12, ghosts=False)
+    gpu.run_phase("implicit")
+    for b in range(nb):
+        orc.phase("implicit", b)
+    compare(gpu, orc, ["dq", "dq0"], 1e-12, ghosts=False)
+    gpu.run_phase("update")
+    for b in range(nb):
+        orc.phase("update", b)
+    compare(gpu, orc, ["bv", "sv", "cv", "vel"], 1e-12)
+    gpu.run_phase("bc")
+    for b in range(nb):
+        orc.phase("bc", b)
+    compare(gpu, orc, ["bv", "sv", "cv", "vel", "mut"], 1e-12)
+    gpu.run_phase("exchange")
+    orc.phase("exchange")
+    compare(gpu, orc, STATE, 1e-12)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_ten_steps_match_oracle(case_factory, name):
+    case = make_case(case_factory, name)
+    gpu, orc = pair(case)
+    err_gpu = gpu.step(10)
+    res_orc = None
+    for s in range(1, 11):
+        r = orc.step(s)
+        if r is not None:
+            res_orc = r
+    compare(gpu, orc, STATE, 1e-9)
+    assert np.isfinite(err_gpu)
+
+
+@pytest.mark.parametrize("name,steps", [(n, s) for n in CASES for s in (1, 10, 100)])
+def test_matches_reference_program(case_factory, name, steps):
+    """Fields of the reference's own flowfield.plt after `steps` steps."""
+    fix = GOLDEN / f"{name}_s{steps}.npz"
+    if not fix.exists():
+        pytest.skip(f"no reference fixture {fix.name}")
+    gold = np.load(fix)
+    gpu = ostc.Driver(make_case(case_factory, name, steps))
+    gpu.initialize()
+    gpu.step(steps)
+    names = [k.split("/", 1)[1] for k in gold.files if k.startswith("b0/")]
+    info = gpu.info()
+    worst = {}
+    for b in range(info.n_block):
+        bv, sv, mach = gpu.get(b, "bv"), gpu.get(b, "sv") if info.n_scalar else None, gpu.get(b, "mach")
+        mut = gpu.get(b, "mut") if info.rans else None
+        g = info.ngg
+        cols = {"density": bv[0], "u": bv[1], "v": bv[2], "w": bv[3], "pressure": bv[4], "temperature": bv[5],
+                "mach": mach[0]}
+        sp = [n for n in names if n not in cols and n not in ("tke", "omega", "mut")]
+        for l, n in enumerate(sp):
+            cols[n] = sv[l]
+        if info.rans:
+            cols["tke"], cols["omega"], cols["mut"] = sv[info.n_spec], sv[info.n_spec + 1], mut[0]
+        for n, a in cols.items():
+            worst[f"b{b}/{n}"] = rel_err(interior(a, g), gold[f"b{b}/{n}"])
+    bad = {k: v for k, v in worst.items() if not v <= 1e-10}
+    assert not bad, f"fields beyond 1e-10 vs the reference program: {bad}"
