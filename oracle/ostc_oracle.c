@@ -1607,7 +1607,10 @@ int orc_initialize(orc_solver *s) {
           }
     }
   }
-  orc_phase_exchange(s);
+  /* data_communication then update_physical_properties; unlike the step
+     loop there is no 2-D k copy here (src/Driver.cu:91-103) */
+  for (int q = 0; q < s->ninner; ++q) inner_exchange(s, &s->inner[q]);
+  for (int b = 0; b < s->nb; ++b) properties(s, &s->b[b]);
   return 0;
 }
 

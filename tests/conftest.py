@@ -30,7 +30,7 @@ def case_factory(tmp_path_factory):
     cache: dict = {}
 
     def make(name, builder, **kw):
-        key = (name, builder.__name__, tuple(sorted(kw.items())))
+        key = (name, builder.__name__, tuple(sorted((k, tuple(v) if isinstance(v, list) else v) for k, v in kw.items())))
         if key not in cache:
             cache[key] = builder(tmp_path_factory.mktemp(name), **kw)
         return cache[key]
@@ -51,6 +51,33 @@ def rel_err(a: np.ndarray, b: np.ndarray) -> float:
     if scale == 0.0:
         return float(np.max(np.abs(a - b))) if a.size else 0.0
     return float(np.max(np.abs(a - b))) / scale
+
+
+VELOCITY = ("u", "v", "w")
+SPECIES = ("H2", "H", "O2", "O", "OH", "HO2", "H2O2", "H2O", "N2")
+
+
+def scaled_err(fields: dict, gold: dict) -> dict:
+    """Per field: max|a - ref| divided by the variable's natural scale:
+    the velocity magnitude scale (max over u, v, w) for velocity components,
+    1 for mass fractions, the field's own max|ref| otherwise."""
+    vscale = max(float(np.max(np.abs(gold[n]))) for n in VELOCITY if n in gold) if any(
+        n in gold for n in VELOCITY) else 1.0
+    out = {}
+    for n, a in fields.items():
+        b = np.asarray(gold[n], dtype=np.float64)
+        a = np.asarray(a, dtype=np.float64)
+        if n in VELOCITY:
+            scale = vscale
+        elif n in SPECIES:
+            scale = 1.0
+        else:
+            scale = float(np.max(np.abs(b))) or 1.0
+        d = np.abs(a - b)
+        both_nan = np.isnan(a) & np.isnan(b)
+        d[both_nan] = 0.0
+        out[n] = float(np.max(d)) / scale if d.size else 0.0
+    return out
 
 
 def has_gpu() -> bool:
