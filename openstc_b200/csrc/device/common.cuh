@@ -34,6 +34,7 @@ struct DevParams {
   double ll[7], ul[7];
   double sv_inf[kMaxSpec + 2];
   double mw[kMaxSpec], t_low[kMaxSpec], t_mid[kMaxSpec];
+  double ru_mw[kMaxSpec];  // R_u / W_k (the quotient the reference divides out each time)
   double low[kMaxSpec * 7], high[kMaxSpec * 7];
   double lj_inv[kMaxSpec], vis_coeff[kMaxSpec];
   double wq[kMaxSpec * kMaxSpec], w8[kMaxSpec * kMaxSpec];

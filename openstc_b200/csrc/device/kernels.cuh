@@ -274,8 +274,8 @@ __device__ __forceinline__ void inviscid_face(const DevBlock &B, int64_t n, doub
     OSTC_UNROLL for (int l = 0; l < NS; ++l) {
       cpl += cpl_i[l] * pl[l + 5];
       cpr += cpr_i[l] * pr[l + 5];
-      cvl += pl[l + 5] * (cpl_i[l] - kDR_u / cP.mw[l]);
-      cvr += pr[l + 5] * (cpr_i[l] - kDR_u / cP.mw[l]);
+      cvl += pl[l + 5] * (cpl_i[l] - cP.ru_mw[l]);
+      cvr += pr[l + 5] * (cpr_i[l] - cP.ru_mw[l]);
       el += hl[l] * pl[l + 5];
       er += hr[l] * pr[l + 5];
     }

@@ -655,7 +655,7 @@ __global__ void __launch_bounds__(kCta) k_props(const DevBlock *__restrict__ blk
       Y[l] = B.sv[l * sz + n];
       mw += Y[l] / cP.mw[l];
       cp_tot += Y[l] * cp[l];
-      cv += Y[l] * (cp[l] - kDR_u / cP.mw[l]);
+      cv += Y[l] * (cp[l] - cP.ru_mw[l]);
     }
     mw = 1 / mw;
     const double gamma = cp_tot / cv;

@@ -3,6 +3,12 @@
 // operation order of the reference function it restates (cited), which is
 // what lets the FP64 path track the reference's CUDA build bit for bit where
 // the compiler contracts the same expressions the same way.
+//
+// The reference compiles its thermodynamic functions in their own
+// translation unit, so their outputs reach the callers already rounded.
+// These functions are inlined here; their final scaling uses __dmul_rn so
+// that no caller can fuse it into an FMA (cp - R/W, cp + 1.25 R/W, ...),
+// which keeps the callers' arithmetic identical to the reference's.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -54,7 +60,7 @@ __device__ __forceinline__ void enthalpy(double t, double *h) {
       h[i] = nasa(i, 0, lo) * t + 0.5 * nasa(i, 1, lo) * t2 + nasa(i, 2, lo) * t3 / 3 + 0.25 * nasa(i, 3, lo) * t4 +
              0.2 * nasa(i, 4, lo) * t5 + nasa(i, 5, lo);
     }
-    h[i] *= kDR_u / cP.mw[i];
+    h[i] = __dmul_rn(h[i], cP.ru_mw[i]);
   }
 }
 
@@ -77,8 +83,8 @@ __device__ __forceinline__ void enthalpy_cp(double t, double *h, double *cp) {
              0.2 * nasa(i, 4, lo) * t5 + nasa(i, 5, lo);
       cp[i] = nasa(i, 0, lo) + nasa(i, 1, lo) * t + nasa(i, 2, lo) * t2 + nasa(i, 3, lo) * t3 + nasa(i, 4, lo) * t4;
     }
-    h[i] *= kDR_u / cP.mw[i];
-    cp[i] *= kDR_u / cP.mw[i];
+    h[i] = __dmul_rn(h[i], cP.ru_mw[i]);
+    cp[i] = __dmul_rn(cp[i], cP.ru_mw[i]);
   }
 }
 
@@ -96,7 +102,7 @@ __device__ __forceinline__ void heat_capacity(double t, double *cp) {
       const bool lo = t < cP.t_mid[i];
       cp[i] = nasa(i, 0, lo) + nasa(i, 1, lo) * t + nasa(i, 2, lo) * t2 + nasa(i, 3, lo) * t3 + nasa(i, 4, lo) * t4;
     }
-    cp[i] *= kDR_u / cP.mw[i];
+    cp[i] = __dmul_rn(cp[i], cP.ru_mw[i]);
   }
 }
 

@@ -102,6 +102,7 @@ void Driver::build_dev_params() {
   const int ns = p.ns;
   for (int i = 0; i < ns; ++i) {
     p.mw[i] = spec.mw[i];
+    p.ru_mw[i] = kRu / spec.mw[i];
     p.t_low[i] = spec.t_low[i];
     p.t_mid[i] = spec.t_mid[i];
     for (int q = 0; q < 7; ++q) {
