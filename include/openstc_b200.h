@@ -164,6 +164,20 @@ int ostc_driver_profile_step(ostc_driver *d, char *buf, int buflen);
 /* The CUDA stream the engine launches on (cudaStream_t). */
 void *ostc_driver_stream(ostc_driver *d);
 
+/* No counterpart in the reference.  Recomputes, from the device state, the
+   normalised residuals of rho, |V|, p, T of the last step that stored its
+   previous state (every output_screen-th step; the same values
+   ostc_driver_residual returns right after such a step), without allocating
+   any device memory: the reduction runs in a static 2 MiB device scratch.
+   For callers that must not allocate, such as a convergence monitor polling
+   a solver whose flow state fills the device.  Limit: grids of at most
+   65536 tiles of 32x4x1 cells (8,388,608 interior cells); larger grids get
+   OSTC_ERR_INPUT.  The first call on a device performs set-up (the scratch's
+   address is looked up once) and should come before any stream capture on
+   that device.  One scratch per device: overlapping calls on the same device
+   race; serialise them.  Requires at least one step (OSTC_ERR_STATE). */
+int ostc_driver_residual_noalloc(ostc_driver *d, double res[4]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -113,6 +113,7 @@ def library() -> C.CDLL:
         "ostc_driver_simulate": ([P], C.c_int),
         "ostc_driver_step": ([P, C.c_int, D], C.c_int),
         "ostc_driver_residual": ([P, D], C.c_int),
+        "ostc_driver_residual_noalloc": ([P, D], C.c_int),
         "ostc_driver_run_phase": ([P, C.c_int], C.c_int),
         "ostc_driver_get_field": ([P, C.c_int, C.c_int, D, I64], C.c_int),
         "ostc_driver_set_field": ([P, C.c_int, C.c_int, D, I64], C.c_int),
@@ -236,6 +237,14 @@ class Driver:
     def residual(self) -> np.ndarray:
         r = np.zeros(4)
         _check(library().ostc_driver_residual(self._h, _dptr(r)))
+        return r
+
+    def residual_noalloc(self) -> np.ndarray:
+        """The residual of the last stored step recomputed on the device in
+        a static scratch (ostc_driver_residual_noalloc): no device memory
+        is allocated."""
+        r = np.zeros(4)
+        _check(library().ostc_driver_residual_noalloc(self._h, _dptr(r)))
         return r
 
     def run_phase(self, phase: str) -> None:

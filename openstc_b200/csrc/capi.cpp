@@ -1,11 +1,13 @@
 // extern "C" boundary of libopenstc_b200.so (declared in include/openstc_b200.h).
 #include "../../include/openstc_b200.h"
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <exception>
 #include <string>
 
+#include "device/engine.hpp"
 #include "host/driver.hpp"
 
 struct ostc_driver {
@@ -262,6 +264,27 @@ int ostc_driver_residual(const ostc_driver *d, double res[4]) {
   if (!d || !res) return fail(OSTC_ERR_INPUT, "null argument");
   for (int l = 0; l < 4; ++l) res[l] = d->drv.res[l];
   return OSTC_OK;
+}
+
+int ostc_driver_residual_noalloc(ostc_driver *d, double res[4]) {
+  if (!d || !res) return fail(OSTC_ERR_INPUT, "null argument");
+  if (!d->drv.initialized()) return fail(OSTC_ERR_STATE, "initialize first");
+  if (d->drv.step < 1) return fail(OSTC_ERR_STATE, "no step taken yet: the residual scale is set at step 1");
+  return guarded([&]() -> int {
+    ostc::Engine &E = d->drv.engine();
+    double raw[4] = {0, 0, 0, 0};
+    const char *why = "";
+    const int st = ostc::residual_sums_noalloc(E, d->drv.opt.device, raw, &why);
+    if (st == 1)
+      return fail(OSTC_ERR_INPUT, "ostc_driver_residual_noalloc: the grid has " + std::to_string(E.residual_tiles()) +
+                                      " residual tiles (32x4x1 cells); the static scratch holds at most " +
+                                      std::to_string(ostc::kNoAllocMaxTiles) + " (8388608 interior cells)");
+    if (st != 0) return fail(OSTC_ERR_CUDA, std::string("CUDA error in ostc_driver_residual_noalloc: ") + why);
+    // the normalisation of Driver::compute_residual, without touching its state
+    const double n = static_cast<double>(d->drv.mesh.n_grid_total);
+    for (int l = 0; l < 4; ++l) res[l] = std::sqrt(raw[l] / n) / d->drv.res_scale[l];
+    return OSTC_OK;
+  });
 }
 
 int ostc_driver_run_phase(ostc_driver *d, int phase) {

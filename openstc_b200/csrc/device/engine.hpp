@@ -66,7 +66,27 @@ class Engine {
   // returns (kernel name, launches, total ms).  Advances the solution.
   virtual std::vector<std::tuple<std::string, int, double>> profile_step() = 0;
   virtual double last_step_ms() const = 0;
+  // Number of 32x4x1-cell tiles of the residual reduction (one partial sum
+  // per variable per tile).
+  virtual int residual_tiles() const = 0;
+  // Launches on the engine stream the residual reduction of step(): the sums
+  // over interior cells of (current - bv_last)^2 for rho, |V|, p and T, with
+  // the per-tile partials in partial[4 * residual_tiles()] and the totals in
+  // out[4] (both device memory supplied by the caller).  Same kernels and
+  // summation order as the residual of step().
+  virtual void residual_sums_to(double *partial, double *out) = 0;
 };
+
+// Largest grid ostc_driver_residual_noalloc accepts, in residual tiles
+// (65536 tiles x 128 cells = 8,388,608 interior cells); its static device
+// scratch holds 4 partial sums per tile plus the 4 totals (2 MiB + 32 B).
+constexpr int kNoAllocMaxTiles = 65536;
+
+// The residual of the last stored step through the static device scratch of
+// residual_noalloc.cu, with no device allocation.  raw receives the four
+// sums.  Returns 0; 1 when the grid has more than kNoAllocMaxTiles tiles;
+// 2 on a CUDA error (*why: the runtime's static message).
+int residual_sums_noalloc(Engine &engine, int device, double raw[4], const char **why);
 
 std::unique_ptr<Engine> make_engine(const EngineSetup &setup);
 

@@ -464,6 +464,15 @@ class EngineT final : public Engine {
     cuda_check(cudaGetLastError(), "step launch");
   }
 
+  int residual_tiles() const override { return tiles0_.begin[tiles0_.nblk]; }
+
+  void residual_sums_to(double *partial, double *out) override {
+    const int n_part = tiles0_.begin[tiles0_.nblk];
+    k_res_partial<<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_, partial);
+    k_res_final<<<1, 128, 0, stream_>>>(partial, n_part, out);
+    cuda_check(cudaGetLastError(), "residual launch");
+  }
+
   void mark(const char *name) {
     if (!marks_) return;
     cudaEvent_t e;
