@@ -53,7 +53,10 @@ typedef enum ostc_phase {
   OSTC_PHASE_UPDATE = 2,   /* update_cv_and_bv + limit_flow (src/Driver.cu:248-251) */
   OSTC_PHASE_BC = 3,       /* boundary conditions (src/BoundCond.cuh:321-412) */
   OSTC_PHASE_EXCHANGE = 4, /* inner faces, 2-D k copy, properties (src/Driver.cu:257-272) */
-  OSTC_PHASE_STORE = 5     /* store_last_step (src/TimeAdvanceFunc.cu:5-16) */
+  OSTC_PHASE_STORE = 5,    /* store_last_step (src/TimeAdvanceFunc.cu:5-16) */
+  OSTC_PHASE_SOURCE = 6,   /* first half of RESIDUAL: dq = source terms (src/SourceTerm.cuh:12-40) */
+  OSTC_PHASE_FLUX = 7      /* second half of RESIDUAL: inviscid + viscous fluxes, local dt
+                              (src/SchemeSelector.cuh:38-280, src/TimeAdvanceFunc.cuh:21-71) */
 } ostc_phase;
 
 typedef struct ostc_options {

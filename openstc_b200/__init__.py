@@ -25,7 +25,7 @@ FIELDS = [
     "inv_spec", "visc_spec", "dt_local", "bv_last",
 ]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
-PHASES = {"residual": 0, "implicit": 1, "update": 2, "bc": 3, "exchange": 4, "store": 5}
+PHASES = {"residual": 0, "implicit": 1, "update": 2, "bc": 3, "exchange": 4, "store": 5, "source": 6, "flux": 7}
 
 
 class OstcError(RuntimeError):

@@ -183,6 +183,12 @@ class EngineT final : public Engine {
       case 5:
         k_store_last<<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_);
         break;
+      case 6:
+        k_source<C><<<grid(tiles0_), block3(), source_smem_, stream_>>>(d_blocks_, tiles0_);
+        break;
+      case 7:
+        k_flux<C><<<grid(tiles0_), block3(), flux_smem_, stream_>>>(d_blocks_, tiles0_);
+        break;
       default:
         throw std::runtime_error("unknown phase");
     }

@@ -330,14 +330,17 @@ __device__ __forceinline__ void inviscid_face(const DevBlock &B, int64_t n, doub
   const double mach_pos = 0.5 * (m_half + fabs(m_half));
   const double mach_neg = 0.5 * (m_half - fabs(m_half));
   const double mass_flux_half = c * (rho_l * mach_pos + rho_r * mach_neg);
-  const double coeff = mass_flux_half * gk;
+  // The reference stores each face flux (shared memory) before the cell
+  // differences; rounding the bare products here keeps the compiler from
+  // fusing them into those differences.
+  const double coeff = __dmul_rn(mass_flux_half, gk);
   const bool up = mass_flux_half >= 0;
   fc[0] = coeff;
   fc[1] = coeff * (up ? pl[1] : pr[1]) + p_coeff * k1;
   fc[2] = coeff * (up ? pl[2] : pr[2]) + p_coeff * k2;
   fc[3] = coeff * (up ? pl[3] : pr[3]) + p_coeff * k3;
   fc[4] = up ? coeff * (pl[NV] + pl[4]) / pl[0] : coeff * (pr[NV] + pr[4]) / pr[0];
-  OSTC_UNROLL for (int l = 5; l < NV; ++l) fc[l] = coeff * (up ? pl[l] : pr[l]);
+  OSTC_UNROLL for (int l = 5; l < NV; ++l) fc[l] = __dmul_rn(coeff, up ? pl[l] : pr[l]);
 }
 
 // ---------------------------------------------------------------- viscous
@@ -483,8 +486,9 @@ __device__ __forceinline__ void viscous_face(const DevBlock &B, int64_t n, doubl
     }
     const double sigma_k = sst::sigma_k2 + sst::delta_sigma_k * f1;
     const double sigma_omega = sst::sigma_omega2 + sst::delta_sigma_omega * f1;
-    fv[5 + NS] = (mul + mut * sigma_k) * (kx * k_x + ky * k_y + kz * k_z);
-    fv[6 + NS] = (mul + mut * sigma_omega) * (kx * omega_x + ky * omega_y + kz * omega_z);
+    // stored by the reference before use: keep the products rounded
+    fv[5 + NS] = __dmul_rn(mul + mut * sigma_k, kx * k_x + ky * k_y + kz * k_z);
+    fv[6 + NS] = __dmul_rn(mul + mut * sigma_omega, kx * omega_x + ky * omega_y + kz * omega_z);
   }
 }
 

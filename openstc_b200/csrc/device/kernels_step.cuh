@@ -716,7 +716,8 @@ __device__ __forceinline__ void total_energy(const DevBlock &B, int64_t n) {
   const int64_t sz = B.G.size;
   const double u = B.bv[sz + n], v = B.bv[2 * sz + n], w = B.bv[3 * sz + n];
   const double vel = u * u + v * v + w * w;
-  double e = 0.5 * B.bv[n] * vel;
+  // the reference stores this product in cv before adding the enthalpies
+  double e = __dmul_rn(0.5 * B.bv[n], vel);
   if constexpr (C::mix != 0) {
     double h[NS];
     enthalpy<NS>(B.bv[5 * sz + n], h);

@@ -135,3 +135,34 @@ def test_matches_reference_program(case_factory, name, steps):
         worst.update({f"b{b}/{n}": v for n, v in errs.items()})
     bad = {k: v for k, v in worst.items() if not v <= 1e-10}
     assert not bad, f"fields beyond 1e-10 vs the reference program: {bad}"
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_first_step_bit_identical_to_reference(case_factory, name):
+    """After one step every stored variable equals the reference program's
+    output bit for bit (same operation order, same rounding points)."""
+    fix = GOLDEN / f"{name}_s1.npz"
+    if not fix.exists():
+        pytest.skip(f"no reference fixture {fix.name}")
+    gold = np.load(fix)
+    gpu = ostc.Driver(make_case(case_factory, name, 1))
+    gpu.initialize()
+    gpu.step(1)
+    info = gpu.info()
+    names = [k.split("/", 1)[1] for k in gold.files if k.startswith("b0/")]
+    differ = []
+    for b in range(info.n_block):
+        bv, g = gpu.get(b, "bv"), info.ngg
+        cols = {"density": bv[0], "u": bv[1], "v": bv[2], "w": bv[3], "pressure": bv[4], "temperature": bv[5]}
+        if info.n_scalar:
+            sv = gpu.get(b, "sv")
+            sp = [n for n in names if n not in cols and n not in ("mach", "tke", "omega", "mut")]
+            for l, n in enumerate(sp):
+                cols[n] = sv[l]
+        for n, a in cols.items():
+            ref = gold[f"b{b}/{n}"]
+            same = interior(a, g) == ref
+            if not same.all():
+                differ.append(f"b{b}/{n}: {int((~same).sum())} of {same.size}")
+    assert not differ, differ
+
