@@ -69,6 +69,9 @@ struct DevBlock {
   double *chem_jac, *turb_src_jac;
   unsigned char *lu_piv;
   double *dq, *dq0, *dqk, *inv_spec, *visc_spec, *dt_local, *bv_last;
+  // species enthalpies h_k(T) of each cell, written by k_dq0 for the DPLUR
+  // sweeps (layout D, ns components; mixtures under DPLUR only)
+  double *h_spec;
 };
 
 // Work table of a launch: CTA-tiles of every block, in block order.

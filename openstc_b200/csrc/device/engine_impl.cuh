@@ -333,6 +333,15 @@ class EngineT final : public Engine {
       allocations_.push_back(q);
       ptr = static_cast<double *>(q);
     }
+    B.h_spec = nullptr;
+    if (C::mix != 0 && p.implicit_method == 1) {
+      void *q = nullptr;
+      const size_t bytes = sizeof(double) * static_cast<size_t>(B.D.size) * C::ns;
+      cuda_check(cudaMalloc(&q, bytes), "cudaMalloc h_spec");
+      cuda_check(cudaMemset(q, 0, bytes), "memset h_spec");
+      allocations_.push_back(q);
+      B.h_spec = static_cast<double *>(q);
+    }
     B.lu_piv = nullptr;
     if (C::mix == 2 && p.chem_src_method == 1) {
       void *q = nullptr;

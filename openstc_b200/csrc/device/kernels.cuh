@@ -229,11 +229,12 @@ __device__ __forceinline__ void chemistry(double density, double t, const double
 // ---------------------------------------------------------------- inviscid
 // reconstruction + AUSM+ face flux between the points n and n+s along
 // direction D, src/InviscidScheme.cuh:21-149, src/Reconstruction.cu:5-46.
-template <class C, int D>
-__device__ __forceinline__ void inviscid_face(const DevBlock &B, int64_t n, double *fc) {
+// The direction d (0 xi, 1 eta, 2 zeta) and its index stride s are run-time
+// values so that one copy of the face code serves all faces of a cell.
+template <class C>
+__device__ __forceinline__ void inviscid_face(const DevBlock &B, int64_t n, int d, int64_t s, double *fc) {
   constexpr int NV = C::nv, NS = C::ns;
   const int64_t sz = B.G.size;
-  const int64_t s = D == 0 ? 1 : (D == 1 ? B.G.sx : B.G.sxy);
   double pl[NV + 2], pr[NV + 2];
   const int rec = cP.reconstruction;
   OSTC_UNROLL for (int l = 0; l < NV; ++l) {
@@ -289,7 +290,7 @@ __device__ __forceinline__ void inviscid_face(const DevBlock &B, int64_t n, doub
     pl[NV] = el * pl[0] + pl[4] / (kDGammaAir - 1);
     pr[NV] = er * pr[0] + pr[4] / (kDGammaAir - 1);
   }
-  const double *m = B.metric + 3 * D * sz;
+  const double *m = B.metric + 3 * d * sz;
   const double jl = ld(B.jac + n), jr = ld(B.jac + n + s);
   const double k1 = 0.5 * (jl * ld(m + n) + jr * ld(m + n + s));
   const double k2 = 0.5 * (jl * ld(m + sz + n) + jr * ld(m + sz + n + s));
@@ -346,31 +347,32 @@ __device__ __forceinline__ void inviscid_face(const DevBlock &B, int64_t n, doub
 // ---------------------------------------------------------------- viscous
 // compute_{fv,gv,hv}_2nd_order, src/ViscousScheme.cuh:22-613, for the face
 // between n and n1 = n + e_D.
-template <int D>
-__device__ __forceinline__ void face_grad(const double *a, int64_t n, int64_t n1, int64_t sx, int64_t sxy, double &dxi,
-                                          double &deta, double &dzeta) {
-  if constexpr (D == 0) {
+// Derivatives along xi, eta, zeta at the face between n and n1 = n + e_d:
+// the face-normal one by a two-point difference, the others by the
+// four-point average.
+__device__ __forceinline__ void face_grad(const double *a, int64_t n, int64_t n1, int d, int64_t sx, int64_t sxy,
+                                          double &dxi, double &deta, double &dzeta) {
+  if (d == 0) {
     dxi = ld(a + n1) - ld(a + n);
   } else {
     dxi = 0.25 * (ld(a + n + 1) - ld(a + n - 1) + ld(a + n1 + 1) - ld(a + n1 - 1));
   }
-  if constexpr (D == 1) {
+  if (d == 1) {
     deta = ld(a + n1) - ld(a + n);
   } else {
     deta = 0.25 * (ld(a + n + sx) - ld(a + n - sx) + ld(a + n1 + sx) - ld(a + n1 - sx));
   }
-  if constexpr (D == 2) {
+  if (d == 2) {
     dzeta = ld(a + n1) - ld(a + n);
   } else {
     dzeta = 0.25 * (ld(a + n + sxy) - ld(a + n - sxy) + ld(a + n1 + sxy) - ld(a + n1 - sxy));
   }
 }
 
-template <class C, int D>
-__device__ __forceinline__ void viscous_face(const DevBlock &B, int64_t n, double *fv) {
+template <class C>
+__device__ __forceinline__ void viscous_face(const DevBlock &B, int64_t n, int d, int64_t s, double *fv) {
   constexpr int NS = C::ns;
   const int64_t sz = B.G.size, sx = B.G.sx, sxy = B.G.sxy;
-  const int64_t s = D == 0 ? 1 : (D == 1 ? sx : sxy);
   const int64_t n1 = n + s;
   const double *m = B.metric;
   const double xi_x = 0.5 * (ld(m + n) + ld(m + n1));
@@ -383,10 +385,10 @@ __device__ __forceinline__ void viscous_face(const DevBlock &B, int64_t n, doubl
   const double zeta_y = 0.5 * (ld(m + 7 * sz + n) + ld(m + 7 * sz + n1));
   const double zeta_z = 0.5 * (ld(m + 8 * sz + n) + ld(m + 8 * sz + n1));
   double u_xi, u_eta, u_zeta, v_xi, v_eta, v_zeta, w_xi, w_eta, w_zeta, t_xi, t_eta, t_zeta;
-  face_grad<D>(B.bv + sz, n, n1, sx, sxy, u_xi, u_eta, u_zeta);
-  face_grad<D>(B.bv + 2 * sz, n, n1, sx, sxy, v_xi, v_eta, v_zeta);
-  face_grad<D>(B.bv + 3 * sz, n, n1, sx, sxy, w_xi, w_eta, w_zeta);
-  face_grad<D>(B.bv + 5 * sz, n, n1, sx, sxy, t_xi, t_eta, t_zeta);
+  face_grad(B.bv + sz, n, n1, d, sx, sxy, u_xi, u_eta, u_zeta);
+  face_grad(B.bv + 2 * sz, n, n1, d, sx, sxy, v_xi, v_eta, v_zeta);
+  face_grad(B.bv + 3 * sz, n, n1, d, sx, sxy, w_xi, w_eta, w_zeta);
+  face_grad(B.bv + 5 * sz, n, n1, d, sx, sxy, t_xi, t_eta, t_zeta);
   const double u_x = u_xi * xi_x + u_eta * eta_x + u_zeta * zeta_x;
   const double u_y = u_xi * xi_y + u_eta * eta_y + u_zeta * zeta_y;
   const double u_z = u_xi * xi_z + u_eta * eta_z + u_zeta * zeta_z;
@@ -413,7 +415,7 @@ __device__ __forceinline__ void viscous_face(const DevBlock &B, int64_t n, doubl
     tau_yy += tt;
     tau_zz += tt;
   }
-  const double *mr = m + 3 * D * sz;
+  const double *mr = m + 3 * d * sz;
   const double ja = ld(B.jac + n), jb = ld(B.jac + n1);
   const double kx = 0.5 * (ld(mr + n) * ja + ld(mr + n1) * jb);
   const double ky = 0.5 * (ld(mr + sz + n) * ja + ld(mr + sz + n1) * jb);
@@ -441,7 +443,7 @@ __device__ __forceinline__ void viscous_face(const DevBlock &B, int64_t n, doubl
     OSTC_UNROLL for (int l = 0; l < NS; ++l) {
       dif[l] = 0.5 * (ld(B.rho_d + l * sz + n) + ld(B.rho_d + l * sz + n1)) + turb_d;
       double y_xi, y_eta, y_zeta;
-      face_grad<D>(B.sv + l * sz, n, n1, sx, sxy, y_xi, y_eta, y_zeta);
+      face_grad(B.sv + l * sz, n, n1, d, sx, sxy, y_xi, y_eta, y_zeta);
       yx[l] = y_xi * xi_x + y_eta * eta_x + y_zeta * zeta_x;
       yy[l] = y_xi * xi_y + y_eta * eta_y + y_zeta * zeta_y;
       yz[l] = y_xi * xi_z + y_eta * eta_z + y_zeta * zeta_z;
@@ -461,11 +463,11 @@ __device__ __forceinline__ void viscous_face(const DevBlock &B, int64_t n, doubl
   if constexpr (C::turb) {
     const double *tk = B.sv + NS * sz, *tw = B.sv + (NS + 1) * sz;
     double k_xi, k_eta, k_zeta, o_xi, o_eta, o_zeta;
-    face_grad<D>(tk, n, n1, sx, sxy, k_xi, k_eta, k_zeta);
+    face_grad(tk, n, n1, d, sx, sxy, k_xi, k_eta, k_zeta);
     const double k_x = k_xi * xi_x + k_eta * eta_x + k_zeta * zeta_x;
     const double k_y = k_xi * xi_y + k_eta * eta_y + k_zeta * zeta_y;
     const double k_z = k_xi * xi_z + k_eta * eta_z + k_zeta * zeta_z;
-    face_grad<D>(tw, n, n1, sx, sxy, o_xi, o_eta, o_zeta);
+    face_grad(tw, n, n1, d, sx, sxy, o_xi, o_eta, o_zeta);
     const double omega_x = o_xi * xi_x + o_eta * eta_x + o_zeta * zeta_x;
     const double omega_y = o_xi * xi_y + o_eta * eta_y + o_zeta * zeta_y;
     const double omega_z = o_xi * xi_z + o_eta * eta_z + o_zeta * zeta_z;

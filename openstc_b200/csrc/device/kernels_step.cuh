@@ -77,12 +77,22 @@ __global__ void __launch_bounds__(kCta) k_source(const DevBlock *__restrict__ bl
   OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq[l * szd + nd] = dq[l];
 }
 
+// Minimum resident CTAs per SM requested from the register allocator for the
+// two heaviest kernels (a tuning knob: more CTAs means fewer registers per
+// thread and possibly spills).
+#ifndef OSTC_FLUX_MIN_BLOCKS
+#define OSTC_FLUX_MIN_BLOCKS 4
+#endif
+#ifndef OSTC_SWEEP_MIN_BLOCKS
+#define OSTC_SWEEP_MIN_BLOCKS 4
+#endif
+
 // ---------------------------------------------------------------- fluxes
 // Inviscid (AUSM+/MUSCL) then viscous (central) flux differences in the
 // reference's accumulation order, plus local_time_step
 // (src/TimeAdvanceFunc.cuh:21-71).
 template <class C>
-__global__ void __launch_bounds__(kCta) k_flux(const DevBlock *__restrict__ blks, Tiles T) {
+__global__ void __launch_bounds__(kCta, OSTC_FLUX_MIN_BLOCKS) k_flux(const DevBlock *__restrict__ blks, Tiles T) {
   constexpr int NV = C::nv;
   extern __shared__ double sf[];
   int b, i, j, k;
@@ -95,54 +105,36 @@ __global__ void __launch_bounds__(kCta) k_flux(const DevBlock *__restrict__ blks
   const bool three_d = B.mz > 1;
   double dq[NV];
   OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] = B.dq[l * szd + nd];
-  double fp[NV];
-  // inviscid, i / j / k
-  {
+  // Inviscid faces, then viscous faces, each direction as minus face (staged
+  // in shared memory) then plus face: dq -= f(+) - f(-) for inviscid and
+  // dq += f(+) - f(-) for viscous, the reference's accumulation order.  The
+  // loops are not unrolled: one copy of each face routine keeps the kernel
+  // within the instruction cache.
+  const int n_face = three_d ? 6 : 4;
+#pragma unroll 1
+  for (int f = 0; f < n_face; ++f) {
+    const int d = f >> 1;
+    const int64_t s = d == 0 ? 1 : (d == 1 ? sx : sxy);
     double t[NV];
-    inviscid_face<C, 0>(B, n - 1, t);
-    OSTC_UNROLL for (int l = 0; l < NV; ++l) fm[l * kCta] = t[l];
-  }
-  inviscid_face<C, 0>(B, n, fp);
-  OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] -= fp[l] - fm[l * kCta];
-  {
-    double t[NV];
-    inviscid_face<C, 1>(B, n - sx, t);
-    OSTC_UNROLL for (int l = 0; l < NV; ++l) fm[l * kCta] = t[l];
-  }
-  inviscid_face<C, 1>(B, n, fp);
-  OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] -= fp[l] - fm[l * kCta];
-  if (three_d) {
-    {
-      double t[NV];
-      inviscid_face<C, 2>(B, n - sxy, t);
+    inviscid_face<C>(B, (f & 1) ? n : n - s, d, s, t);
+    if ((f & 1) == 0) {
       OSTC_UNROLL for (int l = 0; l < NV; ++l) fm[l * kCta] = t[l];
+    } else {
+      OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] -= t[l] - fm[l * kCta];
     }
-    inviscid_face<C, 2>(B, n, fp);
-    OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] -= fp[l] - fm[l * kCta];
   }
   if (cP.viscous_order != 0) {
-    {
+#pragma unroll 1
+    for (int f = 0; f < n_face; ++f) {
+      const int d = f >> 1;
+      const int64_t s = d == 0 ? 1 : (d == 1 ? sx : sxy);
       double t[NV];
-      viscous_face<C, 0>(B, n - 1, t);
-      OSTC_UNROLL for (int l = 0; l < NV; ++l) fm[l * kCta] = t[l];
-    }
-    viscous_face<C, 0>(B, n, fp);
-    OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] += fp[l] - fm[l * kCta];
-    {
-      double t[NV];
-      viscous_face<C, 1>(B, n - sx, t);
-      OSTC_UNROLL for (int l = 0; l < NV; ++l) fm[l * kCta] = t[l];
-    }
-    viscous_face<C, 1>(B, n, fp);
-    OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] += fp[l] - fm[l * kCta];
-    if (three_d) {
-      {
-        double t[NV];
-        viscous_face<C, 2>(B, n - sxy, t);
+      viscous_face<C>(B, (f & 1) ? n : n - s, d, s, t);
+      if ((f & 1) == 0) {
         OSTC_UNROLL for (int l = 0; l < NV; ++l) fm[l * kCta] = t[l];
+      } else {
+        OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] += t[l] - fm[l * kCta];
       }
-      viscous_face<C, 2>(B, n, fp);
-      OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] += fp[l] - fm[l * kCta];
     }
   }
   OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq[l * szd + nd] = dq[l];
@@ -289,6 +281,12 @@ __global__ void __launch_bounds__(kCta) k_dq0(const DevBlock *__restrict__ blks,
   const int64_t nd = B.D.at(i, j, k), nz = B.Z.at(i, j, k), szd = B.D.size, sz0 = B.Z.size;
   const double dt = B.dt_local[nz];
   const double diag = 1 + dt * (B.inv_spec[nd] + B.inv_spec[szd + nd] + B.inv_spec[2 * szd + nd]);
+  if constexpr (C::mix != 0) {
+    // T is fixed during the sweeps: evaluate the species enthalpies once
+    double hk[NS];
+    enthalpy<NS>(B.bv[5 * B.G.size + B.G.at(i, j, k)], hk);
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) B.h_spec[l * szd + nd] = hk[l];
+  }
   double dq[NV];
   OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] = B.dq[l * szd + nd];
   if constexpr (C::mix != 2) {
@@ -327,13 +325,14 @@ __global__ void __launch_bounds__(kCta) k_dq0(const DevBlock *__restrict__ blks,
 }
 
 // compute_jacobian_times_dq, src/DPLURHPP.cuh:78-125, accumulated into tot
-// with weight +-0.5 (sign < 0 subtracts).
-template <class C, int D>
+// with weight +-0.5 (sign < 0 subtracts), for the neighbour n along the
+// run-time direction dir.  The species enthalpies come from h_spec (k_dq0).
+template <class C>
 __device__ __forceinline__ void add_jac_dq(const DevBlock &B, const double *__restrict__ dqin, int64_t n,
-                                           int64_t nd, double pm_sr, bool subtract, double *tot) {
+                                           int64_t nd, int dir, double pm_sr, bool subtract, double *tot) {
   constexpr int NS = C::ns, NV = C::nv;
   const int64_t sz = B.G.size, szd = B.D.size;
-  const double *mr = B.metric + 3 * D * sz;
+  const double *mr = B.metric + 3 * dir * sz;
   const double xi_x = ld(mr + n), xi_y = ld(mr + sz + n), xi_z = ld(mr + 2 * sz + n);
   const double u = ld(B.bv + sz + n), v = ld(B.bv + 2 * sz + n), w = ld(B.bv + 3 * sz + n);
   const double U = xi_x * u + xi_y * v + xi_z * w;
@@ -346,7 +345,7 @@ __device__ __forceinline__ void add_jac_dq(const DevBlock &B, const double *__re
   if constexpr (C::mix != 0) {
     double hk[NS];
     const double t = ld(B.bv + 5 * sz + n);
-    enthalpy<NS>(t, hk);
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) hk[l] = ld(B.h_spec + l * szd + nd);
     gamma = ld(B.gamma + n);
     OSTC_UNROLL for (int l = 0; l < NS; ++l) {
       b3 += kDR_u * t / cP.mw[l] * d[5 + l];
@@ -378,7 +377,7 @@ __device__ __forceinline__ void add_jac_dq(const DevBlock &B, const double *__re
 // DPLUR_inner_iteration, src/DPLURHPP.cuh:127-249: dqout = dq0 + dt*sum/diag
 // with the neighbours' A(+-)*dqin; the point-implicit blocks reuse the LU.
 template <class C>
-__global__ void __launch_bounds__(kCta) k_sweep(const DevBlock *__restrict__ blks, Tiles T, int in_sel, int out_sel) {
+__global__ void __launch_bounds__(kCta, OSTC_SWEEP_MIN_BLOCKS) k_sweep(const DevBlock *__restrict__ blks, Tiles T, int in_sel, int out_sel) {
   constexpr int NS = C::ns, NV = C::nv;
   int b, i, j, k;
   if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
@@ -391,12 +390,20 @@ __global__ void __launch_bounds__(kCta) k_sweep(const DevBlock *__restrict__ blk
   double tot[NV];
   OSTC_UNROLL for (int l = 0; l < NV; ++l) tot[l] = 0;
   const double *isr = B.inv_spec;
-  if (i > 0) add_jac_dq<C, 0>(B, dqin, n - 1, nd - 1, isr[nd - 1], false, tot);
-  if (j > 0) add_jac_dq<C, 1>(B, dqin, n - sx, nd - dsx, isr[szd + nd - dsx], false, tot);
-  if (k > 0) add_jac_dq<C, 2>(B, dqin, n - sxy, nd - dsxy, isr[2 * szd + nd - dsxy], false, tot);
-  if (i != B.mx - 1) add_jac_dq<C, 0>(B, dqin, n + 1, nd + 1, -isr[nd + 1], true, tot);
-  if (j != B.my - 1) add_jac_dq<C, 1>(B, dqin, n + sx, nd + dsx, -isr[szd + nd + dsx], true, tot);
-  if (k != B.mz - 1) add_jac_dq<C, 2>(B, dqin, n + sxy, nd + dsxy, -isr[2 * szd + nd + dsxy], true, tot);
+  // neighbours i-1, j-1, k-1 (added with +lambda), then i+1, j+1, k+1
+  // (subtracted with -lambda); neighbours outside the block are skipped
+#pragma unroll 1
+  for (int q = 0; q < 6; ++q) {
+    const int d = q < 3 ? q : q - 3;
+    const bool plus = q >= 3;
+    const int id = d == 0 ? i : (d == 1 ? j : k);
+    const int ext = d == 0 ? B.mx : (d == 1 ? B.my : B.mz);
+    if (plus ? id == ext - 1 : id == 0) continue;
+    const int64_t gs = d == 0 ? 1 : (d == 1 ? sx : sxy), ds = d == 0 ? 1 : (d == 1 ? dsx : dsxy);
+    const int64_t on = plus ? n + gs : n - gs, od = plus ? nd + ds : nd - ds;
+    const double sr = isr[d * szd + od];
+    add_jac_dq<C>(B, dqin, on, od, d, plus ? -sr : sr, plus, tot);
+  }
   const double dt = B.dt_local[nz];
   const double diag = 1 + dt * (isr[nd] + isr[szd + nd] + isr[2 * szd + nd]);
   double out[NV];
