@@ -144,10 +144,21 @@ __device__ __forceinline__ double sst_mut(const DevBlock &B, int64_t n, double m
 }
 
 // ---------------------------------------------------------------- chemistry
-__device__ __forceinline__ double arrhenius(double t, double A, double b, double Ea) {
-  // src/FiniteRateChem.cu:110-112
-  return A * std::pow(t, b) * std::exp(-Ea / t);
+// A T^b exp(-Ea/T) evaluated as (A T^b) exp(-Ea/T), src/FiniteRateChem.cu:110-112.
+// pow(T, 0) and exp(-0/T) are exactly 1, so those calls are skipped without
+// changing a bit of the result.
+__device__ __forceinline__ double arrhenius_pow(double t, double A, double b) {
+  return b != 0 ? A * std::pow(t, b) : A;
 }
+
+__device__ __forceinline__ double arrhenius(double t, double A, double b, double Ea) {
+  const double ab = arrhenius_pow(t, A, b);
+  return Ea != 0 ? ab * std::exp(-Ea / t) : ab;
+}
+
+#ifndef OSTC_DUP_FMA
+#define OSTC_DUP_FMA 1
+#endif
 
 // finite_rate_chemistry, src/FiniteRateChem.cu:7-63 with the rate helpers
 // :65-171.  q1/q2 live in shared memory with stride `st` (CTA size).
@@ -164,7 +175,16 @@ __device__ __forceinline__ void chemistry(double density, double t, const double
   for (int r = 0; r < nr; ++r) {
     const int type = cP.label[r];
     double kf = arrhenius(t, cP.A[r], cP.b[r], cP.Ea[r]);
-    if (type == 3) kf += arrhenius(t, cP.A2[r], cP.b2[r], cP.Ea2[r]);
+    if (type == 3) {
+      // duplicate reaction: the reference adds the second rate in a new basic
+      // block, so only its last product can fuse into the sum
+#if OSTC_DUP_FMA
+      const double e2 = cP.Ea2[r] != 0 ? std::exp(-cP.Ea2[r] / t) : 1.0;
+      kf = __fma_rn(arrhenius_pow(t, cP.A2[r], cP.b2[r]), e2, kf);
+#else
+      kf = __dadd_rn(kf, arrhenius(t, cP.A2[r], cP.b2[r], cP.Ea2[r]));
+#endif
+    }
     if (type > 3) {
       double cc = 0;
       OSTC_UNROLL for (int l = 0; l < NS; ++l) cc += c[l] * cP.tb[r * NS + l];
