@@ -60,8 +60,12 @@ typedef enum ostc_phase {
 } ostc_phase;
 
 typedef struct ostc_options {
-  int device; /* CUDA device ordinal */
-  int quiet;  /* suppress the reference's screen output */
+  int device;    /* CUDA device ordinal */
+  int quiet;     /* suppress the reference's screen output */
+  int precision; /* 0: FP64, the reference's arithmetic; 1: FP32 fluxes, limiter, SST,
+                    flux Jacobians and transport, FP64 state, update, temperature
+                    inversion, chemistry, point-implicit solve and residual (finite-rate
+                    SST cases only) */
 } ostc_options;
 
 typedef struct ostc_info {

@@ -25,6 +25,7 @@ FIELDS = [
     "inv_spec", "visc_spec", "dt_local", "bv_last",
 ]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
+PRECISIONS = {"fp64": 0, "mixed": 1}
 PHASES = {"residual": 0, "implicit": 1, "update": 2, "bc": 3, "exchange": 4, "store": 5, "source": 6, "flux": 7}
 
 
@@ -33,7 +34,7 @@ class OstcError(RuntimeError):
 
 
 class Options(C.Structure):
-    _fields_ = [("device", C.c_int), ("quiet", C.c_int)]
+    _fields_ = [("device", C.c_int), ("quiet", C.c_int), ("precision", C.c_int)]
 
 
 class Info(C.Structure):
@@ -149,10 +150,15 @@ class Driver:
     ``step(n)`` n loop iterations without file output.
     """
 
-    def __init__(self, case_dir: str | Path, device: int = 0, quiet: bool = True):
+    def __init__(self, case_dir: str | Path, device: int = 0, quiet: bool = True, precision: str = "fp64"):
+        """precision: "fp64" (the reference's arithmetic) or "mixed" (FP32 fluxes,
+        limiter, SST, flux Jacobians and transport; FP64 state, update,
+        temperature inversion, chemistry, point-implicit solve, residual)."""
         lib = library()
         self._h = C.c_void_p()
-        opt = Options(device, 1 if quiet else 0)
+        if precision not in PRECISIONS:
+            raise OstcError(f"precision must be one of {sorted(PRECISIONS)}")
+        opt = Options(device, 1 if quiet else 0, PRECISIONS[precision])
         _check(lib.ostc_driver_create(str(case_dir).encode(), C.byref(opt), C.byref(self._h)))
         self.case_dir = Path(case_dir)
 

@@ -77,6 +77,7 @@ int ostc_driver_create(const char *case_dir, const ostc_options *opt, ostc_drive
     if (opt) {
       o.device = opt->device;
       o.quiet = opt->quiet != 0;
+      o.precision = opt->precision;
     }
     *out = new ostc_driver(case_dir, o);
     return OSTC_OK;

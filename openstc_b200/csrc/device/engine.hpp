@@ -42,6 +42,7 @@ struct EngineSetup {
   std::vector<HostInner> inner;   // application order
   std::vector<double> wall_points;  // x,y,z triples for the wall distance
   int device = 0;
+  int precision = 0;  // 0 FP64 (the reference's arithmetic), 1 FP32-bulk / FP64-critical
 };
 
 class Engine {
@@ -97,6 +98,7 @@ std::unique_ptr<Engine> make_engine_mix9_lam(const EngineSetup &);
 std::unique_ptr<Engine> make_engine_mix9_sst(const EngineSetup &);
 std::unique_ptr<Engine> make_engine_fr9_lam(const EngineSetup &);
 std::unique_ptr<Engine> make_engine_fr9_sst(const EngineSetup &);
+std::unique_ptr<Engine> make_engine_fr9_sst_mixed(const EngineSetup &);
 
 void cuda_check(int err, const char *what);
 

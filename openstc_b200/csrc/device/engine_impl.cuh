@@ -11,7 +11,7 @@
 #include <string>
 
 #include "engine.hpp"
-#include "kernels_step.cuh"
+#include "kernels_mixed.cuh"
 
 namespace ostc {
 
@@ -75,11 +75,17 @@ class EngineT final : public Engine {
                  "copy wall");
     }
     source_smem_ = C::mix == 2 ? 2 * std::max(1, s.params.nr) * kCta * sizeof(double) : 0;
-    flux_smem_ = C::nv * kCta * sizeof(double);
-    if (source_smem_ > 48 * 1024)
-      cuda_check(cudaFuncSetAttribute(k_source<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(source_smem_)),
-                 "smem attribute");
+    flux_smem_ = C::nv * kCta * (C::mixed ? sizeof(float) : sizeof(double));
+    if (source_smem_ > 48 * 1024) {
+      if constexpr (C::mixed)
+        cuda_check(cudaFuncSetAttribute(k_source_mx<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(source_smem_)),
+                   "smem attribute");
+      else
+        cuda_check(cudaFuncSetAttribute(k_source<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(source_smem_)),
+                   "smem attribute");
+    }
     cuda_check(cudaEventCreate(&ev0_), "event");
     cuda_check(cudaEventCreate(&ev1_), "event");
   }
@@ -134,7 +140,7 @@ class EngineT final : public Engine {
     k_cv_from_bv<C><<<grid(tilesg_), block3(), 0, stream_>>>(d_blocks_, tilesg_);
     if constexpr (C::turb) k_init_mut<C><<<grid(tiles1_), block3(), 0, stream_>>>(d_blocks_, tiles1_);
     launch_inner();
-    k_props<C><<<grid(tiles1_), block3(), 0, stream_>>>(d_blocks_, tiles1_);
+    launch_props();
     cuda_check(cudaGetLastError(), "initialize launch");
     cuda_check(cudaStreamSynchronize(stream_), "initialize");
   }
@@ -184,10 +190,10 @@ class EngineT final : public Engine {
         k_store_last<<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_);
         break;
       case 6:
-        k_source<C><<<grid(tiles0_), block3(), source_smem_, stream_>>>(d_blocks_, tiles0_);
+        launch_source();
         break;
       case 7:
-        k_flux<C><<<grid(tiles0_), block3(), flux_smem_, stream_>>>(d_blocks_, tiles0_);
+        launch_flux();
         break;
       default:
         throw std::runtime_error("unknown phase");
@@ -254,6 +260,10 @@ class EngineT final : public Engine {
     static const void *owner = nullptr;
     if (owner != this) {
       cuda_check(cudaMemcpyToSymbol(cP, &setup_.params, sizeof(DevParams)), "upload params");
+      if constexpr (C::mixed) {
+        const MixParams f = make_mix_params(setup_.params);
+        cuda_check(cudaMemcpyToSymbol(cF, &f, sizeof(MixParams)), "upload float params");
+      }
       owner = this;
     }
   }
@@ -386,10 +396,31 @@ class EngineT final : public Engine {
   static dim3 grid(const Tiles &t) { return dim3(static_cast<unsigned>(t.begin[t.nblk])); }
   static dim3 block3() { return dim3(kTX, kTY, kTZ); }
 
+  void launch_source() {
+    if constexpr (C::mixed)
+      k_source_mx<C><<<grid(tiles0_), block3(), source_smem_, stream_>>>(d_blocks_, tiles0_);
+    else
+      k_source<C><<<grid(tiles0_), block3(), source_smem_, stream_>>>(d_blocks_, tiles0_);
+  }
+
+  void launch_flux() {
+    if constexpr (C::mixed)
+      k_flux_mx<C><<<grid(tiles0_), block3(), flux_smem_, stream_>>>(d_blocks_, tiles0_);
+    else
+      k_flux<C><<<grid(tiles0_), block3(), flux_smem_, stream_>>>(d_blocks_, tiles0_);
+  }
+
+  void launch_props() {
+    if constexpr (C::mixed)
+      k_props_mx<C><<<grid(tiles1_), block3(), 0, stream_>>>(d_blocks_, tiles1_);
+    else
+      k_props<C><<<grid(tiles1_), block3(), 0, stream_>>>(d_blocks_, tiles1_);
+  }
+
   void launch_residual() {
-    k_source<C><<<grid(tiles0_), block3(), source_smem_, stream_>>>(d_blocks_, tiles0_);
+    launch_source();
     mark("source");
-    k_flux<C><<<grid(tiles0_), block3(), flux_smem_, stream_>>>(d_blocks_, tiles0_);
+    launch_flux();
     mark("flux");
   }
 
@@ -402,7 +433,10 @@ class EngineT final : public Engine {
       int in = 1;
       for (int s = 0; s < p.dplur_inner_step; ++s) {
         const int out = (s % 2 == 0) ? 2 : 0;
-        k_sweep<C><<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_, in, out);
+        if constexpr (C::mixed)
+          k_sweep_mx<C><<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_, in, out);
+        else
+          k_sweep<C><<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_, in, out);
         mark("dplur_sweep");
         in = out;
       }
@@ -457,7 +491,7 @@ class EngineT final : public Engine {
   void launch_exchange() {
     launch_inner();
     if (setup_.params.dim == 2) launch_kcopy();
-    k_props<C><<<grid(tiles1_), block3(), 0, stream_>>>(d_blocks_, tiles1_);
+    launch_props();
     mark("properties");
   }
 

@@ -1,0 +1,696 @@
+// FP32-bulk / FP64-critical kernels of the reacting-RANS step.
+//
+// Same discretisation and step structure as the FP64 kernels (and the
+// reference), with the precision split:
+//   FP32: reconstruction and limiter, mixture thermodynamics at faces, AUSM+
+//         and viscous fluxes, local time step, SST source, DPLUR flux-Jacobian
+//         products, transport properties (mu, lambda, rho D, cp, gamma, a);
+//   FP64: the state arrays and the conservative update accumulation, the
+//         temperature Newton inversion (k_update), the finite-rate chemistry
+//         with its equilibrium constants exp(-dG/RT) and reverse rates, the
+//         point-implicit (EPI) Jacobian and its LU solve, the residual norms.
+// Device arrays stay FP64 (one state for both paths); the FP32 kernels
+// convert on load and round their results back on store.
+#pragma once
+
+#include "kernels_step.cuh"
+
+namespace ostc {
+
+// Float copies of the tables the FP32 kernels read.
+struct MixParams {
+  float mw[kMaxSpec], mw_inv[kMaxSpec], ru_mw[kMaxSpec], t_low[kMaxSpec], t_mid[kMaxSpec];
+  float low[kMaxSpec * 7], high[kMaxSpec * 7];
+  float lj_inv[kMaxSpec], vis_coeff[kMaxSpec];
+  float wq[kMaxSpec * kMaxSpec], w8[kMaxSpec * kMaxSpec];
+  float cfl, Pr, Prt, Sct, Sc;
+};
+
+static __constant__ MixParams cF;
+
+inline MixParams make_mix_params(const DevParams &p) {
+  MixParams f{};
+  for (int i = 0; i < kMaxSpec; ++i) {
+    f.mw[i] = static_cast<float>(p.mw[i]);
+    f.mw_inv[i] = p.mw[i] != 0 ? static_cast<float>(1.0 / p.mw[i]) : 0.f;
+    f.ru_mw[i] = static_cast<float>(p.ru_mw[i]);
+    f.t_low[i] = static_cast<float>(p.t_low[i]);
+    f.t_mid[i] = static_cast<float>(p.t_mid[i]);
+    f.lj_inv[i] = static_cast<float>(p.lj_inv[i]);
+    f.vis_coeff[i] = static_cast<float>(p.vis_coeff[i]);
+  }
+  for (int i = 0; i < kMaxSpec * 7; ++i) {
+    f.low[i] = static_cast<float>(p.low[i]);
+    f.high[i] = static_cast<float>(p.high[i]);
+  }
+  for (int i = 0; i < kMaxSpec * kMaxSpec; ++i) {
+    f.wq[i] = static_cast<float>(p.wq[i]);
+    f.w8[i] = static_cast<float>(p.w8[i]);
+  }
+  f.cfl = static_cast<float>(p.cfl);
+  f.Pr = static_cast<float>(p.Pr);
+  f.Prt = static_cast<float>(p.Prt);
+  f.Sct = static_cast<float>(p.Sct);
+  f.Sc = static_cast<float>(p.Sc);
+  return f;
+}
+
+namespace fp32 {
+
+constexpr float kRu = 8314.462618f;
+
+__device__ __forceinline__ float ldf(const double *p) { return static_cast<float>(__ldg(p)); }
+
+__device__ __forceinline__ float minmod(float a, float b) {
+  return 0.5f * ((a < 0 ? -1.f : 1.f) + (b < 0 ? -1.f : 1.f)) * fminf(fabsf(a), fabsf(b));
+}
+
+// NASA-7 polynomial coefficient q of species i (two ranges)
+__device__ __forceinline__ float nasa(int i, int q, bool lowrange) {
+  return lowrange ? cF.low[i * 7 + q] : cF.high[i * 7 + q];
+}
+
+// Species h_k and cp_k (J/kg, J/kg/K) at t; below T_low h is extrapolated
+// linearly with cp frozen, as in the FP64 path.
+template <int NS, bool WANT_H, bool WANT_CP>
+__device__ __forceinline__ void thermo(float t, float *h, float *cp) {
+  OSTC_UNROLL for (int i = 0; i < NS; ++i) {
+    const bool below = t < cF.t_low[i];
+    const float tt = below ? cF.t_low[i] : t;
+    const bool lo = below || tt < cF.t_mid[i];
+    const float c0 = nasa(i, 0, lo), c1 = nasa(i, 1, lo), c2 = nasa(i, 2, lo), c3 = nasa(i, 3, lo),
+                c4 = nasa(i, 4, lo);
+    const float c = c0 + tt * (c1 + tt * (c2 + tt * (c3 + tt * c4)));
+    if constexpr (WANT_H) {
+      float hh = tt * (c0 + tt * (0.5f * c1 + tt * (c2 * (1.f / 3.f) + tt * (0.25f * c3 + tt * (0.2f * c4))))) +
+                 nasa(i, 5, lo);
+      if (below) hh += c * (t - tt);
+      h[i] = hh * cF.ru_mw[i];
+    }
+    if constexpr (WANT_CP) cp[i] = c * cF.ru_mw[i];
+  }
+}
+
+// ------------------------------------------------------------ inviscid face
+template <class C>
+__device__ __forceinline__ void inviscid_face(const DevBlock &B, int64_t n, int d, int64_t s, float *fc) {
+  constexpr int NV = C::nv, NS = C::ns;
+  const int64_t sz = B.G.size;
+  float pl[NV + 2], pr[NV + 2];
+  const int rec = cP.reconstruction;
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) {
+    const double *a = l < 5 ? B.bv + l * sz : B.sv + (l - 5) * sz;
+    const float p0 = ldf(a + n), p1 = ldf(a + n + s);
+    if (rec == 2 || rec == 3) {
+      const float pm = ldf(a + n - s), p2 = ldf(a + n + 2 * s);
+      const float d_i = p0 - pm, d_i1 = p1 - p0, d_i2 = p2 - p1;
+      if (rec == 2) {
+        const float neg_l = minmod(d_i, d_i1), pos_l = minmod(d_i1, d_i);
+        const float neg_r = minmod(d_i1, d_i2), pos_r = minmod(d_i2, d_i1);
+        pl[l] = p0 + 0.25f * ((2.f / 3.f) * neg_l + (4.f / 3.f) * pos_l);
+        pr[l] = p1 - 0.25f * ((2.f / 3.f) * pos_r + (4.f / 3.f) * neg_r);
+      } else {
+        pl[l] = p0 + 0.5f * minmod(d_i, d_i1);
+        pr[l] = p1 - 0.5f * minmod(d_i1, d_i2);
+      }
+    } else {
+      pl[l] = p0;
+      pr[l] = p1;
+    }
+  }
+  float el = 0.5f * (pl[1] * pl[1] + pl[2] * pl[2] + pl[3] * pl[3]);
+  float er = 0.5f * (pr[1] * pr[1] + pr[2] * pr[2] + pr[3] * pr[3]);
+  if constexpr (C::mix != 0) {
+    float mwl = 0, mwr = 0;
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) {
+      mwl += pl[5 + l] * cF.mw_inv[l];
+      mwr += pr[5 + l] * cF.mw_inv[l];
+    }
+    const float tl = pl[4] / (pl[0] * kRu * mwl);
+    const float tr = pr[4] / (pr[0] * kRu * mwr);
+    float hl[NS], hr[NS], cpl_i[NS], cpr_i[NS];
+    thermo<NS, true, true>(tl, hl, cpl_i);
+    thermo<NS, true, true>(tr, hr, cpr_i);
+    float cpl = 0, cpr = 0, cvl = 0, cvr = 0;
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) {
+      cpl += cpl_i[l] * pl[l + 5];
+      cpr += cpr_i[l] * pr[l + 5];
+      cvl += pl[l + 5] * (cpl_i[l] - cF.ru_mw[l]);
+      cvr += pr[l + 5] * (cpr_i[l] - cF.ru_mw[l]);
+      el += hl[l] * pl[l + 5];
+      er += hr[l] * pr[l + 5];
+    }
+    pl[NV] = pl[0] * el - pl[4];
+    pr[NV] = pr[0] * er - pr[4];
+    pl[NV + 1] = cpl / cvl;
+    pr[NV + 1] = cpr / cvr;
+  } else {
+    constexpr float g1 = 1.f / (1.4f - 1.f);
+    pl[NV] = el * pl[0] + pl[4] * g1;
+    pr[NV] = er * pr[0] + pr[4] * g1;
+    pl[NV + 1] = 1.4f;
+    pr[NV + 1] = 1.4f;
+  }
+  const double *m = B.metric + 3 * d * sz;
+  const float jl = ldf(B.jac + n), jr = ldf(B.jac + n + s);
+  const float k1 = 0.5f * (jl * ldf(m + n) + jr * ldf(m + n + s));
+  const float k2 = 0.5f * (jl * ldf(m + sz + n) + jr * ldf(m + sz + n + s));
+  const float k3 = 0.5f * (jl * ldf(m + 2 * sz + n) + jr * ldf(m + 2 * sz + n + s));
+  const float gk = sqrtf(k1 * k1 + k2 * k2 + k3 * k3);
+  const float inv_gk = 1.f / gk;
+  const float ul = (k1 * pl[1] + k2 * pl[2] + k3 * pl[3]) * inv_gk;
+  const float ur = (k1 * pr[1] + k2 * pr[2] + k3 * pr[3]) * inv_gk;
+  const float p_l = pl[4], p_r = pr[4], rho_l = pl[0], rho_r = pr[0];
+  const float c = 0.5f * (sqrtf(pl[NV + 1] * p_l / rho_l) + sqrtf(pr[NV + 1] * p_r / rho_r));
+  const float inv_c = 1.f / c;
+  const float mach_l = ul * inv_c, mach_r = ur * inv_c;
+  float mlp, mrn, plp, prn;
+  constexpr float alpha = 3.f / 16.f;
+  if (fabsf(mach_l) > 1) {
+    mlp = 0.5f * (mach_l + fabsf(mach_l));
+    plp = mlp / mach_l;
+  } else {
+    const float a = (mach_l + 1) * (mach_l + 1) * 0.25f;
+    const float b = (mach_l * mach_l - 1) * (mach_l * mach_l - 1);
+    mlp = a + 0.125f * b;
+    plp = a * (2 - mach_l) + alpha * mach_l * b;
+  }
+  if (fabsf(mach_r) > 1) {
+    mrn = 0.5f * (mach_r - fabsf(mach_r));
+    prn = mrn / mach_r;
+  } else {
+    const float a = (mach_r - 1) * (mach_r - 1) * 0.25f;
+    const float b = (mach_r * mach_r - 1) * (mach_r * mach_r - 1);
+    mrn = -a - 0.125f * b;
+    prn = a * (2 + mach_r) - alpha * mach_r * b;
+  }
+  const float p_coeff = plp * p_l + prn * p_r;
+  const float m_half = mlp + mrn;
+  const float mach_pos = 0.5f * (m_half + fabsf(m_half));
+  const float mach_neg = 0.5f * (m_half - fabsf(m_half));
+  const float mass_flux_half = c * (rho_l * mach_pos + rho_r * mach_neg);
+  const float coeff = mass_flux_half * gk;
+  const bool up = mass_flux_half >= 0;
+  const float *q = up ? pl : pr;
+  fc[0] = coeff;
+  fc[1] = coeff * q[1] + p_coeff * k1;
+  fc[2] = coeff * q[2] + p_coeff * k2;
+  fc[3] = coeff * q[3] + p_coeff * k3;
+  fc[4] = coeff * (q[NV] + q[4]) / q[0];
+  OSTC_UNROLL for (int l = 5; l < NV; ++l) fc[l] = coeff * q[l];
+}
+
+// ------------------------------------------------------------- viscous face
+__device__ __forceinline__ void face_grad(const double *a, int64_t n, int64_t n1, int d, int64_t sx, int64_t sxy,
+                                          float &dxi, float &deta, float &dzeta) {
+  dxi = d == 0 ? ldf(a + n1) - ldf(a + n)
+               : 0.25f * (ldf(a + n + 1) - ldf(a + n - 1) + ldf(a + n1 + 1) - ldf(a + n1 - 1));
+  deta = d == 1 ? ldf(a + n1) - ldf(a + n)
+                : 0.25f * (ldf(a + n + sx) - ldf(a + n - sx) + ldf(a + n1 + sx) - ldf(a + n1 - sx));
+  dzeta = d == 2 ? ldf(a + n1) - ldf(a + n)
+                 : 0.25f * (ldf(a + n + sxy) - ldf(a + n - sxy) + ldf(a + n1 + sxy) - ldf(a + n1 - sxy));
+}
+
+template <class C>
+__device__ __forceinline__ void viscous_face(const DevBlock &B, int64_t n, int d, int64_t s, float *fv) {
+  constexpr int NS = C::ns;
+  const int64_t sz = B.G.size, sx = B.G.sx, sxy = B.G.sxy;
+  const int64_t n1 = n + s;
+  const double *m = B.metric;
+  float mm[9];
+  OSTC_UNROLL for (int q = 0; q < 9; ++q) mm[q] = 0.5f * (ldf(m + q * sz + n) + ldf(m + q * sz + n1));
+  const float xi_x = mm[0], xi_y = mm[1], xi_z = mm[2], eta_x = mm[3], eta_y = mm[4], eta_z = mm[5];
+  const float zeta_x = mm[6], zeta_y = mm[7], zeta_z = mm[8];
+  auto cart = [&](float a_xi, float a_eta, float a_zeta, float &ax, float &ay, float &az) {
+    ax = a_xi * xi_x + a_eta * eta_x + a_zeta * zeta_x;
+    ay = a_xi * xi_y + a_eta * eta_y + a_zeta * zeta_y;
+    az = a_xi * xi_z + a_eta * eta_z + a_zeta * zeta_z;
+  };
+  float g0, g1, g2;
+  float u_x, u_y, u_z, v_x, v_y, v_z, w_x, w_y, w_z, t_x, t_y, t_z;
+  face_grad(B.bv + sz, n, n1, d, sx, sxy, g0, g1, g2);
+  cart(g0, g1, g2, u_x, u_y, u_z);
+  face_grad(B.bv + 2 * sz, n, n1, d, sx, sxy, g0, g1, g2);
+  cart(g0, g1, g2, v_x, v_y, v_z);
+  face_grad(B.bv + 3 * sz, n, n1, d, sx, sxy, g0, g1, g2);
+  cart(g0, g1, g2, w_x, w_y, w_z);
+  face_grad(B.bv + 5 * sz, n, n1, d, sx, sxy, g0, g1, g2);
+  cart(g0, g1, g2, t_x, t_y, t_z);
+  const float mul = 0.5f * (ldf(B.mul + n) + ldf(B.mul + n1));
+  float mut = 0;
+  if constexpr (C::turb) mut = 0.5f * (ldf(B.mut + n) + ldf(B.mut + n1));
+  const float viscosity = mul + mut;
+  constexpr float third = 1.f / 3.f;
+  float tau_xx = viscosity * (4 * u_x - 2 * v_y - 2 * w_z) * third;
+  float tau_yy = viscosity * (4 * v_y - 2 * u_x - 2 * w_z) * third;
+  float tau_zz = viscosity * (4 * w_z - 2 * u_x - 2 * v_y) * third;
+  const float tau_xy = viscosity * (u_y + v_x);
+  const float tau_xz = viscosity * (u_z + w_x);
+  const float tau_yz = viscosity * (v_z + w_y);
+  if constexpr (C::turb) {
+    const float tt = -(1.f / 3.f) * (ldf(B.bv + n) * ldf(B.sv + NS * sz + n) + ldf(B.bv + n1) * ldf(B.sv + NS * sz + n1));
+    tau_xx += tt;
+    tau_yy += tt;
+    tau_zz += tt;
+  }
+  const double *mr = m + 3 * d * sz;
+  const float ja = ldf(B.jac + n), jb = ldf(B.jac + n1);
+  const float kx = 0.5f * (ldf(mr + n) * ja + ldf(mr + n1) * jb);
+  const float ky = 0.5f * (ldf(mr + sz + n) * ja + ldf(mr + sz + n1) * jb);
+  const float kz = 0.5f * (ldf(mr + 2 * sz + n) * ja + ldf(mr + 2 * sz + n1) * jb);
+  fv[0] = 0;
+  fv[1] = kx * tau_xx + ky * tau_xy + kz * tau_xz;
+  fv[2] = kx * tau_xy + ky * tau_yy + kz * tau_yz;
+  fv[3] = kx * tau_xz + ky * tau_yz + kz * tau_zz;
+  const float um = 0.5f * (ldf(B.bv + sz + n) + ldf(B.bv + sz + n1));
+  const float vm = 0.5f * (ldf(B.bv + 2 * sz + n) + ldf(B.bv + 2 * sz + n1));
+  const float wm = 0.5f * (ldf(B.bv + 3 * sz + n) + ldf(B.bv + 3 * sz + n1));
+  float conductivity = 0.5f * (ldf(B.cond + n) + ldf(B.cond + n1));
+  if constexpr (C::turb) conductivity += 0.5f * (ldf(B.turb_cond + n) + ldf(B.turb_cond + n1));
+  fv[4] = um * fv[1] + vm * fv[2] + wm * fv[3] + conductivity * (kx * t_x + ky * t_y + kz * t_z);
+  if constexpr (C::mix != 0) {
+    float turb_d = 0;
+    if constexpr (C::turb) turb_d = mut / cF.Sct;
+    float h[NS], dif[NS], yx[NS], yy[NS], yz[NS];
+    const float tm = 0.5f * (ldf(B.bv + 5 * sz + n) + ldf(B.bv + 5 * sz + n1));
+    thermo<NS, true, false>(tm, h, nullptr);
+    float rho_uc = 0, rho_vc = 0, rho_wc = 0, hflux = 0;
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) {
+      dif[l] = 0.5f * (ldf(B.rho_d + l * sz + n) + ldf(B.rho_d + l * sz + n1)) + turb_d;
+      face_grad(B.sv + l * sz, n, n1, d, sx, sxy, g0, g1, g2);
+      cart(g0, g1, g2, yx[l], yy[l], yz[l]);
+      hflux += dif[l] * h[l] * (kx * yx[l] + ky * yy[l] + kz * yz[l]);
+      rho_uc += dif[l] * yx[l];
+      rho_vc += dif[l] * yy[l];
+      rho_wc += dif[l] * yz[l];
+    }
+    fv[4] += hflux;
+    const float corr = kx * rho_uc + ky * rho_vc + kz * rho_wc;
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) {
+      fv[5 + l] = dif[l] * (kx * yx[l] + ky * yy[l] + kz * yz[l]) -
+                  0.5f * (ldf(B.sv + l * sz + n) + ldf(B.sv + l * sz + n1)) * corr;
+    }
+  }
+  if constexpr (C::turb) {
+    const double *tk = B.sv + NS * sz, *tw = B.sv + (NS + 1) * sz;
+    float k_x, k_y, k_z, o_x, o_y, o_z;
+    face_grad(tk, n, n1, d, sx, sxy, g0, g1, g2);
+    cart(g0, g1, g2, k_x, k_y, k_z);
+    face_grad(tw, n, n1, d, sx, sxy, g0, g1, g2);
+    cart(g0, g1, g2, o_x, o_y, o_z);
+    const float wall_dist = 0.5f * (ldf(B.wall_dist + n) + ldf(B.wall_dist + n1));
+    float f1 = 1;
+    if (wall_dist > 1e-25f) {
+      const float km = 0.5f * (ldf(tk + n) + ldf(tk + n1));
+      const float omegam = 0.5f * (ldf(tw + n) + ldf(tw + n1));
+      const float param1 = sqrtf(km) / (0.09f * omegam * wall_dist);
+      const float rhom = 0.5f * (ldf(B.bv + n) + ldf(B.bv + n1));
+      const float d2 = wall_dist * wall_dist;
+      const float param2 = 500 * mul / (rhom * d2 * omegam);
+      constexpr float so2 = static_cast<float>(sst::sigma_omega2);
+      const float CDkomega = fmaxf(1e-20f, 2 * rhom * so2 / omegam * (k_x * o_x + k_y * o_y + k_z * o_z));
+      const float param3 = 4 * rhom * so2 * km / (CDkomega * d2);
+      const float arg1 = fminf(fmaxf(param1, param2), param3);
+      f1 = tanhf(arg1 * arg1 * arg1 * arg1);
+    }
+    const float sigma_k = static_cast<float>(sst::sigma_k2) + static_cast<float>(sst::delta_sigma_k) * f1;
+    const float sigma_omega =
+        static_cast<float>(sst::sigma_omega2) + static_cast<float>(sst::delta_sigma_omega) * f1;
+    fv[5 + NS] = (mul + mut * sigma_k) * (kx * k_x + ky * k_y + kz * k_z);
+    fv[6 + NS] = (mul + mut * sigma_omega) * (kx * o_x + ky * o_y + kz * o_z);
+  }
+}
+
+// ------------------------------------------------------------- SST source
+template <class C>
+__device__ __forceinline__ void sst_source(const DevBlock &B, int64_t n, double &src_k, double &src_w,
+                                           double &mut_out, double &jk, double &jw) {
+  constexpr int NS = C::ns;
+  const int64_t sz = B.G.size, sx = B.G.sx, sxy = B.G.sxy;
+  const double *m = B.metric;
+  const float xi_x = ldf(m + n), xi_y = ldf(m + sz + n), xi_z = ldf(m + 2 * sz + n);
+  const float eta_x = ldf(m + 3 * sz + n), eta_y = ldf(m + 4 * sz + n), eta_z = ldf(m + 5 * sz + n);
+  const float zeta_x = ldf(m + 6 * sz + n), zeta_y = ldf(m + 7 * sz + n), zeta_z = ldf(m + 8 * sz + n);
+  auto cgrad = [&](const double *a, float &gx, float &gy, float &gz) {
+    const float a_xi = ldf(a + n + 1) - ldf(a + n - 1), a_eta = ldf(a + n + sx) - ldf(a + n - sx),
+                a_zeta = ldf(a + n + sxy) - ldf(a + n - sxy);
+    gx = 0.5f * (xi_x * a_xi + eta_x * a_eta + zeta_x * a_zeta);
+    gy = 0.5f * (xi_y * a_xi + eta_y * a_eta + zeta_y * a_zeta);
+    gz = 0.5f * (xi_z * a_xi + eta_z * a_eta + zeta_z * a_zeta);
+  };
+  float u_x, u_y, u_z, v_x, v_y, v_z, w_x, w_y, w_z, k_x, k_y, k_z, o_x, o_y, o_z;
+  cgrad(B.bv + sz, u_x, u_y, u_z);
+  cgrad(B.bv + 2 * sz, v_x, v_y, v_z);
+  cgrad(B.bv + 3 * sz, w_x, w_y, w_z);
+  const double *tk = B.sv + NS * sz, *tw = B.sv + (NS + 1) * sz;
+  cgrad(tk, k_x, k_y, k_z);
+  cgrad(tw, o_x, o_y, o_z);
+  const float density = ldf(B.bv + n), omega = ldf(tw + n), tke = ldf(tk + n);
+  constexpr float so2 = static_cast<float>(sst::sigma_omega2), a1 = static_cast<float>(sst::a_1);
+  const float inter_var = 2 * density * so2 / omega * (k_x * o_x + k_y * o_y + k_z * o_z);
+  const float rhoK = density * tke;
+  const float vorticity =
+      sqrtf((v_x - u_y) * (v_x - u_y) + (w_x - u_z) * (w_x - u_z) + (w_y - v_z) * (w_y - v_z));
+  float f1 = 1, f2 = 1;
+  const float dy = ldf(B.wall_dist + n);
+  if (dy > 1e-25f) {
+    const float param1 = sqrtf(tke) / (0.09f * omega * dy);
+    const float d2 = dy * dy;
+    const float param2 = 500 * ldf(B.mul + n) / (density * d2 * omega);
+    const float arg2 = fmaxf(2 * param1, param2);
+    f2 = tanhf(arg2 * arg2);
+    const float CDkomega = fmaxf(1e-20f, inter_var);
+    const float param3 = 4 * density * so2 * tke / (CDkomega * d2);
+    const float arg1 = fminf(fmaxf(param1, param2), param3);
+    f1 = tanhf(arg1 * arg1 * arg1 * arg1);
+  }
+  float mut = 0;
+  if (const float den = fmaxf(a1 * omega, vorticity * f2); den > 1e-25f) mut = a1 * rhoK / den;
+  mut_out = mut;
+  const float beta = static_cast<float>(sst::beta_2) + static_cast<float>(sst::delta_beta) * f1;
+  src_k = 0;
+  src_w = 0;
+  if (mut > 1e-25f) {
+    const float divU = u_x + v_y + w_z;
+    const float prod_k = mut * (2 * (u_x * u_x + v_y * v_y + w_z * w_z) - (2.f / 3.f) * divU * divU +
+                                (u_y + v_x) * (u_y + v_x) + (u_z + w_x) * (u_z + w_x) + (v_z + w_y) * (v_z + w_y)) -
+                         (2.f / 3.f) * rhoK * divU;
+    const float diss_k = static_cast<float>(sst::beta_star) * rhoK * omega;
+    const float jac = ldf(B.jac + n);
+    src_k = jac * (prod_k - diss_k);
+    const float gamma = static_cast<float>(sst::gamma2) + static_cast<float>(sst::delta_gamma) * f1;
+    const float prod_omega = gamma * density / mut * prod_k + (1 - f1) * inter_var;
+    const float diss_omega = beta * density * omega * omega;
+    src_w = jac * (prod_omega - diss_omega);
+  }
+  jk = -2 * sst::beta_star * omega;
+  jw = -2.0 * beta * omega;
+}
+
+}  // namespace fp32
+
+// dq = source terms: SST in FP32, finite-rate chemistry and its EPI Jacobian
+// in FP64 (the same code as the FP64 path).
+template <class C>
+__global__ void __launch_bounds__(kCta) k_source_mx(const DevBlock *__restrict__ blks, Tiles T) {
+  constexpr int NS = C::ns, NV = C::nv;
+  extern __shared__ double sq[];
+  int b, i, j, k;
+  if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
+  const DevBlock &B = blks[b];
+  const int64_t n = B.G.at(i, j, k), nd = B.D.at(i, j, k), nz = B.Z.at(i, j, k);
+  const int64_t sz = B.G.size, szd = B.D.size, sz0 = B.Z.size;
+  double dq[NV];
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] = 0;
+  if constexpr (C::turb) {
+    double sk, sw, mut, jk, jw;
+    fp32::sst_source<C>(B, n, sk, sw, mut, jk, jw);
+    B.mut[n] = mut;
+    dq[NS + 5] = sk;
+    dq[NS + 6] = sw;
+    if (cP.turb_implicit == 1) {
+      B.turb_src_jac[nz] = jk;
+      B.turb_src_jac[sz0 + nz] = jw;
+    }
+    B.turb_cond[n] = static_cast<float>(mut) * fp32::ldf(B.cp + n) / cF.Prt;
+  }
+  if constexpr (C::mix == 2) {
+    const int tid = threadIdx.x + kTX * (threadIdx.y + kTY * threadIdx.z);
+    double *q1 = sq + tid, *q2 = sq + cP.nr * kCta + tid;
+    double Y[NS], omega[NS], omega_d[NS];
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) Y[l] = ld(B.sv + l * sz + n);
+    const double density = ld(B.bv + n), t = ld(B.bv + 5 * sz + n);
+    chemistry<NS>(density, t, Y, omega, omega_d, q1, q2, kCta);
+    const double jac = ld(B.jac + n);
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) dq[l + 5] = jac * omega[l];
+    const int method = cP.chem_src_method;
+    if (method == 1) {
+      const int nr = cP.nr;
+      OSTC_UNROLL for (int m = 0; m < NS; ++m) {
+        OSTC_UNROLL for (int q = 0; q < NS; ++q) {
+          double zz = 0;
+          if (Y[q] > 1e-25) {
+            for (int r = 0; r < nr; ++r) {
+              const int dn = cP.sb[r * NS + m] - cP.sf[r * NS + m];
+              if (dn == 0) continue;
+              zz += dn * (cP.sf[r * NS + q] * q1[r * kCta] - cP.sb[r * NS + q] * q2[r * kCta]);
+            }
+            zz /= density * Y[q];
+          }
+          B.chem_jac[(m * NS + q) * sz0 + nz] = cP.mw[m] * zz * 1e+3;
+        }
+      }
+    } else if (method == 2) {
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) {
+        double v = 0;
+        if (Y[l] > 1e-25) v = -omega_d[l] / (Y[l] * density);
+        B.chem_jac[l * sz0 + nz] = v;
+      }
+    }
+  }
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq[l * szd + nd] = dq[l];
+}
+
+// Inviscid + viscous flux differences in FP32 (accumulated in FP32 and added
+// to the FP64 source terms), then the local time step.
+template <class C>
+__global__ void __launch_bounds__(kCta, 4) k_flux_mx(const DevBlock *__restrict__ blks, Tiles T) {
+  constexpr int NV = C::nv;
+  extern __shared__ float sfm[];
+  int b, i, j, k;
+  if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
+  const DevBlock &B = blks[b];
+  const int tid = threadIdx.x + kTX * (threadIdx.y + kTY * threadIdx.z);
+  float *fm = sfm + tid;
+  const int64_t n = B.G.at(i, j, k), nd = B.D.at(i, j, k), szd = B.D.size;
+  const int64_t sx = B.G.sx, sxy = B.G.sxy;
+  const bool three_d = B.mz > 1;
+  float acc[NV];
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) acc[l] = 0;
+  const int n_face = three_d ? 6 : 4;
+#pragma unroll 1
+  for (int f = 0; f < n_face; ++f) {
+    const int d = f >> 1;
+    const int64_t s = d == 0 ? 1 : (d == 1 ? sx : sxy);
+    float t[NV];
+    fp32::inviscid_face<C>(B, (f & 1) ? n : n - s, d, s, t);
+    if ((f & 1) == 0) {
+      OSTC_UNROLL for (int l = 0; l < NV; ++l) fm[l * kCta] = t[l];
+    } else {
+      OSTC_UNROLL for (int l = 0; l < NV; ++l) acc[l] -= t[l] - fm[l * kCta];
+    }
+  }
+  if (cP.viscous_order != 0) {
+#pragma unroll 1
+    for (int f = 0; f < n_face; ++f) {
+      const int d = f >> 1;
+      const int64_t s = d == 0 ? 1 : (d == 1 ? sx : sxy);
+      float t[NV];
+      fp32::viscous_face<C>(B, (f & 1) ? n : n - s, d, s, t);
+      if ((f & 1) == 0) {
+        OSTC_UNROLL for (int l = 0; l < NV; ++l) fm[l * kCta] = t[l];
+      } else {
+        OSTC_UNROLL for (int l = 0; l < NV; ++l) acc[l] += t[l] - fm[l * kCta];
+      }
+    }
+  }
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq[l * szd + nd] += static_cast<double>(acc[l]);
+
+  const int64_t sz = B.G.size;
+  const double *m = B.metric;
+  using fp32::ldf;
+  const float m11 = ldf(m + n), m12 = ldf(m + sz + n), m13 = ldf(m + 2 * sz + n);
+  const float m21 = ldf(m + 3 * sz + n), m22 = ldf(m + 4 * sz + n), m23 = ldf(m + 5 * sz + n);
+  const float m31 = ldf(m + 6 * sz + n), m32 = ldf(m + 7 * sz + n), m33 = ldf(m + 8 * sz + n);
+  const float grad_xi = sqrtf(m11 * m11 + m12 * m12 + m13 * m13);
+  const float grad_eta = sqrtf(m21 * m21 + m22 * m22 + m23 * m23);
+  const float grad_zeta = sqrtf(m31 * m31 + m32 * m32 + m33 * m33);
+  const float u = ldf(B.bv + sz + n), v = ldf(B.bv + 2 * sz + n), w = ldf(B.bv + 3 * sz + n);
+  const float a = ldf(B.acoustic + n);
+  const float s0 = fabsf(u * m11 + v * m12 + w * m13) + a * grad_xi;
+  const float s1 = fabsf(u * m21 + v * m22 + w * m23) + a * grad_eta;
+  const float s2 = three_d ? fabsf(u * m31 + v * m32 + w * m33) + a * grad_zeta : 0.f;
+  B.inv_spec[nd] = s0;
+  B.inv_spec[szd + nd] = s1;
+  B.inv_spec[2 * szd + nd] = s2;
+  float gamma = 1.4f;
+  if constexpr (C::mix != 0) gamma = ldf(B.gamma + n);
+  const float coeff_1 = fmaxf(gamma, 4.f / 3.f) / ldf(B.bv + n);
+  float coeff_2 = ldf(B.mul + n) / cF.Pr;
+  if constexpr (C::turb) coeff_2 += ldf(B.mut + n) / cF.Prt;
+  float srv = grad_xi * grad_xi + grad_eta * grad_eta;
+  if (three_d) srv += grad_zeta * grad_zeta;
+  srv *= coeff_1 * coeff_2;
+  B.visc_spec[nd] = srv;
+  B.dt_local[B.Z.at(i, j, k)] = cF.cfl / (s0 + s1 + s2 + srv);
+}
+
+// DPLUR sweep with FP32 flux-Jacobian products; the update of the point
+// implicit blocks (EPI: stored LU factors) in FP64.
+template <class C>
+__global__ void __launch_bounds__(kCta, 4) k_sweep_mx(const DevBlock *__restrict__ blks, Tiles T, int in_sel,
+                                                      int out_sel) {
+  constexpr int NS = C::ns, NV = C::nv;
+  using fp32::ldf;
+  int b, i, j, k;
+  if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
+  const DevBlock &B = blks[b];
+  const double *dqin = in_sel == 0 ? B.dq : (in_sel == 1 ? B.dq0 : B.dqk);
+  double *dqout = out_sel == 0 ? B.dq : B.dqk;
+  const int64_t sz = B.G.size, szd = B.D.size, sz0 = B.Z.size;
+  const int64_t n = B.G.at(i, j, k), nd = B.D.at(i, j, k), nz = B.Z.at(i, j, k);
+  const int64_t sx = B.G.sx, sxy = B.G.sxy, dsx = B.D.sx, dsxy = B.D.sxy;
+  float tot[NV];
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) tot[l] = 0;
+  const double *isr = B.inv_spec;
+#pragma unroll 1
+  for (int q = 0; q < 6; ++q) {
+    const int dir = q < 3 ? q : q - 3;
+    const bool plus = q >= 3;
+    const int id = dir == 0 ? i : (dir == 1 ? j : k);
+    const int ext = dir == 0 ? B.mx : (dir == 1 ? B.my : B.mz);
+    if (plus ? id == ext - 1 : id == 0) continue;
+    const int64_t gs = dir == 0 ? 1 : (dir == 1 ? sx : sxy), ds = dir == 0 ? 1 : (dir == 1 ? dsx : dsxy);
+    const int64_t on = plus ? n + gs : n - gs, od = plus ? nd + ds : nd - ds;
+    const float sr = ldf(isr + dir * szd + od);
+    // compute_jacobian_times_dq (src/DPLURHPP.cuh:78-125) at the neighbour
+    const double *mr = B.metric + 3 * dir * sz;
+    const float xi_x = ldf(mr + on), xi_y = ldf(mr + sz + on), xi_z = ldf(mr + 2 * sz + on);
+    const float u = ldf(B.bv + sz + on), v = ldf(B.bv + 2 * sz + on), w = ldf(B.bv + 3 * sz + on);
+    const float U = xi_x * u + xi_y * v + xi_z * w;
+    const float lmd1 = U + (plus ? -sr : sr);
+    const float vel = ldf(B.vel + on);
+    const float e = 0.5f * vel * vel;
+    float d[NV];
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) d[l] = ldf(dqin + l * szd + od);
+    float gamma = 1.4f, b3 = 0, b4 = 0, h = 0;
+    if constexpr (C::mix != 0) {
+      const float t = ldf(B.bv + 5 * sz + on);
+      gamma = ldf(B.gamma + on);
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) {
+        const float hk = ldf(B.h_spec + l * szd + od);
+        b3 += fp32::kRu * t * cF.mw_inv[l] * d[5 + l];
+        b4 += hk * d[5 + l];
+        h += ldf(B.sv + l * sz + on) * hk;
+      }
+      b3 *= gamma;
+      b4 *= gamma - 1;
+      h += e;
+    } else {
+      h = gamma / (gamma - 1) * ldf(B.bv + 4 * sz + on) / ldf(B.bv + on) + e;
+    }
+    const float b1 = xi_x * d[1] + xi_y * d[2] + xi_z * d[3] - U * d[0];
+    const float b2 = (gamma - 1) * (e * d[0] - u * d[1] - v * d[2] - w * d[3] + d[4]);
+    const float b34 = b3 - b4;
+    const float sg = plus ? -0.5f : 0.5f;
+    tot[0] += sg * (b1 + lmd1 * d[0]);
+    tot[1] += sg * (u * b1 + xi_x * b2 + lmd1 * d[1] + xi_x * b34);
+    tot[2] += sg * (v * b1 + xi_y * b2 + lmd1 * d[2] + xi_y * b34);
+    tot[3] += sg * (w * b1 + xi_z * b2 + lmd1 * d[3] + xi_z * b34);
+    tot[4] += sg * (h * b1 + U * b2 + lmd1 * d[4] + U * b34);
+    OSTC_UNROLL for (int l = 0; l < C::nsc; ++l) tot[5 + l] += sg * (lmd1 * d[5 + l] + ldf(B.sv + l * sz + on) * b1);
+  }
+  const double dt = B.dt_local[nz];
+  const double diag = 1 + dt * (isr[nd] + isr[szd + nd] + isr[2 * szd + nd]);
+  double out[NV];
+  if constexpr (C::mix != 2) {
+    OSTC_UNROLL for (int l = 0; l < 5 + NS; ++l) out[l] = B.dq0[l * szd + nd] + dt * tot[l] / diag;
+  } else {
+    OSTC_UNROLL for (int l = 0; l < 5; ++l) out[l] = B.dq0[l * szd + nd] + dt * tot[l] / diag;
+    const int method = cP.chem_src_method;
+    if (method == 1) {
+      double lhs[NS * NS];
+      int piv[NS];
+      OSTC_UNROLL for (int q = 0; q < NS * NS; ++q) lhs[q] = B.chem_jac[q * sz0 + nz];
+      OSTC_UNROLL for (int q = 0; q < NS; ++q) piv[q] = B.lu_piv[q * sz0 + nz];
+      double rhs[NS];
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) rhs[l] = static_cast<double>(tot[5 + l]) * dt;
+      lu_solve<NS>(lhs, piv, rhs);
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) out[5 + l] = B.dq0[(5 + l) * szd + nd] + rhs[l];
+    } else if (method == 2) {
+      OSTC_UNROLL for (int l = 0; l < NS; ++l)
+        out[5 + l] = B.dq0[(5 + l) * szd + nd] + dt * tot[5 + l] / (diag - dt * B.chem_jac[l * sz0 + nz]);
+    } else {
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) out[5 + l] = B.dq0[(5 + l) * szd + nd] + dt * tot[5 + l] / diag;
+    }
+  }
+  if constexpr (C::turb) {
+    if (cP.turb_implicit == 1) {
+      out[NS + 5] = B.dq0[(NS + 5) * szd + nd] + dt * tot[5 + NS] / (diag - dt * B.turb_src_jac[nz]);
+      out[NS + 6] = B.dq0[(NS + 6) * szd + nd] + dt * tot[6 + NS] / (diag - dt * B.turb_src_jac[sz0 + nz]);
+    } else {
+      out[NS + 5] = B.dq0[(NS + 5) * szd + nd] + dt * tot[5 + NS] / diag;
+      out[NS + 6] = B.dq0[(NS + 6) * szd + nd] + dt * tot[6 + NS] / diag;
+    }
+  }
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) dqout[l * szd + nd] = out[l];
+}
+
+// Thermodynamic and transport properties in FP32 (update_physical_properties).
+template <class C>
+__global__ void __launch_bounds__(kCta) k_props_mx(const DevBlock *__restrict__ blks, Tiles T) {
+  constexpr int NS = C::ns;
+  using fp32::ldf;
+  int b, i, j, k;
+  if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
+  const DevBlock &B = blks[b];
+  const int64_t n = B.G.at(i, j, k), sz = B.G.size;
+  const float t = ldf(B.bv + 5 * sz + n);
+  if constexpr (C::mix != 0) {
+    float cp[NS], Y[NS];
+    fp32::thermo<NS, false, true>(t, nullptr, cp);
+    float mw_inv = 0, cp_tot = 0, cv = 0;
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) {
+      Y[l] = ldf(B.sv + l * sz + n);
+      mw_inv += Y[l] * cF.mw_inv[l];
+      cp_tot += Y[l] * cp[l];
+      cv += Y[l] * (cp[l] - cF.ru_mw[l]);
+    }
+    const float gamma = cp_tot / cv;
+    B.cp[n] = cp_tot;
+    B.gamma[n] = gamma;
+    const float a = sqrtf(gamma * fp32::kRu * t * mw_inv);
+    B.acoustic[n] = a;
+    const float mw = 1.f / mw_inv;
+    float X[NS], vis[NS];
+    const float st = sqrtf(t);
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) {
+      X[l] = Y[l] * mw * cF.mw_inv[l];
+      const float t_dl = t * cF.lj_inv[l];
+      const float r = 1.f / (t_dl + 0.5f);
+      const float ci = 1.147f * powf(t_dl, -0.145f) + r * r;
+      vis[l] = cF.vis_coeff[l] * st / ci;
+    }
+    float viscosity = 0, conductivity = 0;
+    OSTC_UNROLL for (int m = 0; m < NS; ++m) {
+      float vt = 0;
+      OSTC_UNROLL for (int q = 0; q < NS; ++q) {
+        float phi = 1.f;
+        if (m != q) {
+          const float num = 1 + sqrtf(vis[m] / vis[q]) * cF.wq[m * NS + q];
+          phi = num * num * cF.w8[m * NS + q];
+        }
+        vt += phi * X[q];
+      }
+      viscosity += vis[m] * X[m] / vt;
+      const float lambda = vis[m] * (cp[m] + 1.25f * cF.ru_mw[m]);
+      conductivity += lambda * X[m] / (1.065f * vt - 0.065f * X[m]);
+    }
+    B.mul[n] = viscosity;
+    B.cond[n] = conductivity;
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) {
+      const float dd = fabsf(X[l] - 1) < 1e-3f ? viscosity / cF.Sc : (1 - Y[l]) * viscosity / ((1 - X[l]) * cF.Sc);
+      B.rho_d[l * sz + n] = dd;
+    }
+    B.mach[n] = ldf(B.vel + n) / a;
+  } else {
+    const float a = sqrtf(1.4f * fp32::kRu / static_cast<float>(kDMwAir) * t);
+    B.acoustic[n] = a;
+    const float mul = 1.716e-5f * powf(t / 273.f, 1.5f) * (273.f + 111.f) / (t + 111.f);
+    B.mul[n] = mul;
+    B.cond[n] = mul * static_cast<float>(kDGammaAir * kDR_u / kDMwAir / (kDGammaAir - 1)) / cF.Pr;
+    B.mach[n] = ldf(B.vel + n) / a;
+  }
+}
+
+}  // namespace ostc

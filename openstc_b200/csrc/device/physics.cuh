@@ -23,11 +23,12 @@ namespace ostc {
 // set_params() entry.
 static __constant__ DevParams cP;
 
-template <int MIX, int TURB, int NS>
+template <int MIX, int TURB, int NS, bool MIXED = false>
 struct Cfg {
   static constexpr int mix = MIX;    // 0 air, 1 mixture, 2 finite-rate chemistry
   static constexpr int turb = TURB;  // 0 laminar, 1 k-omega SST
   static constexpr int ns = NS;
+  static constexpr bool mixed = MIXED;  // FP32-bulk / FP64-critical kernels
   static constexpr int nsc = NS + (TURB ? 2 : 0);
   static constexpr int nv = 5 + nsc;
 };

@@ -216,6 +216,7 @@ void Driver::initialize_computation() {
   s.inner = host_inner;
   s.wall_points = wall_points;
   s.device = opt.device;
+  s.precision = opt.precision;
   engine_ = make_engine(s);
   for (int b = 0; b < mesh.n_block; ++b) {
     const Block &B = mesh[b];

@@ -19,6 +19,7 @@ namespace ostc {
 struct DriverOptions {
   int device = 0;
   bool quiet = false;
+  int precision = 0;  // 0 FP64, 1 FP32-bulk / FP64-critical
 };
 
 class Driver {
