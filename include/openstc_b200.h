@@ -171,6 +171,18 @@ int ostc_driver_profile_step(ostc_driver *d, char *buf, int buflen);
 /* The CUDA stream the engine launches on (cudaStream_t). */
 void *ostc_driver_stream(ostc_driver *d);
 
+/* ---- chemistry surrogate (no counterpart in the reference) ----------------
+   The reference integrates the stiff chemistry with the point-implicit (EPI)
+   step only.  These entry points serve the learned replacement of that step. */
+
+/* D (FP32, row-major, leading dimension ldd) = A * B^T with A (M x K) and B
+   (N x K) BF16 row-major, on the tcgen05 tensor cores with FP32 accumulation.
+   All pointers are device memory; err is a device int set to 1 if a
+   tensor-core wait timed out.  splits > 1 writes `splits` partial results
+   (split-K) one after another, each M x ldd.  K, lda, ldb multiples of 8. */
+int ostc_tc_gemm_bf16(const void *A, int lda, const void *B, int ldb, float *D, int ldd, int M, int N, int K,
+                      int splits, int *err, void *stream);
+
 /* No counterpart in the reference.  Recomputes, from the device state, the
    normalised residuals of rho, |V|, p, T of the last step that stored its
    previous state (every output_screen-th step; the same values

@@ -115,6 +115,7 @@ def library() -> C.CDLL:
         "ostc_driver_step": ([P, C.c_int, D], C.c_int),
         "ostc_driver_residual": ([P, D], C.c_int),
         "ostc_driver_residual_noalloc": ([P, D], C.c_int),
+        "ostc_tc_gemm_bf16": ([P, C.c_int, P, C.c_int, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, P], C.c_int),
         "ostc_driver_run_phase": ([P, C.c_int], C.c_int),
         "ostc_driver_get_field": ([P, C.c_int, C.c_int, D, I64], C.c_int),
         "ostc_driver_set_field": ([P, C.c_int, C.c_int, D, I64], C.c_int),

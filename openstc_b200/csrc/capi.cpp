@@ -16,12 +16,7 @@ struct ostc_driver {
 };
 
 namespace {
-thread_local std::string g_error;
-
-int fail(int code, const std::string &msg) {
-  g_error = msg;
-  return code;
-}
+int fail(int code, const std::string &msg) { return ostc::abi_error(code, msg); }
 
 template <typename F>
 int guarded(F &&f) {
@@ -67,7 +62,7 @@ void field_layout(const ostc::DevParams &p, int ngg, int field, int &ghost, int 
 
 extern "C" {
 
-const char *ostc_last_error(void) { return g_error.c_str(); }
+const char *ostc_last_error(void) { return ostc::abi_last_error(); }
 
 int ostc_driver_create(const char *case_dir, const ostc_options *opt, ostc_driver **out) {
   if (!case_dir || !out) return fail(OSTC_ERR_INPUT, "null argument");

@@ -91,6 +91,10 @@ int residual_sums_noalloc(Engine &engine, int device, double raw[4], const char 
 
 std::unique_ptr<Engine> make_engine(const EngineSetup &setup);
 
+// Sets the message of ostc_last_error() for this host thread; returns code.
+int abi_error(int code, const std::string &msg);
+const char *abi_last_error();
+
 // Per-configuration factories (one translation unit each).
 std::unique_ptr<Engine> make_engine_air_lam(const EngineSetup &);
 std::unique_ptr<Engine> make_engine_air_sst(const EngineSetup &);
