@@ -183,6 +183,54 @@ void *ostc_driver_stream(ostc_driver *d);
 int ostc_tc_gemm_bf16(const void *A, int lda, const void *B, int ldb, float *D, int ldd, int M, int N, int K,
                       int splits, int *err, void *stream);
 
+/* The learned replacement of one point-implicit (EPI) chemistry step,
+   (T, p, Y_k, dt) -> dY_k, where the EPI step at fixed density is
+   rho dY = (I - dt J)^-1 dt omega (src/ImplicitTreatmentHPP.cuh:14-35 with
+   src/FiniteRateChem.cu:7-234).  MLP 12 -> 4 x 256 (GELU) -> 9, BF16 weights
+   and activations on the tensor cores with FP32 accumulation, FP32 master
+   weights, Adam. */
+typedef struct ostc_surrogate ostc_surrogate;
+
+typedef struct ostc_surrogate_eval {
+  double mean_rel;    /* mean over samples of max_k |dY - dY_EPI| / max_k |dY_EPI| (samples with max |dY_EPI| > 1e-8) */
+  double max_rel;
+  double mean_abs;    /* mean |dY - dY_EPI| */
+  double max_defect;  /* element-conservation defect, max over elements of |sum_k a_ek dY_k/W_k| / sum_k a_ek Y_k/W_k */
+  double mean_defect;
+  double gate_pass;   /* fraction of samples the trust gate accepts */
+  long long count;
+} ostc_surrogate_eval;
+
+/* Mechanism and device from the driver (9-species finite-rate case). */
+int ostc_surrogate_create(const ostc_driver *d, unsigned long long seed, ostc_surrogate **out);
+void ostc_surrogate_destroy(ostc_surrogate *s);
+/* Number of floats of ostc_surrogate_get_params / _gradients: per layer the
+   weight (out x in, padded to 16 inputs / 16 outputs) then the bias. */
+int ostc_surrogate_param_count(void);
+/* n samples: field_fraction of them from the cells of block 0 of `field`
+   (perturbed; NULL: none), the rest uniform in T [250, 2800] K, log10 p
+   [4.5, 6], log10 dt [-9, -6] with Dirichlet(1) mass fractions; labels from
+   the FP64 EPI step; sets the feature/target normalisation. */
+int ostc_surrogate_generate(ostc_surrogate *s, const ostc_driver *field, long long n, unsigned long long seed,
+                            double field_fraction);
+/* Adam steps on random batches of samples [0, n_train); losses[steps] may be NULL. */
+int ostc_surrogate_train(ostc_surrogate *s, int steps, int batch, double lr, long long n_train, float *losses);
+int ostc_surrogate_evaluate(ostc_surrogate *s, long long begin, long long count, ostc_surrogate_eval *out);
+/* states: n x 12 host doubles (T [K], p [Pa], Y[9], dt [s]); dy: n x 9. */
+int ostc_surrogate_label(ostc_surrogate *s, const double *states, long long n, double *dy);
+int ostc_surrogate_predict(ostc_surrogate *s, const double *states, long long n, double *dy, int *accepted);
+/* Mean-squared loss of the normalised targets of one batch (n multiple of
+   128) and its gradients (ostc_surrogate_param_count floats). */
+int ostc_surrogate_gradients(ostc_surrogate *s, const double *states, const double *dy, long long n, float *grads,
+                             double *loss);
+int ostc_surrogate_get_params(const ostc_surrogate *s, float *flat);
+int ostc_surrogate_set_params(ostc_surrogate *s, const float *flat);
+/* Features x_j = (f_j - in_mu_j) / in_sig_j of f = (T, log10 p, Y[9], log10 dt);
+   network output o_k maps to dY_k = out_c_k * sinh(out_scale_k * o_k). */
+int ostc_surrogate_normalisation(const ostc_surrogate *s, float *in_mu, float *in_sig, float *out_c, float *out_scale);
+int ostc_surrogate_save(const ostc_surrogate *s, const char *path);
+int ostc_surrogate_load(ostc_surrogate *s, const char *path);
+
 /* No counterpart in the reference.  Recomputes, from the device state, the
    normalised residuals of rho, |V|, p, T of the last step that stored its
    previous state (every output_screen-th step; the same values

@@ -37,6 +37,12 @@ class Options(C.Structure):
     _fields_ = [("device", C.c_int), ("quiet", C.c_int), ("precision", C.c_int)]
 
 
+class SurrogateEval(C.Structure):
+    _fields_ = [("mean_rel", C.c_double), ("max_rel", C.c_double), ("mean_abs", C.c_double),
+                ("max_defect", C.c_double), ("mean_defect", C.c_double), ("gate_pass", C.c_double),
+                ("count", C.c_longlong)]
+
+
 class Info(C.Structure):
     _fields_ = [
         ("n_block", C.c_int), ("ngg", C.c_int), ("dimension", C.c_int), ("n_spec", C.c_int), ("n_reac", C.c_int),
@@ -116,6 +122,20 @@ def library() -> C.CDLL:
         "ostc_driver_residual": ([P, D], C.c_int),
         "ostc_driver_residual_noalloc": ([P, D], C.c_int),
         "ostc_tc_gemm_bf16": ([P, C.c_int, P, C.c_int, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, P], C.c_int),
+        "ostc_surrogate_create": ([P, C.c_ulonglong, C.POINTER(P)], C.c_int),
+        "ostc_surrogate_destroy": ([P], None),
+        "ostc_surrogate_param_count": ([], C.c_int),
+        "ostc_surrogate_generate": ([P, P, C.c_longlong, C.c_ulonglong, C.c_double], C.c_int),
+        "ostc_surrogate_train": ([P, C.c_int, C.c_int, C.c_double, C.c_longlong, P], C.c_int),
+        "ostc_surrogate_evaluate": ([P, C.c_longlong, C.c_longlong, C.POINTER(SurrogateEval)], C.c_int),
+        "ostc_surrogate_label": ([P, P, C.c_longlong, P], C.c_int),
+        "ostc_surrogate_predict": ([P, P, C.c_longlong, P, P], C.c_int),
+        "ostc_surrogate_gradients": ([P, P, P, C.c_longlong, P, C.POINTER(C.c_double)], C.c_int),
+        "ostc_surrogate_get_params": ([P, P], C.c_int),
+        "ostc_surrogate_set_params": ([P, P], C.c_int),
+        "ostc_surrogate_normalisation": ([P, P, P, P, P], C.c_int),
+        "ostc_surrogate_save": ([P, C.c_char_p], C.c_int),
+        "ostc_surrogate_load": ([P, C.c_char_p], C.c_int),
         "ostc_driver_run_phase": ([P, C.c_int], C.c_int),
         "ostc_driver_get_field": ([P, C.c_int, C.c_int, D, I64], C.c_int),
         "ostc_driver_set_field": ([P, C.c_int, C.c_int, D, I64], C.c_int),
@@ -298,3 +318,89 @@ class Driver:
 
     def stream(self) -> int:
         return library().ostc_driver_stream(self._h) or 0
+
+
+def _vp(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Surrogate:
+    """The learned EPI chemistry step (ostc_surrogate_*): data generation with
+    the FP64 EPI step, training on the tensor cores, evaluation."""
+
+    def __init__(self, driver: "Driver", seed: int = 1):
+        h = C.c_void_p()
+        _check(library().ostc_surrogate_create(driver._h, seed, C.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if self._h:
+            library().ostc_surrogate_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def param_count() -> int:
+        return library().ostc_surrogate_param_count()
+
+    def generate(self, n: int, seed: int = 1, field: "Driver | None" = None, field_fraction: float = 0.5) -> None:
+        _check(library().ostc_surrogate_generate(self._h, field._h if field else None, n, seed, field_fraction))
+
+    def train(self, steps: int, batch: int = 65536, lr: float = 1e-3, n_train: int = 0) -> np.ndarray:
+        losses = np.zeros(max(steps, 1), dtype=np.float32)
+        _check(library().ostc_surrogate_train(self._h, steps, batch, lr, n_train, _vp(losses)))
+        return losses[:steps]
+
+    def evaluate(self, begin: int, count: int) -> dict:
+        e = SurrogateEval()
+        _check(library().ostc_surrogate_evaluate(self._h, begin, count, C.byref(e)))
+        return {f: getattr(e, f) for f, _ in SurrogateEval._fields_}
+
+    def label(self, states: np.ndarray) -> np.ndarray:
+        s = np.ascontiguousarray(states, dtype=np.float64)
+        out = np.zeros((s.shape[0], 9))
+        _check(library().ostc_surrogate_label(self._h, _vp(s), s.shape[0], _vp(out)))
+        return out
+
+    def predict(self, states: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+        s = np.ascontiguousarray(states, dtype=np.float64)
+        out = np.zeros((s.shape[0], 9))
+        acc = np.zeros(s.shape[0], dtype=np.int32)
+        _check(library().ostc_surrogate_predict(self._h, _vp(s), s.shape[0], _vp(out), _vp(acc)))
+        return out, acc.astype(bool)
+
+    def gradients(self, states: np.ndarray, dy: np.ndarray) -> tuple[float, np.ndarray]:
+        s = np.ascontiguousarray(states, dtype=np.float64)
+        d = np.ascontiguousarray(dy, dtype=np.float64)
+        g = np.zeros(self.param_count(), dtype=np.float32)
+        loss = C.c_double()
+        _check(library().ostc_surrogate_gradients(self._h, _vp(s), _vp(d), s.shape[0], _vp(g), C.byref(loss)))
+        return loss.value, g
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.param_count(), dtype=np.float32)
+        _check(library().ostc_surrogate_get_params(self._h, _vp(p)))
+        return p
+
+    def set_params(self, p: np.ndarray) -> None:
+        a = np.ascontiguousarray(p, dtype=np.float32)
+        _check(library().ostc_surrogate_set_params(self._h, _vp(a)))
+
+    def normalisation(self) -> tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]:
+        """(in_mu, in_sig, out_c, out_s): x = (f - in_mu) / in_sig; dY = out_c sinh(out_s o)."""
+        mu, sig = np.zeros(12, np.float32), np.zeros(12, np.float32)
+        c, sc = np.zeros(9, np.float32), np.zeros(9, np.float32)
+        _check(library().ostc_surrogate_normalisation(self._h, _vp(mu), _vp(sig), _vp(c), _vp(sc)))
+        return mu, sig, c, sc
+
+    def save(self, path) -> None:
+        _check(library().ostc_surrogate_save(self._h, str(path).encode()))
+
+    def load(self, path) -> None:
+        _check(library().ostc_surrogate_load(self._h, str(path).encode()))
+

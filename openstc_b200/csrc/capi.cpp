@@ -8,6 +8,7 @@
 #include <string>
 
 #include "device/engine.hpp"
+#include "device/surrogate.hpp"
 #include "host/driver.hpp"
 
 struct ostc_driver {
@@ -355,3 +356,175 @@ void *ostc_driver_stream(ostc_driver *d) {
 }
 
 }  // extern "C"
+
+namespace ostc {
+cudaError_t tc_gemm(const uint16_t *A, int lda, const uint16_t *B, int ldb, float *D, int ldd, int M, int N, int K,
+                    int splits, int *err, cudaStream_t st);
+}
+
+struct ostc_surrogate {
+  std::unique_ptr<ostc::Surrogate> s;
+};
+
+namespace {
+constexpr int kSurParamCount() {
+  int n = 0;
+  const int dims[ostc::kSurLayers + 1] = {ostc::kSurInPad, ostc::kSurHidden, ostc::kSurHidden, ostc::kSurHidden,
+                                          ostc::kSurHidden, ostc::kSurOutPad};
+  for (int l = 0; l < ostc::kSurLayers; ++l) n += dims[l + 1] * dims[l] + dims[l + 1];
+  return n;
+}
+}  // namespace
+
+extern "C" {
+
+int ostc_tc_gemm_bf16(const void *A, int lda, const void *B, int ldb, float *D, int ldd, int M, int N, int K,
+                      int splits, int *err, void *stream) {
+  if (!A || !B || !D || !err || M <= 0 || N <= 0 || K <= 0 || splits <= 0)
+    return fail(OSTC_ERR_INPUT, "ostc_tc_gemm_bf16: null pointer or non-positive size");
+  if (K % 8 || lda % 8 || ldb % 8 || lda < K || ldb < K || ldd < N)
+    return fail(OSTC_ERR_INPUT, "ostc_tc_gemm_bf16: K, lda and ldb must be multiples of 8, lda/ldb >= K, ldd >= N");
+  const cudaError_t e = ostc::tc_gemm(static_cast<const uint16_t *>(A), lda, static_cast<const uint16_t *>(B), ldb, D,
+                                      ldd, M, N, K, splits, err, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return fail(OSTC_ERR_CUDA, std::string("ostc_tc_gemm_bf16: ") + cudaGetErrorString(e));
+  return OSTC_OK;
+}
+
+int ostc_surrogate_create(const ostc_driver *d, unsigned long long seed, ostc_surrogate **out) {
+  if (!d || !out) return fail(OSTC_ERR_INPUT, "null argument");
+  return guarded([&] {
+    const auto &sp = d->drv.spec;
+    auto h = std::make_unique<ostc_surrogate>();
+    h->s = std::make_unique<ostc::Surrogate>(d->drv.dev_params, sp.elem_comp, sp.n_elem(), d->drv.opt.device, seed);
+    *out = h.release();
+    return OSTC_OK;
+  });
+}
+
+void ostc_surrogate_destroy(ostc_surrogate *s) { delete s; }
+
+int ostc_surrogate_param_count(void) { return kSurParamCount(); }
+
+int ostc_surrogate_generate(ostc_surrogate *s, const ostc_driver *field, long long n, unsigned long long seed,
+                            double field_fraction) {
+  if (!s) return fail(OSTC_ERR_INPUT, "null argument");
+  if (field && !field->drv.initialized()) return fail(OSTC_ERR_STATE, "the field driver is not initialised");
+  return guarded([&] {
+    const ostc::DevBlock *blk = nullptr;
+    ostc::DevBlock b0{};
+    if (field) {
+      b0 = const_cast<ostc_driver *>(field)->drv.engine().blocks().at(0);
+      blk = &b0;
+    }
+    s->s->generate(n, seed, blk, field_fraction);
+    return OSTC_OK;
+  });
+}
+
+int ostc_surrogate_train(ostc_surrogate *s, int steps, int batch, double lr, long long n_train, float *losses) {
+  if (!s || steps < 0 || batch <= 0) return fail(OSTC_ERR_INPUT, "bad argument");
+  return guarded([&] {
+    s->s->train(steps, batch, lr, n_train, losses);
+    return OSTC_OK;
+  });
+}
+
+int ostc_surrogate_evaluate(ostc_surrogate *s, long long begin, long long count, ostc_surrogate_eval *out) {
+  if (!s || !out) return fail(OSTC_ERR_INPUT, "null argument");
+  return guarded([&] {
+    const ostc::SurrogateEval e = s->s->evaluate(begin, count);
+    out->mean_rel = e.mean_rel;
+    out->max_rel = e.max_rel;
+    out->mean_abs = e.mean_abs;
+    out->max_defect = e.max_defect;
+    out->mean_defect = e.mean_defect;
+    out->gate_pass = e.gate_pass;
+    out->count = e.count;
+    return OSTC_OK;
+  });
+}
+
+int ostc_surrogate_label(ostc_surrogate *s, const double *states, long long n, double *dy) {
+  if (!s || !states || !dy || n <= 0) return fail(OSTC_ERR_INPUT, "bad argument");
+  return guarded([&] {
+    s->s->label_host(states, n, dy);
+    return OSTC_OK;
+  });
+}
+
+int ostc_surrogate_predict(ostc_surrogate *s, const double *states, long long n, double *dy, int *accepted) {
+  if (!s || !states || !dy || !accepted || n <= 0) return fail(OSTC_ERR_INPUT, "bad argument");
+  return guarded([&] {
+    s->s->predict_host(states, n, dy, accepted);
+    return OSTC_OK;
+  });
+}
+
+int ostc_surrogate_gradients(ostc_surrogate *s, const double *states, const double *dy, long long n, float *grads,
+                             double *loss) {
+  if (!s || !states || !dy || !grads || !loss || n <= 0) return fail(OSTC_ERR_INPUT, "bad argument");
+  return guarded([&] {
+    std::vector<std::vector<float>> g;
+    *loss = s->s->grad_host(states, dy, n, g);
+    size_t off = 0;
+    for (const auto &v : g) {
+      std::copy(v.begin(), v.end(), grads + off);
+      off += v.size();
+    }
+    return OSTC_OK;
+  });
+}
+
+int ostc_surrogate_get_params(const ostc_surrogate *s, float *flat) {
+  if (!s || !flat) return fail(OSTC_ERR_INPUT, "null argument");
+  return guarded([&] {
+    size_t off = 0;
+    for (const auto &v : s->s->params()) {
+      std::copy(v.begin(), v.end(), flat + off);
+      off += v.size();
+    }
+    return OSTC_OK;
+  });
+}
+
+int ostc_surrogate_set_params(ostc_surrogate *s, const float *flat) {
+  if (!s || !flat) return fail(OSTC_ERR_INPUT, "null argument");
+  return guarded([&] {
+    auto p = s->s->params();
+    size_t off = 0;
+    for (auto &v : p) {
+      std::copy(flat + off, flat + off + v.size(), v.begin());
+      off += v.size();
+    }
+    s->s->set_params(p);
+    return OSTC_OK;
+  });
+}
+
+int ostc_surrogate_normalisation(const ostc_surrogate *s, float *in_mu, float *in_sig, float *out_c, float *out_scale) {
+  if (!s || !in_mu || !in_sig || !out_c || !out_scale) return fail(OSTC_ERR_INPUT, "null argument");
+  std::copy(s->s->out_c.begin(), s->s->out_c.end(), out_c);
+  std::copy(s->s->in_mu.begin(), s->s->in_mu.end(), in_mu);
+  std::copy(s->s->in_sig.begin(), s->s->in_sig.end(), in_sig);
+  std::copy(s->s->out_s.begin(), s->s->out_s.end(), out_scale);
+  return OSTC_OK;
+}
+
+int ostc_surrogate_save(const ostc_surrogate *s, const char *path) {
+  if (!s || !path) return fail(OSTC_ERR_INPUT, "null argument");
+  return guarded([&] {
+    s->s->save(path);
+    return OSTC_OK;
+  });
+}
+
+int ostc_surrogate_load(ostc_surrogate *s, const char *path) {
+  if (!s || !path) return fail(OSTC_ERR_INPUT, "null argument");
+  return guarded([&] {
+    s->s->load(path);
+    return OSTC_OK;
+  });
+}
+
+}  // extern "C"
+

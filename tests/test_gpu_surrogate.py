@@ -1,0 +1,98 @@
+"""The chemistry surrogate: FP64 EPI labels against the C oracle, tensor-core
+gradients against the NumPy oracle (oracle/mlp_oracle.py), training, the
+trust gate, and what the network gains over the EPI step it replaces."""
+import ctypes as C
+import sys
+import time
+
+import numpy as np
+import pytest
+
+import openstc_b200 as ostc
+from openstc_b200 import cases
+from conftest import ROOT
+from oracle_bridge import oracle_lib, orc_params_from
+
+sys.path.insert(0, str(ROOT / "oracle"))
+import mlp_oracle  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+RU = 8314.462618
+
+
+@pytest.fixture(scope="module")
+def drv(tmp_path_factory):
+    case = tmp_path_factory.mktemp("sur") / "ml"
+    cases.mixing_layer_case(case, mx=8, my=8, mz=4, total_step=1, output_screen=1)
+    return ostc.Driver(case)
+
+
+def random_states(n, seed):
+    rng = np.random.default_rng(seed)
+    s = np.zeros((n, 12))
+    s[:, 0] = rng.uniform(250, 2800, n)
+    s[:, 1] = 10 ** rng.uniform(4.5, 6.0, n)
+    s[:, 2:11] = rng.dirichlet(np.ones(9), n)
+    s[:, 11] = 10 ** rng.uniform(-9, -6, n)
+    return s
+
+
+def test_labels_match_oracle_epi(drv):
+    sur = ostc.Surrogate(drv, seed=3)
+    st = random_states(512, 11)
+    dy = sur.label(st)
+    p = orc_params_from(drv.params())
+    mw = np.array(drv.params().mw[:9])
+    worst = 0.0
+    for i in range(st.shape[0]):
+        Y = np.zeros(20)
+        Y[:9] = st[i, 2:11]
+        rho = st[i, 1] / (RU * st[i, 0] * np.sum(Y[:9] / mw))
+        ref = np.zeros(20)
+        oracle_lib().orc_epi_increment(C.byref(p), rho, st[i, 0], Y.ctypes.data_as(C.POINTER(C.c_double)), st[i, 11],
+                                       ref.ctypes.data_as(C.POINTER(C.c_double)))
+        scale = max(np.max(np.abs(ref[:9])), 1e-30)
+        worst = max(worst, np.max(np.abs(dy[i] - ref[:9])) / scale)
+    assert worst < 1e-9, worst
+
+
+def test_gradients_match_oracle(drv):
+    sur = ostc.Surrogate(drv, seed=5)
+    sur.generate(4096, seed=2)
+    st = random_states(1024, 12)
+    dy = sur.label(st)
+    loss, g = sur.gradients(st, dy)
+    mu, sig, c, sc = sur.normalisation()
+    x = mlp_oracle.features(st, mu, sig)
+    t = (np.arcsinh(dy / c.astype(np.float64)) / sc.astype(np.float64)).astype(np.float32).astype(np.float64)
+    loss_ref, g_ref = mlp_oracle.loss_and_grads(sur.params(), x, t)
+    assert abs(loss - loss_ref) <= 1e-4 * abs(loss_ref)
+    off = 0
+    for l in range(5):
+        for n in (mlp_oracle.DIMS[l] * mlp_oracle.DIMS[l + 1], mlp_oracle.DIMS[l + 1]):
+            a, b = g[off:off + n], g_ref[off:off + n]
+            off += n
+            rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+            assert rel < 2e-3, (l, n, rel)
+
+
+def test_training_learns_and_gate(drv, tmp_path):
+    sur = ostc.Surrogate(drv, seed=7)
+    n = 1 << 19
+    sur.generate(n, seed=4)
+    losses = sur.train(400, batch=16384, lr=2e-3, n_train=n - (1 << 16))
+    assert np.all(np.isfinite(losses))
+    assert np.median(losses[-50:]) < 0.2 * np.median(losses[:5]), (losses[:5], losses[-50:])
+    ev = sur.evaluate(n - (1 << 16), 1 << 16)
+    assert ev["count"] == 1 << 16 and 0.0 <= ev["gate_pass"] <= 1.0
+    # save / load round trip
+    path = tmp_path / "mlp.bin"
+    sur.save(path)
+    other = ostc.Surrogate(drv, seed=99)
+    other.load(path)
+    st = random_states(256, 21)
+    a, ga = sur.predict(st)
+    b, gb = other.predict(st)
+    assert np.array_equal(a, b) and np.array_equal(ga, gb)
+    print("held-out:", ev)
