@@ -55,8 +55,11 @@ typedef enum ostc_phase {
   OSTC_PHASE_EXCHANGE = 4, /* inner faces, 2-D k copy, properties (src/Driver.cu:257-272) */
   OSTC_PHASE_STORE = 5,    /* store_last_step (src/TimeAdvanceFunc.cu:5-16) */
   OSTC_PHASE_SOURCE = 6,   /* first half of RESIDUAL: dq = source terms (src/SourceTerm.cuh:12-40) */
-  OSTC_PHASE_FLUX = 7      /* second half of RESIDUAL: inviscid + viscous fluxes, local dt
+  OSTC_PHASE_FLUX = 7,     /* second half of RESIDUAL: inviscid + viscous fluxes, local dt
                               (src/SchemeSelector.cuh:38-280, src/TimeAdvanceFunc.cuh:21-71) */
+  OSTC_PHASE_CHEMISTRY = 8 /* one chemistry step on its own: the surrogate's dY where the gate
+                              accepts, one EPI step elsewhere, applied to rho Y (needs
+                              ostc_driver_set_surrogate; not part of the step) */
 } ostc_phase;
 
 typedef struct ostc_options {
@@ -226,10 +229,30 @@ int ostc_surrogate_gradients(ostc_surrogate *s, const double *states, const doub
 int ostc_surrogate_get_params(const ostc_surrogate *s, float *flat);
 int ostc_surrogate_set_params(ostc_surrogate *s, const float *flat);
 /* Features x_j = (f_j - in_mu_j) / in_sig_j of f = (T, log10 p, Y[9], log10 dt);
-   network output o_k maps to dY_k = out_c_k * sinh(out_scale_k * o_k). */
+   network output o_k maps to dY_k = (Y_k + 1e-10) * out_c_k * sinh(out_scale_k * o_k). */
 int ostc_surrogate_normalisation(const ostc_surrogate *s, float *in_mu, float *in_sig, float *out_c, float *out_scale);
+/* The per-cell trust gate: inputs in the training box, |network output| <=
+   out_max, element defect <= defect_tol of the element totals, |dY_k| <=
+   rel_max (Y_k + 1e-10); other cells take the EPI fallback.  Takes effect
+   for drivers at their next ostc_driver_set_surrogate. */
+typedef struct ostc_surrogate_gate {
+  float t_min, t_max, lp_min, lp_max, ldt_min, ldt_max, defect_tol, rel_max, out_max;
+} ostc_surrogate_gate;
+int ostc_surrogate_get_gate(const ostc_surrogate *s, ostc_surrogate_gate *g);
+int ostc_surrogate_set_gate(ostc_surrogate *s, const ostc_surrogate_gate *g);
 int ostc_surrogate_save(const ostc_surrogate *s, const char *path);
 int ostc_surrogate_load(ostc_surrogate *s, const char *path);
+/* Chemistry of the driver's steps through the surrogate.  Before the source
+   term of every step the network evaluates each cell (with the cell's local
+   time step); cells the trust gate accepts are chemically quiet and take the
+   network's rate rho dY/dt as an explicit source with no chemistry Jacobian,
+   every other cell keeps the reference's point-implicit (EPI) chemistry inside
+   the coupled DPLUR step -- the fallback.  s = NULL returns to EPI everywhere.
+   The surrogate must stay alive while set; its weights are read at each step. */
+int ostc_driver_set_surrogate(ostc_driver *d, ostc_surrogate *s);
+/* Cell evaluations accepted by the trust gate and sent to the point-implicit
+   fallback since the surrogate was set. */
+int ostc_driver_chemistry_stats(ostc_driver *d, long long *accepted, long long *fallback);
 
 /* No counterpart in the reference.  Recomputes, from the device state, the
    normalised residuals of rho, |V|, p, T of the last step that stored its

@@ -26,7 +26,8 @@ FIELDS = [
 ]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 PRECISIONS = {"fp64": 0, "mixed": 1}
-PHASES = {"residual": 0, "implicit": 1, "update": 2, "bc": 3, "exchange": 4, "store": 5, "source": 6, "flux": 7}
+PHASES = {"residual": 0, "implicit": 1, "update": 2, "bc": 3, "exchange": 4, "store": 5, "source": 6, "flux": 7,
+          "chemistry": 8}
 
 
 class OstcError(RuntimeError):
@@ -41,6 +42,11 @@ class SurrogateEval(C.Structure):
     _fields_ = [("mean_rel", C.c_double), ("max_rel", C.c_double), ("mean_abs", C.c_double),
                 ("max_defect", C.c_double), ("mean_defect", C.c_double), ("gate_pass", C.c_double),
                 ("count", C.c_longlong)]
+
+
+class SurrogateGate(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("t_min", "t_max", "lp_min", "lp_max", "ldt_min", "ldt_max", "defect_tol",
+                                         "rel_max", "out_max")]
 
 
 class Info(C.Structure):
@@ -136,6 +142,10 @@ def library() -> C.CDLL:
         "ostc_surrogate_normalisation": ([P, P, P, P, P], C.c_int),
         "ostc_surrogate_save": ([P, C.c_char_p], C.c_int),
         "ostc_surrogate_load": ([P, C.c_char_p], C.c_int),
+        "ostc_driver_set_surrogate": ([P, P], C.c_int),
+        "ostc_surrogate_get_gate": ([P, C.POINTER(SurrogateGate)], C.c_int),
+        "ostc_surrogate_set_gate": ([P, C.POINTER(SurrogateGate)], C.c_int),
+        "ostc_driver_chemistry_stats": ([P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], C.c_int),
         "ostc_driver_run_phase": ([P, C.c_int], C.c_int),
         "ostc_driver_get_field": ([P, C.c_int, C.c_int, D, I64], C.c_int),
         "ostc_driver_set_field": ([P, C.c_int, C.c_int, D, I64], C.c_int),
@@ -266,6 +276,19 @@ class Driver:
         _check(library().ostc_driver_residual(self._h, _dptr(r)))
         return r
 
+    def set_surrogate(self, sur: "Surrogate | None") -> None:
+        """Chemistry through the surrogate: cells its trust gate accepts take
+        the network's rate as an explicit source, the others keep the coupled
+        point-implicit chemistry (None: point-implicit everywhere)."""
+        self._surrogate = sur
+        _check(library().ostc_driver_set_surrogate(self._h, sur._h if sur is not None else None))
+
+    def chemistry_stats(self) -> tuple[int, int]:
+        """(cells accepted by the trust gate, cells sent to the EPI fallback)."""
+        a, f = C.c_longlong(), C.c_longlong()
+        _check(library().ostc_driver_chemistry_stats(self._h, C.byref(a), C.byref(f)))
+        return a.value, f.value
+
     def residual_noalloc(self) -> np.ndarray:
         """The residual of the last stored step recomputed on the device in
         a static scratch (ostc_driver_residual_noalloc): no device memory
@@ -392,11 +415,26 @@ class Surrogate:
         _check(library().ostc_surrogate_set_params(self._h, _vp(a)))
 
     def normalisation(self) -> tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]:
-        """(in_mu, in_sig, out_c, out_s): x = (f - in_mu) / in_sig; dY = out_c sinh(out_s o)."""
+        """(in_mu, in_sig, out_c, out_s): x = (f - in_mu) / in_sig;
+        dY = (Y + 1e-10) out_c sinh(out_s o)."""
         mu, sig = np.zeros(12, np.float32), np.zeros(12, np.float32)
         c, sc = np.zeros(9, np.float32), np.zeros(9, np.float32)
         _check(library().ostc_surrogate_normalisation(self._h, _vp(mu), _vp(sig), _vp(c), _vp(sc)))
         return mu, sig, c, sc
+
+    def gate(self) -> dict:
+        g = SurrogateGate()
+        _check(library().ostc_surrogate_get_gate(self._h, C.byref(g)))
+        return {n: getattr(g, n) for n, _ in SurrogateGate._fields_}
+
+    def set_gate(self, **kw) -> None:
+        g = SurrogateGate()
+        _check(library().ostc_surrogate_get_gate(self._h, C.byref(g)))
+        for k, v in kw.items():
+            if not hasattr(g, k):
+                raise OstcError(f"unknown gate field {k}")
+            setattr(g, k, v)
+        _check(library().ostc_surrogate_set_gate(self._h, C.byref(g)))
 
     def save(self, path) -> None:
         _check(library().ostc_surrogate_save(self._h, str(path).encode()))

@@ -510,6 +510,46 @@ int ostc_surrogate_normalisation(const ostc_surrogate *s, float *in_mu, float *i
   return OSTC_OK;
 }
 
+int ostc_driver_set_surrogate(ostc_driver *d, ostc_surrogate *s) {
+  if (!d) return fail(OSTC_ERR_INPUT, "null argument");
+  if (!d->drv.initialized()) return fail(OSTC_ERR_STATE, "initialize first");
+  return guarded([&]() -> int {
+    if (s) {
+      if (s->s->device() != d->drv.opt.device) return fail(OSTC_ERR_INPUT, "surrogate and driver are on different devices");
+      const ostc::SurrogateDev p = s->s->device_params();
+      d->drv.engine().set_surrogate(&p);
+    } else {
+      d->drv.engine().set_surrogate(nullptr);
+    }
+    return OSTC_OK;
+  });
+}
+
+int ostc_driver_chemistry_stats(ostc_driver *d, long long *accepted, long long *fallback) {
+  if (!d || !accepted || !fallback) return fail(OSTC_ERR_INPUT, "null argument");
+  if (!d->drv.initialized()) return fail(OSTC_ERR_STATE, "initialize first");
+  return guarded([&] {
+    unsigned long long st[2];
+    d->drv.engine().surrogate_stats(st);
+    *accepted = static_cast<long long>(st[0]);
+    *fallback = static_cast<long long>(st[1]);
+    return OSTC_OK;
+  });
+}
+
+int ostc_surrogate_get_gate(const ostc_surrogate *s, ostc_surrogate_gate *g) {
+  if (!s || !g) return fail(OSTC_ERR_INPUT, "null argument");
+  static_assert(sizeof(ostc_surrogate_gate) == sizeof(ostc::SurrogateGate), "gate layouts differ");
+  std::memcpy(g, &s->s->gate, sizeof(*g));
+  return OSTC_OK;
+}
+
+int ostc_surrogate_set_gate(ostc_surrogate *s, const ostc_surrogate_gate *g) {
+  if (!s || !g) return fail(OSTC_ERR_INPUT, "null argument");
+  std::memcpy(&s->s->gate, g, sizeof(*g));
+  return OSTC_OK;
+}
+
 int ostc_surrogate_save(const ostc_surrogate *s, const char *path) {
   if (!s || !path) return fail(OSTC_ERR_INPUT, "null argument");
   return guarded([&] {

@@ -72,6 +72,10 @@ struct DevBlock {
   // species enthalpies h_k(T) of each cell, written by k_dq0 for the DPLUR
   // sweeps (layout D, ns components; mixtures under DPLUR only)
   double *h_spec;
+  // chemistry surrogate (layout Z; null when off): cells the surrogate judged
+  // chemically quiet take its increment rate rho dY/dt as an explicit source
+  unsigned char *chem_quiet;
+  double *chem_rate;
 };
 
 // Work table of a launch: CTA-tiles of every block, in block order.

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "surrogate.hpp"
 
 namespace ostc {
 
@@ -76,6 +77,13 @@ class Engine {
   // out[4] (both device memory supplied by the caller).  Same kernels and
   // summation order as the residual of step().
   virtual void residual_sums_to(double *partial, double *out) = 0;
+  // Chemistry through the surrogate as a split step after the flow update
+  // (nullptr: back to the coupled point-implicit chemistry).  The parameters
+  // point into the Surrogate's device memory, which must outlive the use.
+  virtual void set_surrogate(const SurrogateDev *p) = 0;
+  // cells accepted by the trust gate and cells sent to the EPI fallback
+  // since the surrogate was set
+  virtual void surrogate_stats(unsigned long long out[2]) = 0;
 };
 
 // Largest grid ostc_driver_residual_noalloc accepts, in residual tiles

@@ -12,6 +12,7 @@
 
 #include "engine.hpp"
 #include "kernels_mixed.cuh"
+#include "kernels_surrogate.cuh"
 
 namespace ostc {
 
@@ -93,6 +94,11 @@ class EngineT final : public Engine {
   ~EngineT() override {
     for (auto &g : graphs_)
       if (g) cudaGraphExecDestroy(g);
+    for (void *q : sur_arrays_) cudaFree(q);
+    cudaFree(d_fb_count_);
+    cudaFree(d_fb_list_);
+    cudaFree(d_sur_stats_);
+    cudaFree(d_sur_err_);
     for (void *p : allocations_) cudaFree(p);
     cudaFree(d_blocks_);
     cudaFree(d_bcs_);
@@ -195,6 +201,10 @@ class EngineT final : public Engine {
       case 7:
         launch_flux();
         break;
+      case 8:
+        if (!sur_on_) throw std::runtime_error("no surrogate is set");
+        launch_chemistry_split();
+        break;
       default:
         throw std::runtime_error("unknown phase");
     }
@@ -254,10 +264,15 @@ class EngineT final : public Engine {
   }
 
  private:
+  static const void *&static_owner() {
+    static const void *owner = nullptr;
+    return owner;
+  }
+
   void upload_params() {
     // The __constant__ parameter block is per translation unit and per
     // device; re-upload when another engine of this configuration ran last.
-    static const void *owner = nullptr;
+    const void *&owner = static_owner();
     if (owner != this) {
       cuda_check(cudaMemcpyToSymbol(cP, &setup_.params, sizeof(DevParams)), "upload params");
       if constexpr (C::mixed) {
@@ -417,7 +432,21 @@ class EngineT final : public Engine {
       k_props<C><<<grid(tiles1_), block3(), 0, stream_>>>(d_blocks_, tiles1_);
   }
 
+  // the surrogate marks chemically quiet cells before the source term
+  void launch_classify() {
+    if constexpr (C::mix == 2) {
+      for (int b = 0; b < static_cast<int>(blocks_.size()); ++b) {
+        const DevBlock &B = blocks_[b];
+        const int64_t cells = static_cast<int64_t>(B.mx) * B.my * B.mz;
+        sur::k_sur_infer<C><<<static_cast<unsigned>((cells + 127) / 128), sur::kThreads, sur::kSmem, stream_>>>(
+            d_blocks_, b, sur_, 1, d_fb_count_, d_fb_list_, d_sur_stats_, d_sur_err_);
+        mark("surrogate");
+      }
+    }
+  }
+
   void launch_residual() {
+    if (sur_on_) launch_classify();
     launch_source();
     mark("source");
     launch_flux();
@@ -448,6 +477,85 @@ class EngineT final : public Engine {
       final_dq_ = 0;
     }
     return final_dq_;
+  }
+
+  void set_surrogate(const SurrogateDev *p) override {
+    if constexpr (C::mix != 2) {
+      if (p) throw std::runtime_error("the chemistry surrogate needs a finite-rate chemistry case");
+    } else {
+      if (p && setup_.params.ns != kSurOut) throw std::runtime_error("the surrogate is built for 9 species");
+      sur_on_ = p != nullptr;
+      if (p) sur_ = *p;
+      if (sur_on_ && !d_fb_count_) {
+        int64_t most = 0;
+        for (const auto &B : blocks_) most = std::max<int64_t>(most, static_cast<int64_t>(B.mx) * B.my * B.mz);
+        cuda_check(cudaMalloc(&d_fb_count_, sizeof(int)), "cudaMalloc fallback count");
+        cuda_check(cudaMalloc(&d_fb_list_, sizeof(int) * most), "cudaMalloc fallback list");
+        cuda_check(cudaMalloc(&d_sur_stats_, 2 * sizeof(unsigned long long)), "cudaMalloc surrogate stats");
+        cuda_check(cudaMalloc(&d_sur_err_, sizeof(int)), "cudaMalloc surrogate err");
+        cuda_check(cudaMemset(d_sur_err_, 0, sizeof(int)), "memset surrogate err");
+        cuda_check(cudaFuncSetAttribute(sur::k_sur_infer<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(sur::kSmem)),
+                   "surrogate smem");
+        const int fb_smem = static_cast<int>(2 * std::max(1, setup_.params.nr) * 128 * sizeof(double));
+        if (fb_smem > 48 * 1024)
+          cuda_check(cudaFuncSetAttribute(sur::k_sur_fallback<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, fb_smem),
+                     "fallback smem");
+      }
+      if (sur_on_) cuda_check(cudaMemset(d_sur_stats_, 0, 2 * sizeof(unsigned long long)), "memset stats");
+      for (auto &B : blocks_) {
+        if (sur_on_ && !B.chem_quiet) {
+          void *q = nullptr;
+          cuda_check(cudaMalloc(&q, static_cast<size_t>(B.Z.size)), "cudaMalloc quiet");
+          cuda_check(cudaMemset(q, 0, static_cast<size_t>(B.Z.size)), "memset quiet");
+          sur_arrays_.push_back(q);
+          quiet_store_.push_back(static_cast<unsigned char *>(q));
+          cuda_check(cudaMalloc(&q, sizeof(double) * B.Z.size * C::ns), "cudaMalloc rate");
+          sur_arrays_.push_back(q);
+          rate_store_.push_back(static_cast<double *>(q));
+        }
+      }
+      for (size_t b = 0; b < blocks_.size(); ++b) {
+        blocks_[b].chem_quiet = sur_on_ ? quiet_store_.at(b) : nullptr;
+        blocks_[b].chem_rate = sur_on_ ? rate_store_.at(b) : nullptr;
+      }
+      cuda_check(cudaMemcpy(d_blocks_, blocks_.data(), sizeof(DevBlock) * blocks_.size(), cudaMemcpyHostToDevice),
+                 "copy blocks");
+    }
+    // the step graphs and the parameter block change
+    for (auto &g : graphs_)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+    static_owner() = nullptr;
+    upload_params();
+  }
+
+  void surrogate_stats(unsigned long long out[2]) override {
+    out[0] = out[1] = 0;
+    if (!d_sur_stats_) return;
+    cuda_check(cudaMemcpy(out, d_sur_stats_, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost), "stats");
+    int err = 0;
+    cuda_check(cudaMemcpy(&err, d_sur_err_, sizeof(int), cudaMemcpyDeviceToHost), "surrogate err");
+    if (err) throw std::runtime_error("CUDA error in the surrogate kernel: a tensor-core wait timed out");
+  }
+
+  // surrogate increments with the trust gate, then the EPI fallback
+  void launch_chemistry_split() {
+    if constexpr (C::mix == 2) {
+      const int fb_smem = static_cast<int>(2 * std::max(1, setup_.params.nr) * 128 * sizeof(double));
+      for (int b = 0; b < static_cast<int>(blocks_.size()); ++b) {
+        const DevBlock &B = blocks_[b];
+        const int64_t cells = static_cast<int64_t>(B.mx) * B.my * B.mz;
+        cuda_check(cudaMemsetAsync(d_fb_count_, 0, sizeof(int), stream_), "memset fallback");
+        sur::k_sur_infer<C><<<static_cast<unsigned>((cells + 127) / 128), sur::kThreads, sur::kSmem, stream_>>>(
+            d_blocks_, b, sur_, 0, d_fb_count_, d_fb_list_, d_sur_stats_, d_sur_err_);
+        mark("surrogate");
+        sur::k_sur_fallback<C><<<148 * 4, 128, fb_smem, stream_>>>(d_blocks_, b, d_fb_count_, d_fb_list_);
+        mark("epi_fallback");
+      }
+    }
   }
 
   void launch_update() {
@@ -544,6 +652,13 @@ class EngineT final : public Engine {
   size_t source_smem_ = 0, flux_smem_ = 0;
   int final_dq_ = 0;
   cudaGraphExec_t graphs_[4] = {nullptr, nullptr, nullptr, nullptr};
+  bool sur_on_ = false;
+  SurrogateDev sur_{};
+  int *d_fb_count_ = nullptr, *d_fb_list_ = nullptr, *d_sur_err_ = nullptr;
+  unsigned long long *d_sur_stats_ = nullptr;
+  std::vector<void *> sur_arrays_;
+  std::vector<unsigned char *> quiet_store_;
+  std::vector<double *> rate_store_;
   cudaEvent_t ev0_{}, ev1_{};
   double last_ms_ = 0;
 };

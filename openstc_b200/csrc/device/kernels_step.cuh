@@ -40,6 +40,13 @@ __global__ void __launch_bounds__(kCta) k_source(const DevBlock *__restrict__ bl
     }
   }
   if constexpr (C::mix == 2) {
+    if (B.chem_quiet && B.chem_quiet[nz]) {
+      // judged chemically quiet by the surrogate: its rate, no Jacobian
+      const double jac = ld(B.jac + n);
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) dq[l + 5] = jac * B.chem_rate[l * sz0 + nz];
+      const int nj = cP.chem_src_method == 1 ? NS * NS : (cP.chem_src_method == 2 ? NS : 0);
+      for (int q = 0; q < nj; ++q) B.chem_jac[q * sz0 + nz] = 0;
+    } else {
     const int tid = threadIdx.x + kTX * (threadIdx.y + kTY * threadIdx.z);
     double *q1 = sq + tid, *q2 = sq + cP.nr * kCta + tid;
     double Y[NS], omega[NS], omega_d[NS];
@@ -72,6 +79,7 @@ __global__ void __launch_bounds__(kCta) k_source(const DevBlock *__restrict__ bl
         if (Y[l] > 1e-25) v = -omega_d[l] / (Y[l] * density);
         B.chem_jac[l * sz0 + nz] = v;
       }
+    }
     }
   }
   OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq[l * szd + nd] = dq[l];

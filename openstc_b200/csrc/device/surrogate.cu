@@ -14,7 +14,7 @@
 #include <string>
 
 #include "engine.hpp"
-#include "kernels_step.cuh"
+#include "kernels_surrogate.cuh"
 #include "openstc_b200.h"
 #include "surrogate.hpp"
 #include "tc_gemm.cuh"
@@ -73,9 +73,15 @@ __device__ inline double gauss(uint64_t &s) {
 __device__ inline uint16_t bf16(float v) { return __bfloat16_as_ushort(__float2bfloat16_rn(v)); }
 __device__ inline float from_bf16(uint16_t v) { return __bfloat162float(__ushort_as_bfloat16(v)); }
 
-__device__ inline float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
+// GELU in its tanh form (the inference kernel evaluates the same form with
+// the hardware tanh)
+__device__ inline float gelu(float x) {
+  const float t = tanhf(0.7978845608028654f * (x + 0.044715f * x * x * x));
+  return 0.5f * x * (1.f + t);
+}
 __device__ inline float gelu_grad(float x) {
-  return 0.5f * (1.f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+  const float t = tanhf(0.7978845608028654f * (x + 0.044715f * x * x * x));
+  return 0.5f * (1.f + t) + 0.5f * x * (1.f - t * t) * 0.7978845608028654f * (1.f + 3.f * 0.044715f * x * x);
 }
 
 // ------------------------------------------------------------------ samples
@@ -122,49 +128,18 @@ __global__ void k_sample(double *states, int64_t n, uint64_t seed, DevBlock F, i
   o[11] = dt;
 }
 
-// One FP64 EPI step at fixed density: rho dY = (I - dt J)^-1 dt omega, with
-// omega and J as the solver computes them (finite_rate_chemistry and
-// compute_chem_src_jacobian, src/FiniteRateChem.cu:7-194; EPI, :211-234).
-__device__ inline void epi_increment(double T, double p, const double *Y, double dt, double *q1, double *q2,
-                                     int stride, double *dy) {
-  double mw_inv = 0;
-  for (int k = 0; k < NS; ++k) mw_inv += Y[k] / cP.mw[k];
-  const double rho = p / (kDR_u * T * mw_inv);
-  double omega[NS], omega_d[NS];
-  chemistry<NS>(rho, T, Y, omega, omega_d, q1, q2, stride);
-  double lhs[NS * NS];
-  const int nr = cP.nr;
-  for (int m = 0; m < NS; ++m) {
-    for (int q = 0; q < NS; ++q) {
-      double zz = 0;
-      if (Y[q] > 1e-25) {
-        for (int r = 0; r < nr; ++r) {
-          const int dn = cP.sb[r * NS + m] - cP.sf[r * NS + m];
-          if (dn == 0) continue;
-          zz += dn * (cP.sf[r * NS + q] * q1[r * stride] - cP.sb[r * NS + q] * q2[r * stride]);
-        }
-        zz /= rho * Y[q];
-      }
-      const double J = cP.mw[m] * zz * 1e+3;
-      lhs[m * NS + q] = (m == q ? 1.0 : 0.0) - dt * J;
-    }
-  }
-  int piv[NS];
-  lu_factor<NS>(lhs, piv);
-  double x[NS];
-  for (int k = 0; k < NS; ++k) x[k] = omega[k];
-  lu_solve<NS>(lhs, piv, x);
-  for (int k = 0; k < NS; ++k) dy[k] = dt * x[k] / rho;
-}
-
 __global__ void __launch_bounds__(128) k_label(const double *states, double *dy, int64_t n) {
   extern __shared__ double sq[];
   const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
   if (i >= n) return;
   const double *s = states + i * kSurIn;
-  double Y[NS], d[NS];
-  for (int k = 0; k < NS; ++k) Y[k] = s[2 + k];
-  epi_increment(s[0], s[1], Y, s[11], sq + threadIdx.x, sq + cP.nr * blockDim.x + threadIdx.x, blockDim.x, d);
+  double Y[NS], d[NS], mw_inv = 0;
+  for (int k = 0; k < NS; ++k) {
+    Y[k] = s[2 + k];
+    mw_inv += Y[k] / cP.mw[k];
+  }
+  const double rho = s[1] / (kDR_u * s[0] * mw_inv);
+  sur::epi_increment<NS>(s[0], rho, Y, s[11], sq + threadIdx.x, sq + cP.nr * blockDim.x + threadIdx.x, blockDim.x, d);
   for (int k = 0; k < NS; ++k) dy[i * NS + k] = d[k];
 }
 
@@ -195,8 +170,9 @@ __global__ void k_stats(const double *states, const double *dy, int64_t n, doubl
   for (int q = threadIdx.x; q < 2 * kSurIn + kSurOut; q += blockDim.x) atomicAdd(&acc[q], sh[q]);
 }
 
-// features x = (f - mu) / sig; targets t_k = asinh(dY_k / c_k) / s_k (the
-// signed-log transform tames the heavy tail of the increments)
+// features x = (f - mu) / sig; targets t_k = asinh(r_k / c_k) / s_k of the
+// relative increments r_k = dY_k / (Y_k + eps) (the signed-log transform tames
+// their heavy tail)
 struct Norm {
   float mu[kSurIn], sig[kSurIn], c[kSurOut], s[kSurOut];
 };
@@ -209,7 +185,9 @@ __global__ void k_features(const double *states, const double *dy, int64_t n, No
   for (int q = 0; q < kSurInPad; ++q) x[i * kSurInPad + q] = q < kSurIn ? bf16((f[q] - nm.mu[q]) / nm.sig[q]) : 0;
   if (t)
     for (int q = 0; q < kSurOutPad; ++q)
-      t[i * kSurOutPad + q] = q < kSurOut ? static_cast<float>(asinh(dy[i * NS + q] / nm.c[q]) / nm.s[q]) : 0.f;
+      t[i * kSurOutPad + q] =
+          q < kSurOut ? static_cast<float>(asinh(dy[i * NS + q] / (states[i * kSurIn + 2 + q] + kSurYEps) / nm.c[q]) / nm.s[q])
+                      : 0.f;
 }
 
 // ---------------------------------------------------------------- training
@@ -329,7 +307,7 @@ __global__ void k_adam(float *p, const float *g, float *m, float *v, int64_t n, 
 }
 
 // bf16 copies of a weight [dout x din]: row-major, transposed, and in the
-// tile order of the fused inference kernel (K chunks of min(64, din)).
+// tile order of the fused inference kernel (K chunks of min(32, din)).
 __global__ void k_pack(const float *w, int dout, int din, uint16_t *wb, uint16_t *wbt, uint8_t *wp) {
   const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
   if (i >= static_cast<int64_t>(dout) * din) return;
@@ -337,7 +315,7 @@ __global__ void k_pack(const float *w, int dout, int din, uint16_t *wb, uint16_t
   const uint16_t v = bf16(w[i]);
   wb[i] = v;
   wbt[static_cast<int64_t>(k) * dout + r] = v;
-  const int bk = din < 64 ? din : 64;
+  const int bk = din < 32 ? din : 32;
   const int c = k / bk, kk = k % bk;
   *reinterpret_cast<uint16_t *>(wp + static_cast<size_t>(c) * dout * bk * 2 + tc::tile_offset(r, kk, bk)) = v;
 }
@@ -463,11 +441,14 @@ void Surrogate::generate(int64_t n, uint64_t seed, const DevBlock *field, double
     in_sig[q] = nm.sig[q] = static_cast<float>(std::sqrt(var));
   }
   {
-    // target transform from a sub-sample of the labels: c_k = median |dY_k|,
-    // s_k = RMS of asinh(dY_k / c_k)
+    // target transform from a sub-sample: c_k = median |r_k|, s_k = RMS of
+    // asinh(r_k / c_k), r_k = dY_k / (Y_k + eps)
     const int64_t m = std::min<int64_t>(n, 1 << 18);
-    std::vector<double> lab(static_cast<size_t>(m) * NS);
+    std::vector<double> lab(static_cast<size_t>(m) * NS), st(static_cast<size_t>(m) * kSurIn);
     ck(cudaMemcpy(lab.data(), labels_, lab.size() * 8, cudaMemcpyDeviceToHost), "labels copy");
+    ck(cudaMemcpy(st.data(), states_, st.size() * 8, cudaMemcpyDeviceToHost), "states copy");
+    for (int64_t i = 0; i < m; ++i)
+      for (int q = 0; q < NS; ++q) lab[i * NS + q] /= st[i * kSurIn + 2 + q] + kSurYEps;
     for (int q = 0; q < kSurOut; ++q) {
       std::vector<double> a(static_cast<size_t>(m));
       for (int64_t i = 0; i < m; ++i) a[i] = std::fabs(lab[i * NS + q]);
@@ -663,26 +644,16 @@ void Surrogate::label_host(const double *states, int64_t n, double *dy) {
 }
 
 namespace {
-// gate + increments of predictions z (batch x 16, normalised, bias added)
-__global__ void k_decode(const float *z, const double *states, int64_t n, Norm nm, SurrogateDev gd, double *dy,
+// decode, project and gate the predictions z (batch x 16, bias added)
+__global__ void k_decode(const float *z, const double *states, int64_t n, SurrogateDev gd, double *dy,
                          int *accepted) {
   const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
   if (i >= n) return;
   const double *s = states + i * kSurIn;
+  float o[NS];
+  for (int k = 0; k < NS; ++k) o[k] = z[i * kSurOutPad + k];
   double d[NS];
-  for (int k = 0; k < NS; ++k) d[k] = nm.c[k] * sinh(static_cast<double>(z[i * kSurOutPad + k]) * nm.s[k]);
-  const float T = static_cast<float>(s[0]), lp = static_cast<float>(log10(s[1])),
-              ldt = static_cast<float>(log10(s[11]));
-  bool ok = T >= gd.gate.t_min && T <= gd.gate.t_max && lp >= gd.gate.lp_min && lp <= gd.gate.lp_max &&
-            ldt >= gd.gate.ldt_min && ldt <= gd.gate.ldt_max;
-  for (int e = 0; e < gd.n_elem && ok; ++e) {
-    double defect = 0, total = 0;
-    for (int k = 0; k < NS; ++k) {
-      defect += gd.elem[e * kMaxSpec + k] * d[k];
-      total += gd.elem[e * kMaxSpec + k] * s[2 + k];
-    }
-    if (total > 0 && fabs(defect) > gd.gate.defect_tol * total) ok = false;
-  }
+  const bool ok = sur::decode<NS>(gd, o, s[0], log10(s[1]), log10(s[11]), s + 2, d);
   for (int k = 0; k < NS; ++k) dy[i * NS + k] = d[k];
   accepted[i] = ok ? 1 : 0;
 }
@@ -705,12 +676,7 @@ void Surrogate::predict_host(const double *states, int64_t n, double *dy, int *a
   const int L = kSurLayers - 1;
   k_act<<<dim3(1, (batch + 31) / 32), dim3(32, 8), 0, stream_>>>(z_[L], batch, kSurOutPad, b_[L], nullptr, 0, z_[L],
                                                                    dz_, dzt_);
-  Norm nm{};
-  for (int q = 0; q < kSurOut; ++q) {
-    nm.s[q] = out_s[q];
-    nm.c[q] = out_c[q];
-  }
-  k_decode<<<(n + 255) / 256, 256, 0, stream_>>>(z_[L], s, n, nm, device_params(), d, acc);
+  k_decode<<<(n + 255) / 256, 256, 0, stream_>>>(z_[L], s, n, device_params(), d, acc);
   ck(cudaGetLastError(), "predict");
   ck(cudaMemcpyAsync(dy, d, n * NS * 8, cudaMemcpyDeviceToHost, stream_), "predict download");
   ck(cudaMemcpyAsync(accepted, acc, n * sizeof(int), cudaMemcpyDeviceToHost, stream_), "predict download");
@@ -837,7 +803,7 @@ const SurrogateDev &Surrogate::device_params() {
 void Surrogate::save(const std::string &path) const {
   std::ofstream f(path, std::ios::binary);
   if (!f) throw std::runtime_error("cannot write " + path);
-  const char magic[8] = {'O', 'S', 'T', 'C', 'M', 'L', 'P', '2'};
+  const char magic[8] = {'O', 'S', 'T', 'C', 'M', 'L', 'P', '3'};
   f.write(magic, 8);
   f.write(reinterpret_cast<const char *>(in_mu.data()), sizeof(in_mu));
   f.write(reinterpret_cast<const char *>(in_sig.data()), sizeof(in_sig));
@@ -852,7 +818,7 @@ void Surrogate::load(const std::string &path) {
   if (!f) throw std::runtime_error("cannot open " + path);
   char magic[8];
   f.read(magic, 8);
-  if (std::memcmp(magic, "OSTCMLP2", 8) != 0) throw std::runtime_error(path + " is not a surrogate file");
+  if (std::memcmp(magic, "OSTCMLP3", 8) != 0) throw std::runtime_error(path + " is not a surrogate file");
   f.read(reinterpret_cast<char *>(in_mu.data()), sizeof(in_mu));
   f.read(reinterpret_cast<char *>(in_sig.data()), sizeof(in_sig));
   f.read(reinterpret_cast<char *>(out_c.data()), sizeof(out_c));

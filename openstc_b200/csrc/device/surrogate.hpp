@@ -26,6 +26,9 @@ constexpr int kSurOutPad = 16;  // N of the last layer
 constexpr int kSurHidden = 256;
 constexpr int kSurLayers = 5;  // 4 hidden (GELU) + linear output
 constexpr int kMaxElem = 8;
+// The network predicts the relative increment r_k = dY_k / (Y_k + kSurYEps)
+// through t_k = asinh(r_k / c_k) / s_k.
+constexpr double kSurYEps = 1e-10;
 
 // Trust region of the network: its training box.
 struct SurrogateGate {
@@ -33,6 +36,8 @@ struct SurrogateGate {
   float lp_min = 4.5f, lp_max = 6.0f;      // log10 p [Pa]
   float ldt_min = -9.0f, ldt_max = -6.0f;  // log10 dt [s]
   float defect_tol = 1e-3f;                // element-conservation defect (relative)
+  float rel_max = 0.05f;                   // largest accepted |dY_k| / (Y_k + eps)
+  float out_max = 6.f;                     // largest accepted |network output|
 };
 
 // Parameters the fused inference kernel reads (device memory).
@@ -84,7 +89,7 @@ class Surrogate {
   cudaStream_t stream() const { return stream_; }
   // the normalisation (features and targets)
   std::array<float, kSurIn> in_mu{}, in_sig{};
-  std::array<float, kSurOut> out_c{}, out_s{};  // dY_k = c_k sinh(s_k * output_k)
+  std::array<float, kSurOut> out_c{}, out_s{};  // dY_k = (Y_k + eps) c_k sinh(s_k * output_k)
   SurrogateGate gate;
 
  private:

@@ -65,7 +65,8 @@ def test_gradients_match_oracle(drv):
     loss, g = sur.gradients(st, dy)
     mu, sig, c, sc = sur.normalisation()
     x = mlp_oracle.features(st, mu, sig)
-    t = (np.arcsinh(dy / c.astype(np.float64)) / sc.astype(np.float64)).astype(np.float32).astype(np.float64)
+    r = dy / (st[:, 2:11] + 1e-10)
+    t = (np.arcsinh(r / c.astype(np.float64)) / sc.astype(np.float64)).astype(np.float32).astype(np.float64)
     loss_ref, g_ref = mlp_oracle.loss_and_grads(sur.params(), x, t)
     assert abs(loss - loss_ref) <= 1e-4 * abs(loss_ref)
     off = 0
@@ -96,3 +97,59 @@ def test_training_learns_and_gate(drv, tmp_path):
     b, gb = other.predict(st)
     assert np.array_equal(a, b) and np.array_equal(ga, gb)
     print("held-out:", ev)
+
+
+def cell_states(d):
+    """(T, p, Y[9], dt) of every interior cell of block 0, i fastest."""
+    info = d.info()
+    g = info.ngg
+    bv = d.get(0, "bv")[:, g:-g, g:-g, g:-g]
+    sv = d.get(0, "sv")[:, g:-g, g:-g, g:-g]
+    dt = d.get(0, "dt_local")[0]
+    n = dt.size
+    st = np.zeros((n, 12))
+    st[:, 0] = bv[5].ravel()
+    st[:, 1] = bv[4].ravel()
+    for k in range(9):
+        st[:, 2 + k] = sv[k].ravel()
+    st[:, 11] = dt.ravel()
+    return st
+
+
+@pytest.fixture(scope="module")
+def trained(drv, tmp_path_factory):
+    case = tmp_path_factory.mktemp("sur_field") / "ml"
+    cases.mixing_layer_case(case, mx=24, my=16, mz=8, total_step=1, output_screen=1)
+    field = ostc.Driver(case, precision="mixed")
+    field.initialize()
+    field.step(20)
+    sur = ostc.Surrogate(field, seed=17)
+    sur.generate(1 << 18, seed=5, field=field, field_fraction=0.9)
+    sur.train(500, batch=16384, lr=2e-3)
+    return case, field, sur
+
+
+def test_fused_inference_matches_unfused(trained):
+    case, field, sur = trained
+    st = cell_states(field)
+    dy_net, acc_net = sur.predict(st)
+    dy_epi = sur.label(st)
+    g = field.info().ngg
+    y0 = field.get(0, "sv")[:9, g:-g, g:-g, g:-g].reshape(9, -1).T.copy()
+    field.set_surrogate(sur)
+    field.run_phase("chemistry")
+    y1 = field.get(0, "sv")[:9, g:-g, g:-g, g:-g].reshape(9, -1).T
+    dy = y1 - y0
+    acc, fb = field.chemistry_stats()
+    assert acc + fb == st.shape[0]
+    # cells that took the EPI fallback: the same FP64 step as the labels
+    scale = np.abs(dy_epi).max(axis=1, keepdims=True) + 1e-30
+    epi_like = np.all(np.abs(dy - dy_epi) <= 1e-9 * scale + 1e-15, axis=1)
+    # the fused kernel evaluates GELU with the hardware tanh: increments agree
+    # to a few per cent of the cell's largest increment (floor 1e-13)
+    net_like = np.all(np.abs(dy - dy_net) <= 5e-2 * np.abs(dy_net).max(axis=1, keepdims=True) + 1e-13, axis=1)
+    assert np.all(epi_like | net_like)
+    # where the unfused gate accepted, the fused kernel gave the network's increment
+    assert np.mean(net_like[acc_net]) > 0.98, np.mean(net_like[acc_net])
+    field.set_surrogate(None)
+    print("fused: accepted", acc, "fallback", fb)
