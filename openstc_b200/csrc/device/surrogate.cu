@@ -93,6 +93,7 @@ __global__ void k_sample(double *states, int64_t n, uint64_t seed, DevBlock F, i
   if (i >= n) return;
   uint64_t s = mix64(seed ^ mix64(static_cast<uint64_t>(i) + 1));
   double T, p, Y[NS];
+  double dt = pow(10.0, g.ldt_min + (g.ldt_max - g.ldt_min) * u01(s));
   if (use_field && u01(s) < field_fraction) {
     const int64_t cells = static_cast<int64_t>(F.mx) * F.my * F.mz;
     int64_t c = static_cast<int64_t>(u01(s) * cells);
@@ -100,14 +101,17 @@ __global__ void k_sample(double *states, int64_t n, uint64_t seed, DevBlock F, i
     const int ci = static_cast<int>(c % F.mx), cj = static_cast<int>((c / F.mx) % F.my),
               ck = static_cast<int>(c / (static_cast<int64_t>(F.mx) * F.my));
     const int64_t m = F.G.at(ci, cj, ck), sz = F.G.size;
-    T = F.bv[5 * sz + m] * (1.0 + 0.05 * gauss(s));
-    p = F.bv[4 * sz + m] * (1.0 + 0.05 * gauss(s));
+    T = F.bv[5 * sz + m] * (1.0 + 0.02 * gauss(s));
+    p = F.bv[4 * sz + m] * (1.0 + 0.02 * gauss(s));
     double sum = 0;
     for (int k = 0; k < NS; ++k) {
-      Y[k] = fmax(F.sv[k * sz + m], 0.0) * exp(0.3 * gauss(s));
+      Y[k] = fmax(F.sv[k * sz + m], 0.0) * exp(0.1 * gauss(s));
       sum += Y[k];
     }
     for (int k = 0; k < NS; ++k) Y[k] /= sum;
+    // the cell's own local time step, perturbed within a factor of 2
+    const double dtc = F.dt_local[F.Z.at(ci, cj, ck)];
+    if (dtc > 0) dt = dtc * pow(10.0, 0.6 * u01(s) - 0.3);
   } else {
     T = g.t_min + (g.t_max - g.t_min) * u01(s);
     p = pow(10.0, g.lp_min + (g.lp_max - g.lp_min) * u01(s));
@@ -120,7 +124,6 @@ __global__ void k_sample(double *states, int64_t n, uint64_t seed, DevBlock F, i
   }
   T = fmin(fmax(T, static_cast<double>(g.t_min)), static_cast<double>(g.t_max));
   p = fmin(fmax(p, pow(10.0, static_cast<double>(g.lp_min))), pow(10.0, static_cast<double>(g.lp_max)));
-  const double dt = pow(10.0, g.ldt_min + (g.ldt_max - g.ldt_min) * u01(s));
   double *o = states + i * kSurIn;
   o[0] = T;
   o[1] = p;
@@ -449,6 +452,16 @@ void Surrogate::generate(int64_t n, uint64_t seed, const DevBlock *field, double
     ck(cudaMemcpy(st.data(), states_, st.size() * 8, cudaMemcpyDeviceToHost), "states copy");
     for (int64_t i = 0; i < m; ++i)
       for (int q = 0; q < NS; ++q) lab[i * NS + q] /= st[i * kSurIn + 2 + q] + kSurYEps;
+    // the trust region in dt follows the data (field samples carry the
+    // cells' own local time steps)
+    double ldt_lo = 1e30, ldt_hi = -1e30;
+    for (int64_t i = 0; i < m; ++i) {
+      const double l = std::log10(st[i * kSurIn + 11]);
+      ldt_lo = std::min(ldt_lo, l);
+      ldt_hi = std::max(ldt_hi, l);
+    }
+    gate.ldt_min = static_cast<float>(ldt_lo - 0.1);
+    gate.ldt_max = static_cast<float>(ldt_hi + 0.1);
     for (int q = 0; q < kSurOut; ++q) {
       std::vector<double> a(static_cast<size_t>(m));
       for (int64_t i = 0; i < m; ++i) a[i] = std::fabs(lab[i * NS + q]);
