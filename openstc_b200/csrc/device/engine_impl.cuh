@@ -438,7 +438,7 @@ class EngineT final : public Engine {
       for (int b = 0; b < static_cast<int>(blocks_.size()); ++b) {
         const DevBlock &B = blocks_[b];
         const int64_t cells = static_cast<int64_t>(B.mx) * B.my * B.mz;
-        sur::k_sur_infer<C><<<static_cast<unsigned>((cells + 127) / 128), sur::kThreads, sur::kSmem, stream_>>>(
+        sur::k_sur_infer<C><<<static_cast<unsigned>((cells + sur::kCells - 1) / sur::kCells), sur::kThreads, sur::kSmem, stream_>>>(
             d_blocks_, b, sur_, 1, d_fb_count_, d_fb_list_, d_sur_stats_, d_sur_err_);
         mark("surrogate");
       }
@@ -549,7 +549,7 @@ class EngineT final : public Engine {
         const DevBlock &B = blocks_[b];
         const int64_t cells = static_cast<int64_t>(B.mx) * B.my * B.mz;
         cuda_check(cudaMemsetAsync(d_fb_count_, 0, sizeof(int), stream_), "memset fallback");
-        sur::k_sur_infer<C><<<static_cast<unsigned>((cells + 127) / 128), sur::kThreads, sur::kSmem, stream_>>>(
+        sur::k_sur_infer<C><<<static_cast<unsigned>((cells + sur::kCells - 1) / sur::kCells), sur::kThreads, sur::kSmem, stream_>>>(
             d_blocks_, b, sur_, 0, d_fb_count_, d_fb_list_, d_sur_stats_, d_sur_err_);
         mark("surrogate");
         sur::k_sur_fallback<C><<<148 * 4, 128, fb_smem, stream_>>>(d_blocks_, b, d_fb_count_, d_fb_list_);

@@ -128,38 +128,55 @@ __device__ inline bool decode(const SurrogateDev &p, const float *o, double T, d
 }
 
 // ------------------------------------------------------------ fused kernel
-constexpr int kThreads = 256;  // 8 warps: 2 per TMEM lane quarter
-constexpr int kChunk = 32;     // K columns of a weight stage
+// One CTA per SM handles two 128-cell tiles per pass over the weights (two
+// accumulators fill the 512 TMEM columns), so every weight byte staged from
+// L2 feeds two MMAs.  The weights stream through a ring of bulk copies in
+// 8 KB chunks far enough ahead to cover the L2 latency.
+constexpr int kTiles = 2;
+constexpr int kCells = 128 * kTiles;
+constexpr int kThreads = 512;  // 16 warps: 4 per TMEM lane quarter (tile x column half)
+constexpr int kStages = 10;    // weight chunks in flight
+constexpr int kLag = 2;        // chunk groups that may still be executing when their stage is refilled
+// Every weight chunk is 8 KB: one K=16 slice [256 x 16] of a hidden layer,
+// the whole first layer [256 x 16] or the whole output layer [16 x 256],
+// all packed K-major canonical with 16-column tiles.
+constexpr uint32_t kChunkBytes = kSurHidden * 16 * 2;
+constexpr int kChunks = 1 + 3 * (kSurHidden / 16) + 1;
 constexpr uint32_t kA0Bytes = 128 * kSurInPad * 2;
 constexpr uint32_t kA1Bytes = 128 * kSurHidden * 2;
-constexpr uint32_t kStageBytes = kSurHidden * kChunk * 2;
-constexpr uint32_t kSmem = kA0Bytes + kA1Bytes + 2 * kStageBytes + 64;
+constexpr uint32_t kSmem = kTiles * (kA0Bytes + kA1Bytes) + kStages * kChunkBytes + (2 * kStages + 2) * 8 + 16;
 
-// 16-byte chunks of a packed weight block into shared memory
-__device__ __forceinline__ void copy_bytes(uint8_t *dst, const uint8_t *src, uint32_t bytes) {
-  for (uint32_t q = threadIdx.x * 16; q < bytes; q += kThreads * 16)
-    *reinterpret_cast<uint4 *>(dst + q) = __ldg(reinterpret_cast<const uint4 *>(src + q));
+// Source of weight chunk i in the stream
+__device__ __forceinline__ const uint8_t *chunk_src(const SurrogateDev &P, int i) {
+  if (i == 0) return P.w_packed[0];
+  if (i == kChunks - 1) return P.w_packed[4];
+  const int l = 1 + (i - 1) / (kSurHidden / 16), c = (i - 1) % (kSurHidden / 16);
+  return P.w_packed[l] + static_cast<size_t>(c) * kChunkBytes;
 }
 
-struct Phases {
-  uint32_t ph[3] = {0, 0, 0};
-};
-
-// Waits for the commit on bar[i]; false on timeout (all threads agree).
-__device__ __forceinline__ bool wait_bar(uint64_t *bar, int i, Phases &P) {
-  const bool ok = tc::mbar_wait(&bar[i], P.ph[i]);
-  P.ph[i] ^= 1;
-  return __syncthreads_and(ok) != 0;
+// Asynchronous bulk copy of one chunk into shared memory; completion is
+// counted in bytes on the stage's mbarrier.
+__device__ __forceinline__ void load_chunk(uint8_t *dst, const uint8_t *src, uint64_t *full) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(kChunkBytes), "r"(tc::smem_u32(full))
+               : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   tc::smem_u32(dst)),
+               "l"(src), "r"(kChunkBytes), "r"(tc::smem_u32(full))
+               : "memory");
 }
 
 // Epilogue of a hidden layer: accumulator + bias -> GELU -> bf16 rows of the
-// next layer's input tile (K-major canonical, 256 columns).
+// next layer's input tile (K-major canonical, 256 columns).  Warp w reads
+// TMEM lane quarter w % 4 of tile (w / 4) / 2, column half (w / 4) % 2.
 __device__ __forceinline__ void hidden_epilogue(uint32_t tmem, const float *bias, uint8_t *a1) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int row = (warp & 3) * 32 + lane, half = warp >> 2;
+  const int quarter = warp & 3, tile = (warp >> 2) >> 1, half = (warp >> 2) & 1;
+  const int row = quarter * 32 + lane;
+  uint8_t *a = a1 + tile * kA1Bytes;
+  const uint32_t tbase = tmem + (static_cast<uint32_t>(quarter * 32) << 16) + tile * kSurHidden;
   for (int c0 = half * 128; c0 < half * 128 + 128; c0 += 32) {
     float v[32];
-    tc::tmem_ld32(tmem + (static_cast<uint32_t>((warp & 3) * 32) << 16) + c0, v);
+    tc::tmem_ld32(tbase + c0, v);
 #pragma unroll
     for (int q = 0; q < 32; q += 8) {
       uint32_t pk[4];
@@ -170,12 +187,12 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t tmem, const float *bias
         const __nv_bfloat162 b2 = __floats2bfloat162_rn(x0, x1);
         pk[h] = *reinterpret_cast<const uint32_t *>(&b2);
       }
-      *reinterpret_cast<uint4 *>(a1 + tc::tile_offset(row, c0 + q, kSurHidden)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+      *reinterpret_cast<uint4 *>(a + tc::tile_offset(row, c0 + q, kSurHidden)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
     }
   }
 }
 
-// One 128-cell tile per CTA: features -> 4 x (256, GELU) -> 9 outputs on the
+// Two 128-cell tiles per CTA: features -> 4 x (256, GELU) -> 9 outputs on the
 // tensor cores, then decode, project and gate, with dt = the cell's local
 // time step.  mode 1 (in the step, before the source term): accepted cells
 // are marked chemically quiet and get the rate rho dY / dt, the others keep
@@ -188,18 +205,18 @@ __global__ void __launch_bounds__(kThreads) k_sur_infer(const DevBlock *__restri
                                                         unsigned long long *stats, int *err) {
   constexpr int NS = C::ns;
   extern __shared__ __align__(128) uint8_t smem[];
-  uint8_t *a0 = smem, *a1 = smem + kA0Bytes;
-  uint8_t *stage[2] = {a1 + kA1Bytes, a1 + kA1Bytes + kStageBytes};
-  uint64_t *bar = reinterpret_cast<uint64_t *>(stage[1] + kStageBytes);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 3);
+  uint8_t *a0 = smem, *a1 = smem + kTiles * kA0Bytes, *stages = a1 + kTiles * kA1Bytes;
+  uint64_t *full = reinterpret_cast<uint64_t *>(stages + kStages * kChunkBytes);
+  uint64_t *empty = full + kStages, *acc_bar = empty + kStages;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(acc_bar + 1);
   const DevBlock &B = blks[b];
   const int tid = threadIdx.x, warp = tid >> 5;
   const int64_t cells = static_cast<int64_t>(B.mx) * B.my * B.mz;
   const int64_t sz = B.G.size;
 
-  // features of this tile's cells (one thread per row)
-  if (tid < 128) {
-    const int64_t c = static_cast<int64_t>(blockIdx.x) * 128 + tid;
+  // features of the CTA's cells: thread t < 256 -> tile t / 128, row t % 128
+  if (tid < kCells) {
+    const int64_t c = static_cast<int64_t>(blockIdx.x) * kCells + tid;
     float f[kSurInPad];
 #pragma unroll
     for (int q = 0; q < kSurInPad; ++q) f[q] = 0.f;
@@ -215,6 +232,7 @@ __global__ void __launch_bounds__(kThreads) k_sur_infer(const DevBlock *__restri
 #pragma unroll
       for (int q = 0; q < kSurIn; ++q) f[q] = (raw[q] - P.in_mu[q]) / P.in_sig[q];
     }
+    uint8_t *a = a0 + (tid >> 7) * kA0Bytes;
 #pragma unroll
     for (int q = 0; q < kSurInPad; q += 8) {
       uint32_t pk[4];
@@ -223,132 +241,136 @@ __global__ void __launch_bounds__(kThreads) k_sur_infer(const DevBlock *__restri
         const __nv_bfloat162 b2 = __floats2bfloat162_rn(f[q + 2 * h], f[q + 2 * h + 1]);
         pk[h] = *reinterpret_cast<const uint32_t *>(&b2);
       }
-      *reinterpret_cast<uint4 *>(a0 + tc::tile_offset(tid, q, kSurInPad)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+      *reinterpret_cast<uint4 *>(a + tc::tile_offset(tid & 127, q, kSurInPad)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
     }
   }
-  if (warp == 0) tc::tmem_alloc(tslot, 256);
+  if (warp == 0) tc::tmem_alloc(tslot, 512);
   if (tid == 0) {
-    for (int q = 0; q < 3; ++q) tc::mbar_init(&bar[q], 1);
+    for (int q = 0; q < kStages; ++q) {
+      tc::mbar_init(&full[q], 1);
+      tc::mbar_init(&empty[q], 1);
+    }
+    tc::mbar_init(acc_bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int q = 0; q < kStages; ++q) load_chunk(stages + q * kChunkBytes, chunk_src(P, q), &full[q]);
   }
-  // layer 0 weights (256 x 16) into stage 0
-  copy_bytes(stage[0], P.w_packed[0], kSurHidden * kSurInPad * 2);
   tc::fence_async_smem();
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = *tslot;
-  Phases ph;
   bool ok = true;
-
-  // ---- layer 0: [128 x 16] x [256 x 16]^T
-  if (tid == 0) {
-    const uint64_t ad = tc::desc_kmajor(tc::smem_u32(a0), 128, (kSurInPad / 8) * 128);
-    const uint64_t bd = tc::desc_kmajor(tc::smem_u32(stage[0]), 128, (kSurInPad / 8) * 128);
-    tc::mma_bf16(tmem, ad, bd, tc::idesc_bf16(128, kSurHidden), 0u);
-    tc::commit(&bar[2]);
-  }
-  ok = wait_bar(bar, 2, ph);
-  tc::fence_after_sync();
-  if (ok) hidden_epilogue(tmem, P.bias[0], a1);
-  tc::fence_before_sync();
-  tc::fence_async_smem();
-  __syncthreads();
-
-  // ---- layers 1..3: [128 x 256] x [256 x 256]^T, K in chunks of 32
-  constexpr int nchunk = kSurHidden / kChunk;
-  for (int l = 1; l <= 3 && ok; ++l) {
-    const uint8_t *w = P.w_packed[l];
-    copy_bytes(stage[0], w, kStageBytes);
-    tc::fence_async_smem();
-    __syncthreads();
-    for (int c = 0; c < nchunk && ok; ++c) {
-      const int s = c & 1;
-      if (tid == 0) {
-        tc::fence_after_sync();
-        for (int q = 0; q < kChunk / 16; ++q) {
-          const int k0 = c * kChunk + q * 16;
-          const uint64_t ad = tc::desc_kmajor(tc::smem_u32(a1) + k0 * 16, 128, (kSurHidden / 8) * 128);
-          const uint64_t bd = tc::desc_kmajor(tc::smem_u32(stage[s]) + q * 256, 128, (kChunk / 8) * 128);
-          tc::mma_bf16(tmem, ad, bd, tc::idesc_bf16(128, kSurHidden), (c > 0 || q > 0) ? 1u : 0u);
+  int chunk = 0;         // next chunk of the stream
+  int issued = kStages;  // chunks whose copy has been started
+  constexpr uint32_t kSboA1 = (kSurHidden / 8) * 128, kSbo16 = (16 / 8) * 128;
+  for (int layer = 0; layer < 5; ++layer) {
+    // thread 0 issues this layer's MMAs (both tiles) as the weight chunks
+    // land and refills the stage of the chunk kLag groups back
+    if (tid == 0) {
+      const int n_here = (layer == 0 || layer == 4) ? 1 : kSurHidden / 16;
+      for (int q = 0; q < n_here && ok; ++q, ++chunk) {
+        const int st = chunk % kStages;
+        if (!tc::mbar_wait(&full[st], (chunk / kStages) & 1)) {
+          ok = false;
+          break;
         }
-        tc::commit(&bar[s]);
+        tc::fence_after_sync();
+        const uint32_t wb = tc::smem_u32(stages + st * kChunkBytes);
+        for (int t = 0; t < kTiles; ++t) {
+          const uint32_t acc = tmem + t * kSurHidden;
+          if (layer == 0) {
+            const uint64_t ad = tc::desc_kmajor(tc::smem_u32(a0 + t * kA0Bytes), 128, kSbo16);
+            tc::mma_bf16(acc, ad, tc::desc_kmajor(wb, 128, kSbo16), tc::idesc_bf16(128, kSurHidden), 0u);
+          } else if (layer < 4) {
+            const uint64_t ad = tc::desc_kmajor(tc::smem_u32(a1 + t * kA1Bytes) + q * 16 * 16, 128, kSboA1);
+            tc::mma_bf16(acc, ad, tc::desc_kmajor(wb, 128, kSbo16), tc::idesc_bf16(128, kSurHidden),
+                         q > 0 ? 1u : 0u);
+          } else {
+            for (int kk = 0; kk < kSurHidden / 16; ++kk) {
+              const uint64_t ad = tc::desc_kmajor(tc::smem_u32(a1 + t * kA1Bytes) + kk * 16 * 16, 128, kSboA1);
+              const uint64_t bd = tc::desc_kmajor(wb + kk * (kSurOutPad * 16 * 2), 128, kSbo16);
+              tc::mma_bf16(acc, ad, bd, tc::idesc_bf16(128, kSurOutPad), kk > 0 ? 1u : 0u);
+            }
+          }
+        }
+        tc::commit(&empty[st]);
+        const int old = chunk - kLag;
+        if (old >= 0 && old + kStages < kChunks) {
+          const int os = old % kStages;
+          if (!tc::mbar_wait(&empty[os], (old / kStages) & 1)) {
+            ok = false;
+            break;
+          }
+          load_chunk(stages + os * kChunkBytes, chunk_src(P, old + kStages), &full[os]);
+          ++issued;
+        }
       }
-      if (c + 1 < nchunk) {
-        // stage s^1 was read by the MMAs of chunk c - 1
-        if (c >= 1) ok = wait_bar(bar, s ^ 1, ph);
-        if (!ok) break;
-        copy_bytes(stage[s ^ 1], w + static_cast<size_t>(c + 1) * kStageBytes, kStageBytes);
-        tc::fence_async_smem();
-        __syncthreads();
-      }
+      if (ok) tc::commit(acc_bar);
     }
-    // the last two commits: chunks nchunk-2 (stage 0) and nchunk-1 (stage 1)
-    if (ok) ok = wait_bar(bar, 0, ph);
-    if (ok) ok = wait_bar(bar, 1, ph);
+    ok = __syncthreads_and(ok) != 0;
+    if (!ok) break;
+    ok = __syncthreads_and(tc::mbar_wait(acc_bar, layer & 1)) != 0;
     tc::fence_after_sync();
-    if (ok) hidden_epilogue(tmem, P.bias[l], a1);
+    if (!ok || layer == 4) break;
+    hidden_epilogue(tmem, P.bias[layer], a1);
     tc::fence_before_sync();
     tc::fence_async_smem();
     __syncthreads();
   }
-
-  // ---- output layer: [128 x 256] x [16 x 256]^T (all 8 chunks in one stage)
-  if (ok) {
-    copy_bytes(stage[0], P.w_packed[4], kSurOutPad * kSurHidden * 2);
-    tc::fence_async_smem();
-    __syncthreads();
-    if (tid == 0) {
-      tc::fence_after_sync();
-      for (int q = 0; q < kSurHidden / 16; ++q) {
-        const int k0 = q * 16;
-        const uint64_t ad = tc::desc_kmajor(tc::smem_u32(a1) + k0 * 16, 128, (kSurHidden / 8) * 128);
-        const uint32_t boff = (k0 / kChunk) * (kSurOutPad * kChunk * 2) + (k0 % kChunk) / 8 * 128;
-        const uint64_t bd = tc::desc_kmajor(tc::smem_u32(stage[0]) + boff, 128, (kChunk / 8) * 128);
-        tc::mma_bf16(tmem, ad, bd, tc::idesc_bf16(128, kSurOutPad), q > 0 ? 1u : 0u);
-      }
-      tc::commit(&bar[2]);
-    }
-    ok = wait_bar(bar, 2, ph);
-    tc::fence_after_sync();
+  if (tid == 0) {
+    // copies issued beyond the last consumed chunk (only on a timeout) land
+    // before the CTA exits
+    for (int c = chunk; c < issued; ++c) tc::mbar_wait(&full[c % kStages], (c / kStages) & 1);
   }
+  // outputs: warps with (w / 4) % 2 == 0 read their tile's 16 output columns
+  const int quarter = warp & 3, tile = (warp >> 2) >> 1, half = (warp >> 2) & 1;
   float o[32];
-  if (ok && warp < 4) tc::tmem_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16), o);
+  if (ok && half == 0)
+    tc::tmem_ld32(tmem + (static_cast<uint32_t>(quarter * 32) << 16) + tile * kSurHidden, o);
   tc::fence_before_sync();
   __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(tmem, 256);
+  if (warp == 0) tc::tmem_dealloc(tmem, 512);
   if (!ok) {
     if (tid == 0) atomicExch(err, 1);
     return;
   }
-  if (tid >= 128) return;
-  const int64_t c = static_cast<int64_t>(blockIdx.x) * 128 + tid;
-  if (c >= cells) return;
-  const int i = static_cast<int>(c % B.mx), j = static_cast<int>((c / B.mx) % B.my),
-            k = static_cast<int>(c / (static_cast<int64_t>(B.mx) * B.my));
-  const int64_t n = B.G.at(i, j, k);
-  double Y[NS], dy[NS];
-  for (int s = 0; s < NS; ++s) Y[s] = B.sv[s * sz + n];
-  float out[NS];
-  for (int s = 0; s < NS; ++s) out[s] = o[s] + __ldg(P.bias[4] + s);
-  const double T = B.bv[5 * sz + n], rho = B.bv[n];
-  const int64_t nz = B.Z.at(i, j, k);
-  const double dt = B.dt_local[nz];
-  const bool acc = dt > 0 && decode<NS>(P, out, T, log10(B.bv[4 * sz + n]), log10(dt), Y, dy);
+  if (half != 0) return;
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * kCells + tile * 128 + quarter * 32 + (tid & 31);
+  const bool valid = c < cells;
+  bool acc = false;
+  int64_t n = 0, nz = 0;
+  double rho = 0, dt = 0, dy[NS];
+  if (valid) {
+    const int i = static_cast<int>(c % B.mx), j = static_cast<int>((c / B.mx) % B.my),
+              k = static_cast<int>(c / (static_cast<int64_t>(B.mx) * B.my));
+    n = B.G.at(i, j, k);
+    nz = B.Z.at(i, j, k);
+    double Y[NS];
+    for (int s = 0; s < NS; ++s) Y[s] = B.sv[s * sz + n];
+    float out[NS];
+    for (int s = 0; s < NS; ++s) out[s] = o[s] + __ldg(P.bias[4] + s);
+    rho = B.bv[n];
+    dt = B.dt_local[nz];
+    acc = dt > 0 && decode<NS>(P, out, B.bv[5 * sz + n], log10(B.bv[4 * sz + n]), log10(dt), Y, dy);
+  }
+  // one counter update per warp
+  const unsigned a_mask = __ballot_sync(0xffffffffu, valid && acc), r_mask = __ballot_sync(0xffffffffu, valid && !acc);
+  if ((tid & 31) == 0) {
+    if (a_mask) atomicAdd(&stats[0], static_cast<unsigned long long>(__popc(a_mask)));
+    if (r_mask) atomicAdd(&stats[1], static_cast<unsigned long long>(__popc(r_mask)));
+  }
+  if (!valid) return;
   if (mode == 1) {
     B.chem_quiet[nz] = acc ? 1 : 0;
     if (acc)
       for (int s = 0; s < NS; ++s) B.chem_rate[s * B.Z.size + nz] = rho * dy[s] / dt;
-    atomicAdd(&stats[acc ? 0 : 1], 1ull);
     return;
   }
   if (acc) {
     for (int s = 0; s < NS; ++s) B.cv[(5 + s) * sz + n] += rho * dy[s];
     primitives_from_q<C>(B, n);
-    atomicAdd(&stats[0], 1ull);
   } else {
     fb_list[atomicAdd(fb_count, 1)] = static_cast<int>(c);
-    atomicAdd(&stats[1], 1ull);
   }
 }
 

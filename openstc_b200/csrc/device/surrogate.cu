@@ -310,7 +310,7 @@ __global__ void k_adam(float *p, const float *g, float *m, float *v, int64_t n, 
 }
 
 // bf16 copies of a weight [dout x din]: row-major, transposed, and in the
-// tile order of the fused inference kernel (K chunks of min(32, din)).
+// tile order of the fused inference kernel (K chunks of 16 columns).
 __global__ void k_pack(const float *w, int dout, int din, uint16_t *wb, uint16_t *wbt, uint8_t *wp) {
   const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
   if (i >= static_cast<int64_t>(dout) * din) return;
@@ -318,7 +318,7 @@ __global__ void k_pack(const float *w, int dout, int din, uint16_t *wb, uint16_t
   const uint16_t v = bf16(w[i]);
   wb[i] = v;
   wbt[static_cast<int64_t>(k) * dout + r] = v;
-  const int bk = din < 32 ? din : 32;
+  const int bk = 16;
   const int c = k / bk, kk = k % bk;
   *reinterpret_cast<uint16_t *>(wp + static_cast<size_t>(c) * dout * bk * 2 + tc::tile_offset(r, kk, bk)) = v;
 }

@@ -2,8 +2,9 @@
 // memory:  D[M x N] = A[M x K] * B[N x K]^T  (A, B row-major with K
 // contiguous, D row-major FP32).  One CTA of 128 threads computes a 128 x BN
 // tile over a K range (split-K along grid.z writes one partial D per split).
-// K is consumed in 64-wide chunks through two shared-memory stages: while the
-// tensor cores work on one stage the threads fill the other.
+// K is consumed in 64-wide chunks (one 128-byte swizzled row per tile row)
+// through two shared-memory stages: while the tensor cores work on one stage
+// the threads fill the other.
 #pragma once
 
 #include "tc_mma.cuh"
@@ -17,7 +18,7 @@ struct GemmTile {
   static constexpr uint32_t a_bytes = 128 * kGemmBK * 2;
   static constexpr uint32_t b_bytes = BN * kGemmBK * 2;
   static constexpr uint32_t stage = a_bytes + b_bytes;
-  static constexpr uint32_t smem = 2 * stage + 64;
+  static constexpr uint32_t smem = 2 * stage + 64 + 1024;  // + alignment slack
   static constexpr uint32_t tcols = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
 };
 
@@ -32,7 +33,7 @@ __device__ __forceinline__ void load_tile(uint8_t *dst, const uint16_t *src, int
     uint4 v = make_uint4(0, 0, 0, 0);
     if (r0 + r < rows_valid && kk < k_end)
       v = __ldg(reinterpret_cast<const uint4 *>(src + static_cast<size_t>(r0 + r) * ld + kk));
-    *reinterpret_cast<uint4 *>(dst + tc::tile_offset(r, c * 8, kGemmBK)) = v;
+    *reinterpret_cast<uint4 *>(dst + tc::sw128_offset(r, c * 8)) = v;
   }
 }
 
@@ -41,7 +42,9 @@ __global__ void __launch_bounds__(128) k_tc_gemm(const uint16_t *__restrict__ A,
                                                  const uint16_t *__restrict__ B, int ldb, float *__restrict__ D,
                                                  int ldd, int M, int N, int K, int k_per_split, int *err) {
   using T = GemmTile<BN>;
-  extern __shared__ __align__(128) uint8_t smem[];
+  extern __shared__ __align__(128) uint8_t smem_raw[];
+  // swizzled tiles need 1024-byte aligned bases
+  uint8_t *smem = smem_raw + ((1024 - (tc::smem_u32(smem_raw) & 1023)) & 1023);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * 128, n0 = blockIdx.y * BN;
   const int ks = blockIdx.z * k_per_split, ke = min(K, ks + k_per_split);
@@ -81,8 +84,8 @@ __global__ void __launch_bounds__(128) k_tc_gemm(const uint16_t *__restrict__ A,
       const uint32_t abase = tc::smem_u32(stage[s]), bbase = abase + T::a_bytes;
       const int ksteps = (min(kGemmBK, ke - k0) + 15) / 16;
       for (int q = 0; q < ksteps; ++q) {
-        const uint64_t ad = tc::desc_kmajor(abase + q * 256, 128, (kGemmBK / 8) * 128);
-        const uint64_t bd = tc::desc_kmajor(bbase + q * 256, 128, (kGemmBK / 8) * 128);
+        const uint64_t ad = tc::desc_sw128(abase + q * 32);
+        const uint64_t bd = tc::desc_sw128(bbase + q * 32);
         tc::mma_bf16(tmem, ad, bd, tc::idesc_bf16(128, BN), (c > 0 || q > 0) ? 1u : 0u);
       }
       tc::commit(&bar[s]);

@@ -34,6 +34,21 @@ __device__ __forceinline__ uint64_t desc_kmajor(uint32_t saddr, uint32_t lbo, ui
          (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
+// Byte offset of element (r, k) in a K-major tile of 64-column (128-byte)
+// rows with the 128-byte swizzle: 8-row atoms of 1024 bytes, the 16-byte
+// chunk c of row r stored at chunk c ^ (r % 8).  The tile base must be
+// 1024-byte aligned.
+__host__ __device__ constexpr uint32_t sw128_offset(int r, int k) {
+  return static_cast<uint32_t>((r >> 3) * 1024 + (r & 7) * 128 + ((((k >> 3) & 7) ^ (r & 7)) << 4) + (k & 7) * 2);
+}
+
+// Descriptor of a K-major SWIZZLE_128B tile (stride 1024 bytes between
+// 8-row atoms); saddr may be advanced by 32 bytes per K=16 step.
+__device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
+  return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (1ull << 16) | (static_cast<uint64_t>(1024 >> 4) << 32) |
+         (1ull << 46) | (2ull << 61);
+}
+
 // Instruction descriptor of kind::f16: D FP32, A and B BF16, both K-major.
 __host__ __device__ constexpr uint32_t idesc_bf16(int m, int n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(n >> 3) << 17) |
