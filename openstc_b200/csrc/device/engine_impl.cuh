@@ -438,8 +438,10 @@ class EngineT final : public Engine {
       for (int b = 0; b < static_cast<int>(blocks_.size()); ++b) {
         const DevBlock &B = blocks_[b];
         const int64_t cells = static_cast<int64_t>(B.mx) * B.my * B.mz;
-        sur::k_sur_infer<C><<<static_cast<unsigned>((cells + sur::kCells - 1) / sur::kCells), sur::kThreads, sur::kSmem, stream_>>>(
-            d_blocks_, b, sur_, 1, d_fb_count_, d_fb_list_, d_sur_stats_, d_sur_err_);
+        auto *fn = sur_.n_elem <= 3 ? sur::k_sur_infer<C, 1, 3> : sur::k_sur_infer<C, 1, 4>;
+        const int64_t tiles = (cells + sur::kCells - 1) / sur::kCells;
+        fn<<<static_cast<unsigned>(std::min<int64_t>(tiles, num_sms_)), sur::kThreads, sur::kSmem, stream_>>>(
+            d_blocks_, b, sur_, d_fb_count_, d_fb_list_, d_sur_stats_, d_sur_err_);
         mark("surrogate");
       }
     }
@@ -484,6 +486,8 @@ class EngineT final : public Engine {
       if (p) throw std::runtime_error("the chemistry surrogate needs a finite-rate chemistry case");
     } else {
       if (p && setup_.params.ns != kSurOut) throw std::runtime_error("the surrogate is built for 9 species");
+      if (p && p->n_elem > sur::kFusedElem)
+        throw std::runtime_error("the fused surrogate kernel handles mechanisms of at most 4 elements");
       sur_on_ = p != nullptr;
       if (p) sur_ = *p;
       if (sur_on_ && !d_fb_count_) {
@@ -494,9 +498,12 @@ class EngineT final : public Engine {
         cuda_check(cudaMalloc(&d_sur_stats_, 2 * sizeof(unsigned long long)), "cudaMalloc surrogate stats");
         cuda_check(cudaMalloc(&d_sur_err_, sizeof(int)), "cudaMalloc surrogate err");
         cuda_check(cudaMemset(d_sur_err_, 0, sizeof(int)), "memset surrogate err");
-        cuda_check(cudaFuncSetAttribute(sur::k_sur_infer<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(sur::kSmem)),
-                   "surrogate smem");
+        for (auto *fn : {sur::k_sur_infer<C, 0, 3>, sur::k_sur_infer<C, 1, 3>, sur::k_sur_infer<C, 0, 4>,
+                         sur::k_sur_infer<C, 1, 4>})
+          cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sur::kSmem)),
+                     "surrogate smem");
+        // the persistent inference kernel runs one CTA per SM
+        cuda_check(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, setup_.device), "SM count");
         const int fb_smem = static_cast<int>(2 * std::max(1, setup_.params.nr) * 128 * sizeof(double));
         if (fb_smem > 48 * 1024)
           cuda_check(cudaFuncSetAttribute(sur::k_sur_fallback<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, fb_smem),
@@ -549,8 +556,10 @@ class EngineT final : public Engine {
         const DevBlock &B = blocks_[b];
         const int64_t cells = static_cast<int64_t>(B.mx) * B.my * B.mz;
         cuda_check(cudaMemsetAsync(d_fb_count_, 0, sizeof(int), stream_), "memset fallback");
-        sur::k_sur_infer<C><<<static_cast<unsigned>((cells + sur::kCells - 1) / sur::kCells), sur::kThreads, sur::kSmem, stream_>>>(
-            d_blocks_, b, sur_, 0, d_fb_count_, d_fb_list_, d_sur_stats_, d_sur_err_);
+        auto *fn = sur_.n_elem <= 3 ? sur::k_sur_infer<C, 0, 3> : sur::k_sur_infer<C, 0, 4>;
+        const int64_t tiles = (cells + sur::kCells - 1) / sur::kCells;
+        fn<<<static_cast<unsigned>(std::min<int64_t>(tiles, num_sms_)), sur::kThreads, sur::kSmem, stream_>>>(
+            d_blocks_, b, sur_, d_fb_count_, d_fb_list_, d_sur_stats_, d_sur_err_);
         mark("surrogate");
         sur::k_sur_fallback<C><<<148 * 4, 128, fb_smem, stream_>>>(d_blocks_, b, d_fb_count_, d_fb_list_);
         mark("epi_fallback");
@@ -654,6 +663,7 @@ class EngineT final : public Engine {
   cudaGraphExec_t graphs_[4] = {nullptr, nullptr, nullptr, nullptr};
   bool sur_on_ = false;
   SurrogateDev sur_{};
+  int num_sms_ = 148;
   int *d_fb_count_ = nullptr, *d_fb_list_ = nullptr, *d_sur_err_ = nullptr;
   unsigned long long *d_sur_stats_ = nullptr;
   std::vector<void *> sur_arrays_;

@@ -47,14 +47,6 @@ __device__ inline void epi_increment(double T, double rho, const double *Y, doub
   for (int k = 0; k < NS; ++k) dy[k] = dt * x[k] / rho;
 }
 
-// GELU in its tanh form; the hardware tanh in inference, tanhf in training.
-__device__ __forceinline__ float gelu_tanh_fast(float x) {
-  const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
-  float t;
-  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
-  return 0.5f * x * (1.f + t);
-}
-
 // Network output o (normalised, bias added) -> dY_k = (Y_k + eps) c_k
 // sinh(s_k o_k); the increment is then projected onto element conservation
 // (weighted least squares, weights |dY_k| + 1e-3 Y_k).  The cell is accepted
@@ -63,279 +55,250 @@ __device__ __forceinline__ float gelu_tanh_fast(float x) {
 // element totals, no increment exceeds gate.rel_max (Y_k + eps), and no mass
 // fraction is driven below -1e-9: the network is trusted where the chemistry
 // changes the composition little, the EPI step takes the reacting cells.
-template <int NS>
-__device__ inline bool decode(const SurrogateDev &p, const float *o, double T, double lp, double ldt, const double *Y,
-                              double *dy) {
+// NE is a compile-time bound on the element count (elements past p.n_elem
+// have zero rows and drop out), so every array lives in registers.  The
+// network's own error is ~1e-2, so the transcendental functions of the decode
+// run in FP32; the projection and the increments stay in FP64.
+template <int NS, int NE>
+__device__ __forceinline__ bool decode_ne(const SurrogateDev &p, const float *o, float T, float lp, float ldt,
+                                          const double *Y, double *dy) {
   const SurrogateGate &g = p.gate;
   bool ok = T >= g.t_min && T <= g.t_max && lp >= g.lp_min && lp <= g.lp_max && ldt >= g.ldt_min && ldt <= g.ldt_max;
+  float w[NS];  // any positive weights conserve the elements exactly; FP32 is enough for them
+#pragma unroll
   for (int k = 0; k < NS; ++k) {
-    const double ok_k = fabs(o[k]) <= g.out_max;
-    ok = ok && ok_k;
-    const double oc = fmin(fmax(static_cast<double>(o[k]), -static_cast<double>(g.out_max)), static_cast<double>(g.out_max));
-    dy[k] = (Y[k] + kSurYEps) * p.out_c[k] * sinh(oc * p.out_s[k]);
+    ok = ok && fabsf(o[k]) <= g.out_max;
+    const float oc = fminf(fmaxf(o[k], -g.out_max), g.out_max);
+    dy[k] = (Y[k] + kSurYEps) * static_cast<double>(p.out_c[k] * sinhf(oc * p.out_s[k]));
     if (fabs(dy[k]) > g.rel_max * (Y[k] + kSurYEps)) ok = false;
+    w[k] = static_cast<float>(fabs(dy[k]) + 1e-3 * Y[k]) + 1e-30f;
   }
-  const int ne = p.n_elem;
-  double r[kMaxElem], M[kMaxElem * kMaxElem], w[NS];
-  for (int k = 0; k < NS; ++k) w[k] = fabs(dy[k]) + 1e-3 * Y[k] + 1e-30;
-  for (int e = 0; e < ne; ++e) {
+  // normal equations (E W E^T) lambda = E dy, E[e][k] = a_ek / W_k
+  double r[NE], M[NE][NE];
+#pragma unroll
+  for (int e = 0; e < NE; ++e) {
     double defect = 0, total = 0;
+#pragma unroll
     for (int k = 0; k < NS; ++k) {
       defect += p.elem[e * kMaxSpec + k] * dy[k];
       total += p.elem[e * kMaxSpec + k] * Y[k];
     }
     r[e] = defect;
     if (total > 0 && fabs(defect) > g.defect_tol * total) ok = false;
-    for (int f = 0; f < ne; ++f) {
+#pragma unroll
+    for (int f = 0; f <= e; ++f) {
       double s = 0;
-      for (int k = 0; k < NS; ++k) s += p.elem[e * kMaxSpec + k] * w[k] * p.elem[f * kMaxSpec + k];
-      M[e * kMaxElem + f] = s;
+#pragma unroll
+      for (int k = 0; k < NS; ++k) s += static_cast<double>(p.elem[e * kMaxSpec + k] * w[k]) * p.elem[f * kMaxSpec + k];
+      M[e][f] = s;
+      M[f][e] = s;
     }
   }
-  // lambda = M^-1 r (Gauss-Jordan, partial pivoting; ne <= 8)
-  for (int c = 0; c < ne; ++c) {
-    int piv = c;
-    for (int q = c + 1; q < ne; ++q)
-      if (fabs(M[q * kMaxElem + c]) > fabs(M[piv * kMaxElem + c])) piv = q;
-    if (fabs(M[piv * kMaxElem + c]) < 1e-300) continue;
-    if (piv != c) {
-      for (int q = 0; q < ne; ++q) {
-        const double t = M[c * kMaxElem + q];
-        M[c * kMaxElem + q] = M[piv * kMaxElem + q];
-        M[piv * kMaxElem + q] = t;
-      }
-      const double t = r[c];
-      r[c] = r[piv];
-      r[piv] = t;
-    }
-    const double inv = 1.0 / M[c * kMaxElem + c];
-    for (int q = 0; q < ne; ++q) {
+  // M is symmetric positive (semi-)definite: Gauss-Jordan without pivoting; an
+  // element absent from the cell (zero row) gets lambda = 0
+#pragma unroll
+  for (int c = 0; c < NE; ++c) {
+    const bool live = M[c][c] > 1e-300;
+    const double inv = live ? 1.0 / M[c][c] : 0.0;
+#pragma unroll
+    for (int q = 0; q < NE; ++q) {
       if (q == c) continue;
-      const double f = M[q * kMaxElem + c] * inv;
-      for (int z = 0; z < ne; ++z) M[q * kMaxElem + z] -= f * M[c * kMaxElem + z];
+      const double f = M[q][c] * inv;
+#pragma unroll
+      for (int z = 0; z < NE; ++z) M[q][z] -= f * M[c][z];
       r[q] -= f * r[c];
     }
     r[c] *= inv;
-    for (int z = 0; z < ne; ++z) M[c * kMaxElem + z] *= inv;
   }
+#pragma unroll
   for (int k = 0; k < NS; ++k) {
     double corr = 0;
-    for (int e = 0; e < ne; ++e) corr += p.elem[e * kMaxSpec + k] * r[e];
+#pragma unroll
+    for (int e = 0; e < NE; ++e) corr += p.elem[e * kMaxSpec + k] * r[e];
     dy[k] -= w[k] * corr;
     if (Y[k] + dy[k] < -1e-9) ok = false;
   }
   return ok;
 }
 
+template <int NS>
+__device__ __forceinline__ bool decode(const SurrogateDev &p, const float *o, float T, float lp, float ldt,
+                                       const double *Y, double *dy) {
+  if (p.n_elem <= 4) return decode_ne<NS, 4>(p, o, T, lp, ldt, Y, dy);
+  return decode_ne<NS, kMaxElem>(p, o, T, lp, ldt, Y, dy);
+}
+
 // ------------------------------------------------------------ fused kernel
-// One CTA per SM handles two 128-cell tiles per pass over the weights (two
-// accumulators fill the 512 TMEM columns), so every weight byte staged from
-// L2 feeds two MMAs.  The weights stream through a ring of bulk copies in
-// 8 KB chunks far enough ahead to cover the L2 latency.
-constexpr int kTiles = 2;
-constexpr int kCells = 128 * kTiles;
-constexpr int kThreads = 512;  // 16 warps: 4 per TMEM lane quarter (tile x column half)
-constexpr int kStages = 10;    // weight chunks in flight
-constexpr int kLag = 2;        // chunk groups that may still be executing when their stage is refilled
+// A persistent kernel, one CTA per SM, that runs the tiles of 128 cells of a
+// block through the network as a software pipeline on mbarriers:
+//   * warp 9 (one lane) streams the hidden layers' weights through a ring of
+//     kStages shared-memory stages, one 32 KB stage (K = 64) per 64-column
+//     activation group, in the order the MMAs consume them; the first and
+//     output layers' weights (8 KB each) stay resident;
+//   * warp 8 issues the tcgen05 MMAs of global layer g (tile g / 5, layer
+//     g % 5) into accumulator g % 2 (2 x 256 TMEM columns);
+//   * warps 0-7 (TMEM lane quarter w % 4, column half w / 4) run the hidden
+//     epilogues: accumulator + bias -> GELU -> bf16 activations, each 64-
+//     column group released to the MMA of the next layer as soon as it is
+//     written, so that MMA overlaps this epilogue;
+//   * warps 10-13 (lane quarters 2, 3, 0, 1) compute the features of the
+//     next tile and decode / gate / apply the outputs of the current one.
+// One activation buffer serves every layer (the epilogue of layer L only
+// starts once the MMAs of layer L, its last readers, have completed), and
+// features alternate between two 4 KB buffers by tile, so no stage waits for
+// the one before it except through the data it needs.  Every wait is bounded: a wait that runs
+// out raises the CTA's abort flag, every role then leaves its loop, the MMAs
+// and copies in flight are drained, and the kernel reports the error.
+constexpr int kCells = 128;
+constexpr int kEpiWarps = 8;
+constexpr int kMmaWarp = 8, kLoadWarp = 9, kIoWarp0 = 10;
+constexpr int kThreads = 32 * 14;
+constexpr int kStageChunks = 4;  // weight chunks per ring stage
+constexpr int kStages = 4;       // ring stages
+constexpr int kFusedElem = 4;  // largest element count of the fused kernel's conservation gate
 // Every weight chunk is 8 KB: one K=16 slice [256 x 16] of a hidden layer,
 // the whole first layer [256 x 16] or the whole output layer [16 x 256],
 // all packed K-major canonical with 16-column tiles.
 constexpr uint32_t kChunkBytes = kSurHidden * 16 * 2;
-constexpr int kChunks = 1 + 3 * (kSurHidden / 16) + 1;
-constexpr uint32_t kA0Bytes = 128 * kSurInPad * 2;
-constexpr uint32_t kA1Bytes = 128 * kSurHidden * 2;
-constexpr uint32_t kSmem = kTiles * (kA0Bytes + kA1Bytes) + kStages * kChunkBytes + (2 * kStages + 2) * 8 + 16;
+constexpr int kTileStages = 3 * 4;  // streamed stages per tile: 3 hidden layers x 4 groups
+constexpr uint32_t kActBytes = 128 * kSurHidden * 2;
+constexpr uint32_t kStageBytes = kStageChunks * kChunkBytes;
+constexpr uint32_t kX0Bytes = 128 * kSurInPad * 2;
+// barriers: full[S], empty[S], feat_full[2], x0_free[2], mma_epi[2], mma_out, acc_free[2], act_ready[4], res,
+// drain.  Each barrier has waiters that are never more than one phase behind
+// its arrivals, which is what parity waits need: the hidden layers' MMAs
+// signal the epilogue through mma_epi (by epilogue index), the output layer's
+// the decode through mma_out (by tile).
+constexpr int kBars = 2 * kStages + 2 + 2 + 2 + 1 + 2 + 4 + 1 + 1;
+constexpr uint32_t kBiasBytes = (4 * kSurHidden + kSurOutPad) * 4;  // every layer's bias, staged once per CTA
+constexpr uint32_t kSmem = kActBytes + 2 * kX0Bytes + 2 * kChunkBytes + kStages * kStageBytes + kBiasBytes + kBars * 8 + 16;
+static_assert(kSmem <= 232448, "shared memory of one CTA");
 
-// Source of weight chunk i in the stream
-__device__ __forceinline__ const uint8_t *chunk_src(const SurrogateDev &P, int i) {
-  if (i == 0) return P.w_packed[0];
-  if (i == kChunks - 1) return P.w_packed[4];
-  const int l = 1 + (i - 1) / (kSurHidden / 16), c = (i - 1) % (kSurHidden / 16);
-  return P.w_packed[l] + static_cast<size_t>(c) * kChunkBytes;
+// A hidden layer's K is consumed in the order the epilogue releases its
+// 64-column activation groups (group j = 2 * half + step / 2 holds K chunks
+// 4j..4j+3, and the two column halves run side by side): groups 0, 2, 1, 3.
+__host__ __device__ constexpr int group_order(int gq) { return gq == 1 ? 2 : (gq == 2 ? 1 : gq); }
+
+// Source of streamed stage s (0..kTileStages-1) of a tile: 4 contiguous K
+// chunks of a hidden layer's packed weights
+__device__ __forceinline__ const uint8_t *stage_src(const SurrogateDev &P, int s) {
+  return P.w_packed[1 + s / 4] + static_cast<size_t>(group_order(s % 4)) * kStageBytes;
 }
 
-// Asynchronous bulk copy of one chunk into shared memory; completion is
-// counted in bytes on the stage's mbarrier.
-__device__ __forceinline__ void load_chunk(uint8_t *dst, const uint8_t *src, uint64_t *full) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(kChunkBytes), "r"(tc::smem_u32(full))
+// Asynchronous bulk copies into shared memory: the stage's mbarrier is told
+// the byte count once, and each chunk's copy completes its share.
+__device__ __forceinline__ void expect_bytes(uint64_t *full, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes), "r"(tc::smem_u32(full))
                : "memory");
+}
+__device__ __forceinline__ void load_bytes(uint8_t *dst, const uint8_t *src, uint32_t bytes, uint64_t *full) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                    tc::smem_u32(dst)),
-               "l"(src), "r"(kChunkBytes), "r"(tc::smem_u32(full))
+               "l"(src), "r"(bytes), "r"(tc::smem_u32(full))
                : "memory");
 }
 
-// Epilogue of a hidden layer: accumulator + bias -> GELU -> bf16 rows of the
-// next layer's input tile (K-major canonical, 256 columns).  Warp w reads
-// TMEM lane quarter w % 4 of tile (w / 4) / 2, column half (w / 4) % 2.
-__device__ __forceinline__ void hidden_epilogue(uint32_t tmem, const float *bias, uint8_t *a1) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int quarter = warp & 3, tile = (warp >> 2) >> 1, half = (warp >> 2) & 1;
-  const int row = quarter * 32 + lane;
-  uint8_t *a = a1 + tile * kA1Bytes;
-  const uint32_t tbase = tmem + (static_cast<uint32_t>(quarter * 32) << 16) + tile * kSurHidden;
-  for (int c0 = half * 128; c0 < half * 128 + 128; c0 += 32) {
-    float v[32];
-    tc::tmem_ld32(tbase + c0, v);
+__device__ __forceinline__ void bar_arrive(uint64_t *bar, uint32_t count = 1) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(bar)), "r"(count) : "memory");
+}
+
+// Bounded wait that gives up early once another role has aborted.
+__device__ __forceinline__ bool wait_bar(uint64_t *bar, uint32_t parity, volatile int *abort) {
+  for (uint32_t it = 0; it < (1u << 24); ++it) {
+    if (tc::mbar_try(bar, parity)) return true;
+    if ((it & 63) == 63 && *abort) return false;
+  }
+  *abort = 1;
+  return false;
+}
+
+__device__ __forceinline__ uint64_t f2_pack(float lo, float hi) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(uint64_t v, float &lo, float &hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+
+// GELU (tanh form) of two pre-activations, returned as packed bf16x2 (lo =
+// x0).  The polynomial runs on packed FP32 pairs; tanh runs on the half-
+// precision pair unit (its argument saturates to the largest finite half,
+// where tanh is 1): the result is rounded to bf16, whose step is 8x the
+// error of the half-precision tanh.
+__device__ __forceinline__ uint32_t gelu2_bf16(float x0, float x1) {
+  const uint64_t x = f2_pack(x0, x1);
+  const uint64_t c0 = f2_pack(0.7978845608028654f, 0.7978845608028654f);
+  const uint64_t c1 = f2_pack(0.7978845608028654f * 0.044715f, 0.7978845608028654f * 0.044715f);
+  const uint64_t half2 = f2_pack(0.5f, 0.5f);
+  uint64_t x2, p, u, hx;
+  asm("mul.rn.f32x2 %0, %1, %1;" : "=l"(x2) : "l"(x));
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(p) : "l"(c1), "l"(x2), "l"(c0));
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(u) : "l"(x), "l"(p));
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(hx) : "l"(x), "l"(half2));
+  float u0, u1;
+  f2_unpack(u, u0, u1);
+  uint32_t h, t;
+  asm("cvt.rn.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(h) : "f"(u1), "f"(u0));
+  asm("tanh.approx.f16x2 %0, %1;" : "=r"(t) : "r"(h));
+  float t0, t1;
+  asm("{\n .reg .f16 a, b;\n mov.b32 {a, b}, %2;\n cvt.f32.f16 %0, a;\n cvt.f32.f16 %1, b;\n}"
+      : "=f"(t0), "=f"(t1)
+      : "r"(t));
+  uint64_t y;
+  asm("fma.rn.f32x2 %0, %1, %2, %1;" : "=l"(y) : "l"(hx), "l"(f2_pack(t0, t1)));
+  float y0, y1;
+  f2_unpack(y, y0, y1);
+  uint32_t r;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(y1), "f"(y0));
+  return r;
+}
+
+// Features of the cell in row `row` of the tile starting at cell0 -> bf16
+// row of the first layer's input (zeros past the last cell).
+template <class C>
+__device__ __forceinline__ void tile_features(const DevBlock &B, const SurrogateDev &P, int64_t cell0, int row,
+                                              uint8_t *x0) {
+  constexpr int NS = C::ns;
+  const int64_t cells = static_cast<int64_t>(B.mx) * B.my * B.mz, sz = B.G.size;
+  const int64_t c = cell0 + row;
+  float f[kSurInPad];
 #pragma unroll
-    for (int q = 0; q < 32; q += 8) {
-      uint32_t pk[4];
+  for (int q = 0; q < kSurInPad; ++q) f[q] = 0.f;
+  if (c < cells) {
+    const int i = static_cast<int>(c % B.mx), j = static_cast<int>((c / B.mx) % B.my),
+              k = static_cast<int>(c / (static_cast<int64_t>(B.mx) * B.my));
+    const int64_t n = B.G.at(i, j, k);
+    float raw[kSurIn];
+    raw[0] = static_cast<float>(B.bv[5 * sz + n]);
+    raw[1] = log10f(static_cast<float>(B.bv[4 * sz + n]));
 #pragma unroll
-      for (int h = 0; h < 4; ++h) {
-        const float x0 = gelu_tanh_fast(v[q + 2 * h] + __ldg(bias + c0 + q + 2 * h));
-        const float x1 = gelu_tanh_fast(v[q + 2 * h + 1] + __ldg(bias + c0 + q + 2 * h + 1));
-        const __nv_bfloat162 b2 = __floats2bfloat162_rn(x0, x1);
-        pk[h] = *reinterpret_cast<const uint32_t *>(&b2);
-      }
-      *reinterpret_cast<uint4 *>(a + tc::tile_offset(row, c0 + q, kSurHidden)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    for (int s = 0; s < NS; ++s) raw[2 + s] = static_cast<float>(B.sv[s * sz + n]);
+    raw[11] = log10f(static_cast<float>(B.dt_local[B.Z.at(i, j, k)]));
+#pragma unroll
+    for (int q = 0; q < kSurIn; ++q) f[q] = (raw[q] - P.in_mu[q]) / P.in_sig[q];
+  }
+#pragma unroll
+  for (int q = 0; q < kSurInPad; q += 8) {
+    uint32_t pk[4];
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const __nv_bfloat162 b2 = __floats2bfloat162_rn(f[q + 2 * h], f[q + 2 * h + 1]);
+      pk[h] = *reinterpret_cast<const uint32_t *>(&b2);
     }
+    *reinterpret_cast<uint4 *>(x0 + tc::tile_offset(row, q, kSurInPad)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
   }
 }
 
-// Two 128-cell tiles per CTA: features -> 4 x (256, GELU) -> 9 outputs on the
-// tensor cores, then decode, project and gate, with dt = the cell's local
-// time step.  mode 1 (in the step, before the source term): accepted cells
-// are marked chemically quiet and get the rate rho dY / dt, the others keep
-// the point-implicit chemistry.  mode 0 (a split step): accepted increments
-// go into cv (rho Y_k) with the primitives recomputed, rejected cells are
-// listed for the EPI fallback.  stats[0] += accepted, stats[1] += rejected.
-template <class C>
-__global__ void __launch_bounds__(kThreads) k_sur_infer(const DevBlock *__restrict__ blks, int b, SurrogateDev P,
-                                                        int mode, int *fb_count, int *fb_list,
-                                                        unsigned long long *stats, int *err) {
+// Decode, gate and apply the network output o of cell c (warp-collective for
+// the statistics).  MODE 1: mark quiet cells and their rate; MODE 0: apply the
+// increment or list the cell for the EPI fallback.
+template <class C, int MODE, int NE>
+__device__ __forceinline__ void tile_apply(const DevBlock &B, const SurrogateDev &P, int64_t c, const float *o,
+                                           const float *bias_out, int *fb_count, int *fb_list,
+                                           unsigned long long *stats) {
   constexpr int NS = C::ns;
-  extern __shared__ __align__(128) uint8_t smem[];
-  uint8_t *a0 = smem, *a1 = smem + kTiles * kA0Bytes, *stages = a1 + kTiles * kA1Bytes;
-  uint64_t *full = reinterpret_cast<uint64_t *>(stages + kStages * kChunkBytes);
-  uint64_t *empty = full + kStages, *acc_bar = empty + kStages;
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(acc_bar + 1);
-  const DevBlock &B = blks[b];
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int64_t cells = static_cast<int64_t>(B.mx) * B.my * B.mz;
-  const int64_t sz = B.G.size;
-
-  // features of the CTA's cells: thread t < 256 -> tile t / 128, row t % 128
-  if (tid < kCells) {
-    const int64_t c = static_cast<int64_t>(blockIdx.x) * kCells + tid;
-    float f[kSurInPad];
-#pragma unroll
-    for (int q = 0; q < kSurInPad; ++q) f[q] = 0.f;
-    if (c < cells) {
-      const int i = static_cast<int>(c % B.mx), j = static_cast<int>((c / B.mx) % B.my),
-                k = static_cast<int>(c / (static_cast<int64_t>(B.mx) * B.my));
-      const int64_t n = B.G.at(i, j, k);
-      float raw[kSurIn];
-      raw[0] = static_cast<float>(B.bv[5 * sz + n]);
-      raw[1] = static_cast<float>(log10(B.bv[4 * sz + n]));
-      for (int s = 0; s < NS; ++s) raw[2 + s] = static_cast<float>(B.sv[s * sz + n]);
-      raw[11] = static_cast<float>(log10(B.dt_local[B.Z.at(i, j, k)]));
-#pragma unroll
-      for (int q = 0; q < kSurIn; ++q) f[q] = (raw[q] - P.in_mu[q]) / P.in_sig[q];
-    }
-    uint8_t *a = a0 + (tid >> 7) * kA0Bytes;
-#pragma unroll
-    for (int q = 0; q < kSurInPad; q += 8) {
-      uint32_t pk[4];
-#pragma unroll
-      for (int h = 0; h < 4; ++h) {
-        const __nv_bfloat162 b2 = __floats2bfloat162_rn(f[q + 2 * h], f[q + 2 * h + 1]);
-        pk[h] = *reinterpret_cast<const uint32_t *>(&b2);
-      }
-      *reinterpret_cast<uint4 *>(a + tc::tile_offset(tid & 127, q, kSurInPad)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-    }
-  }
-  if (warp == 0) tc::tmem_alloc(tslot, 512);
-  if (tid == 0) {
-    for (int q = 0; q < kStages; ++q) {
-      tc::mbar_init(&full[q], 1);
-      tc::mbar_init(&empty[q], 1);
-    }
-    tc::mbar_init(acc_bar, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    for (int q = 0; q < kStages; ++q) load_chunk(stages + q * kChunkBytes, chunk_src(P, q), &full[q]);
-  }
-  tc::fence_async_smem();
-  tc::fence_before_sync();
-  __syncthreads();
-  tc::fence_after_sync();
-  const uint32_t tmem = *tslot;
-  bool ok = true;
-  int chunk = 0;         // next chunk of the stream
-  int issued = kStages;  // chunks whose copy has been started
-  constexpr uint32_t kSboA1 = (kSurHidden / 8) * 128, kSbo16 = (16 / 8) * 128;
-  for (int layer = 0; layer < 5; ++layer) {
-    // thread 0 issues this layer's MMAs (both tiles) as the weight chunks
-    // land and refills the stage of the chunk kLag groups back
-    if (tid == 0) {
-      const int n_here = (layer == 0 || layer == 4) ? 1 : kSurHidden / 16;
-      for (int q = 0; q < n_here && ok; ++q, ++chunk) {
-        const int st = chunk % kStages;
-        if (!tc::mbar_wait(&full[st], (chunk / kStages) & 1)) {
-          ok = false;
-          break;
-        }
-        tc::fence_after_sync();
-        const uint32_t wb = tc::smem_u32(stages + st * kChunkBytes);
-        for (int t = 0; t < kTiles; ++t) {
-          const uint32_t acc = tmem + t * kSurHidden;
-          if (layer == 0) {
-            const uint64_t ad = tc::desc_kmajor(tc::smem_u32(a0 + t * kA0Bytes), 128, kSbo16);
-            tc::mma_bf16(acc, ad, tc::desc_kmajor(wb, 128, kSbo16), tc::idesc_bf16(128, kSurHidden), 0u);
-          } else if (layer < 4) {
-            const uint64_t ad = tc::desc_kmajor(tc::smem_u32(a1 + t * kA1Bytes) + q * 16 * 16, 128, kSboA1);
-            tc::mma_bf16(acc, ad, tc::desc_kmajor(wb, 128, kSbo16), tc::idesc_bf16(128, kSurHidden),
-                         q > 0 ? 1u : 0u);
-          } else {
-            for (int kk = 0; kk < kSurHidden / 16; ++kk) {
-              const uint64_t ad = tc::desc_kmajor(tc::smem_u32(a1 + t * kA1Bytes) + kk * 16 * 16, 128, kSboA1);
-              const uint64_t bd = tc::desc_kmajor(wb + kk * (kSurOutPad * 16 * 2), 128, kSbo16);
-              tc::mma_bf16(acc, ad, bd, tc::idesc_bf16(128, kSurOutPad), kk > 0 ? 1u : 0u);
-            }
-          }
-        }
-        tc::commit(&empty[st]);
-        const int old = chunk - kLag;
-        if (old >= 0 && old + kStages < kChunks) {
-          const int os = old % kStages;
-          if (!tc::mbar_wait(&empty[os], (old / kStages) & 1)) {
-            ok = false;
-            break;
-          }
-          load_chunk(stages + os * kChunkBytes, chunk_src(P, old + kStages), &full[os]);
-          ++issued;
-        }
-      }
-      if (ok) tc::commit(acc_bar);
-    }
-    ok = __syncthreads_and(ok) != 0;
-    if (!ok) break;
-    ok = __syncthreads_and(tc::mbar_wait(acc_bar, layer & 1)) != 0;
-    tc::fence_after_sync();
-    if (!ok || layer == 4) break;
-    hidden_epilogue(tmem, P.bias[layer], a1);
-    tc::fence_before_sync();
-    tc::fence_async_smem();
-    __syncthreads();
-  }
-  if (tid == 0) {
-    // copies issued beyond the last consumed chunk (only on a timeout) land
-    // before the CTA exits
-    for (int c = chunk; c < issued; ++c) tc::mbar_wait(&full[c % kStages], (c / kStages) & 1);
-  }
-  // outputs: warps with (w / 4) % 2 == 0 read their tile's 16 output columns
-  const int quarter = warp & 3, tile = (warp >> 2) >> 1, half = (warp >> 2) & 1;
-  float o[32];
-  if (ok && half == 0)
-    tc::tmem_ld32(tmem + (static_cast<uint32_t>(quarter * 32) << 16) + tile * kSurHidden, o);
-  tc::fence_before_sync();
-  __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(tmem, 512);
-  if (!ok) {
-    if (tid == 0) atomicExch(err, 1);
-    return;
-  }
-  if (half != 0) return;
-  const int64_t c = static_cast<int64_t>(blockIdx.x) * kCells + tile * 128 + quarter * 32 + (tid & 31);
+  const int64_t cells = static_cast<int64_t>(B.mx) * B.my * B.mz, sz = B.G.size;
   const bool valid = c < cells;
   bool acc = false;
   int64_t n = 0, nz = 0;
@@ -346,32 +309,263 @@ __global__ void __launch_bounds__(kThreads) k_sur_infer(const DevBlock *__restri
     n = B.G.at(i, j, k);
     nz = B.Z.at(i, j, k);
     double Y[NS];
+#pragma unroll
     for (int s = 0; s < NS; ++s) Y[s] = B.sv[s * sz + n];
     float out[NS];
-    for (int s = 0; s < NS; ++s) out[s] = o[s] + __ldg(P.bias[4] + s);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) out[s] = o[s] + bias_out[s];
     rho = B.bv[n];
     dt = B.dt_local[nz];
-    acc = dt > 0 && decode<NS>(P, out, B.bv[5 * sz + n], log10(B.bv[4 * sz + n]), log10(dt), Y, dy);
+    acc = dt > 0 && decode_ne<NS, NE>(P, out, static_cast<float>(B.bv[5 * sz + n]),
+                                      log10f(static_cast<float>(B.bv[4 * sz + n])), log10f(static_cast<float>(dt)),
+                                      Y, dy);
   }
   // one counter update per warp
   const unsigned a_mask = __ballot_sync(0xffffffffu, valid && acc), r_mask = __ballot_sync(0xffffffffu, valid && !acc);
-  if ((tid & 31) == 0) {
+  if ((threadIdx.x & 31) == 0) {
     if (a_mask) atomicAdd(&stats[0], static_cast<unsigned long long>(__popc(a_mask)));
     if (r_mask) atomicAdd(&stats[1], static_cast<unsigned long long>(__popc(r_mask)));
   }
   if (!valid) return;
-  if (mode == 1) {
+  if constexpr (MODE == 1) {
     B.chem_quiet[nz] = acc ? 1 : 0;
-    if (acc)
-      for (int s = 0; s < NS; ++s) B.chem_rate[s * B.Z.size + nz] = rho * dy[s] / dt;
-    return;
-  }
-  if (acc) {
-    for (int s = 0; s < NS; ++s) B.cv[(5 + s) * sz + n] += rho * dy[s];
-    primitives_from_q<C>(B, n);
+    if (acc) {
+      const double f = rho / dt;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) B.chem_rate[s * B.Z.size + nz] = f * dy[s];
+    }
   } else {
-    fb_list[atomicAdd(fb_count, 1)] = static_cast<int>(c);
+    if (acc) {
+#pragma unroll
+      for (int s = 0; s < NS; ++s) B.cv[(5 + s) * sz + n] += rho * dy[s];
+      primitives_from_q<C>(B, n);
+    } else {
+      fb_list[atomicAdd(fb_count, 1)] = static_cast<int>(c);
+    }
   }
+}
+
+// The tiles of block b: features -> 4 x (256, GELU) -> 9 outputs on the
+// tensor cores, then decode, project and gate, with dt = the cell's local
+// time step.  MODE 1 (in the step, before the source term): accepted cells
+// are marked chemically quiet and get the rate rho dY / dt, the others keep
+// the point-implicit chemistry.  MODE 0 (a split step): accepted increments
+// go into cv (rho Y_k) with the primitives recomputed, rejected cells are
+// listed for the EPI fallback.  stats[0] += accepted, stats[1] += rejected.
+// NE (3 or 4) bounds the element count of the conservation gate.
+template <class C, int MODE, int NE>
+__global__ void __launch_bounds__(kThreads, 1) k_sur_infer(const DevBlock *__restrict__ blks, int b, SurrogateDev P,
+                                                           int *fb_count, int *fb_list, unsigned long long *stats,
+                                                           int *err) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  uint8_t *act = smem;                     // 64 KB
+  uint8_t *x0 = smem + kActBytes;          // 2 x 4 KB, by tile
+  uint8_t *wres = x0 + 2 * kX0Bytes;       // first and output layers' weights, 2 x 8 KB
+  uint8_t *stages = wres + 2 * kChunkBytes;  // kStages x 32 KB
+  float *sbias = reinterpret_cast<float *>(stages + kStages * kStageBytes);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(reinterpret_cast<uint8_t *>(sbias) + kBiasBytes);
+  uint64_t *full = bars, *empty = full + kStages, *feat_full = empty + kStages, *x0_free = feat_full + 2,
+           *mma_epi = x0_free + 2, *mma_out = mma_epi + 2, *acc_free = mma_out + 1, *act_ready = acc_free + 2,
+           *drain = act_ready + 4, *res_full = drain + 1;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(drain + 1);
+  volatile int *abort = reinterpret_cast<volatile int *>(tslot + 1);
+  const DevBlock &B = blks[b];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int64_t cells = static_cast<int64_t>(B.mx) * B.my * B.mz;
+  const int64_t ntiles = (cells + kCells - 1) / kCells;
+  // this CTA's tiles: blockIdx.x, blockIdx.x + gridDim.x, ...
+  const int my_tiles =
+      blockIdx.x < ntiles ? static_cast<int>((ntiles - 1 - blockIdx.x) / gridDim.x + 1) : 0;
+
+  if (tid == 0) {
+    for (int q = 0; q < kStages; ++q) {
+      tc::mbar_init(&full[q], 1);
+      tc::mbar_init(&empty[q], 1);
+    }
+    for (int q = 0; q < 2; ++q) {
+      tc::mbar_init(&feat_full[q], 4);
+      tc::mbar_init(&x0_free[q], 1);
+      tc::mbar_init(&mma_epi[q], 1);
+      tc::mbar_init(&acc_free[q], kEpiWarps);
+    }
+    for (int q = 0; q < 4; ++q) tc::mbar_init(&act_ready[q], 4);
+    tc::mbar_init(mma_out, 1);
+    tc::mbar_init(drain, 1);
+    tc::mbar_init(res_full, 1);
+    *abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) tc::tmem_alloc(tslot, 512);
+  for (int q = tid; q < 4 * kSurHidden + kSurOutPad; q += kThreads)
+    sbias[q] = q < 4 * kSurHidden ? P.bias[q / kSurHidden][q % kSurHidden] : P.bias[4][q - 4 * kSurHidden];
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tslot;
+
+  const int total = my_tiles * kTileStages;  // this CTA's streamed stages
+  if (warp == kLoadWarp) {
+    // ---- weights: the resident pair once, then stage si of the stream into
+    // ring slot si % kStages once the MMAs of stage si - kStages are done
+    if (lane == 0) {
+      expect_bytes(res_full, 2 * kChunkBytes);
+      load_bytes(wres, P.w_packed[0], kChunkBytes, res_full);
+      load_bytes(wres + kChunkBytes, P.w_packed[4], kChunkBytes, res_full);
+      int si = 0;
+      for (; si < total; ++si) {
+        const int slot = si % kStages;
+        if (si >= kStages && !wait_bar(&empty[slot], ((si / kStages) - 1) & 1, abort)) break;
+        expect_bytes(&full[slot], kStageBytes);
+        load_bytes(stages + slot * kStageBytes, stage_src(P, si % kTileStages), kStageBytes, &full[slot]);
+      }
+      // the copies in flight land before the CTA moves on
+      tc::mbar_wait(res_full, 0);
+      for (int c = si > kStages ? si - kStages : 0; c < si; ++c)
+        tc::mbar_wait(&full[c % kStages], (c / kStages) & 1);
+    }
+  } else if (warp == kMmaWarp) {
+    // ---- tensor-core issue: the whole warp runs the loop, converged, and
+    // one elected lane issues each MMA and commit
+    constexpr uint32_t kSboAct = (kSurHidden / 8) * 128, kSbo16 = (16 / 8) * 128;
+    constexpr uint32_t kIdHidden = tc::idesc_bf16(128, kSurHidden), kIdOut = tc::idesc_bf16(128, kSurOutPad);
+    const uint32_t in = tc::smem_u32(act), w0 = tc::smem_u32(wres), w4 = w0 + kChunkBytes;
+    int si = 0;
+    bool ok = __all_sync(0xffffffffu, wait_bar(res_full, 0, abort));
+    for (int it = 0; it < my_tiles && ok; ++it) {
+      const int tb = it & 1;
+      for (int L = 0; L < 5 && ok; ++L) {
+        const int g = it * 5 + L, p = g & 1;
+        const uint32_t acc = tmem + p * kSurHidden;
+        if (g >= 2) ok = __all_sync(0xffffffffu, wait_bar(&acc_free[p], ((g - 2) >> 1) & 1, abort));
+        const int e_prev = it * 4 + L - 1;  // the epilogue that wrote this layer's input
+        if (L == 0) {
+          if (ok) ok = __all_sync(0xffffffffu, wait_bar(&feat_full[tb], (it >> 1) & 1, abort));
+          if (!ok) break;
+          tc::fence_after_sync();
+          tc::mma_bf16_warp(acc, tc::desc_kmajor(tc::smem_u32(x0 + tb * kX0Bytes), 128, kSbo16),
+                            tc::desc_kmajor(w0, 128, kSbo16), kIdHidden, 0u);
+          tc::commit_warp(&x0_free[tb]);
+        } else if (L < 4) {
+          for (int gq = 0; gq < 4 && ok; ++gq, ++si) {
+            const int j = group_order(gq), slot = si % kStages;
+            ok = __all_sync(0xffffffffu, wait_bar(&act_ready[j], e_prev & 1, abort));
+            if (ok) ok = __all_sync(0xffffffffu, wait_bar(&full[slot], (si / kStages) & 1, abort));
+            if (!ok) break;
+            tc::fence_after_sync();
+            const uint32_t wb = tc::smem_u32(stages + slot * kStageBytes);
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+              tc::mma_bf16_warp(acc, tc::desc_kmajor(in + (4 * j + c) * 16 * 16, 128, kSboAct),
+                                tc::desc_kmajor(wb + c * kChunkBytes, 128, kSbo16), kIdHidden,
+                                (gq > 0 || c > 0) ? 1u : 0u);
+            tc::commit_warp(&empty[slot]);
+          }
+        } else {
+          for (int j = 0; j < 4 && ok; ++j) ok = __all_sync(0xffffffffu, wait_bar(&act_ready[j], e_prev & 1, abort));
+          if (!ok) break;
+          tc::fence_after_sync();
+#pragma unroll 4
+          for (int kk = 0; kk < kSurHidden / 16; ++kk)
+            tc::mma_bf16_warp(acc, tc::desc_kmajor(in + kk * 16 * 16, 128, kSboAct),
+                              tc::desc_kmajor(w4 + kk * (kSurOutPad * 16 * 2), 128, kSbo16), kIdOut,
+                              kk > 0 ? 1u : 0u);
+        }
+        if (!ok) break;
+        if (L < 4)
+          tc::commit_warp(&mma_epi[(it * 4 + L) & 1]);
+        else
+          tc::commit_warp(mma_out);
+      }
+    }
+    // every MMA issued has completed before the TMEM columns are released
+    tc::commit_warp(drain);
+    tc::mbar_wait(drain, 0);
+  } else if (warp < kEpiWarps) {
+    // ---- hidden epilogues
+    const int quarter = warp & 3, half = warp >> 2, row = quarter * 32 + lane;
+    bool ok = true;
+    for (int it = 0; it < my_tiles && ok; ++it) {
+      for (int L = 0; L < 4 && ok; ++L) {
+        const int g = it * 5 + L, p = g & 1, e = it * 4 + L;
+        ok = __all_sync(0xffffffffu, wait_bar(&mma_epi[e & 1], (e >> 1) & 1, abort));
+        if (!ok) break;
+        tc::fence_after_sync();
+        const uint32_t tbase = tmem + p * kSurHidden + (static_cast<uint32_t>(quarter * 32) << 16) + half * 128;
+        const float *bias = sbias + L * kSurHidden + half * 128;
+        uint8_t *out = act;
+        // the load of the next 32 columns overlaps the GELU of these
+        uint32_t ra[32], rb[32];
+        tc::tmem_ld32_issue(tbase, ra);
+        tc::tmem_ld_wait(ra);
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+          uint32_t(&cur)[32] = (s & 1) ? rb : ra;
+          uint32_t(&nxt)[32] = (s & 1) ? ra : rb;
+          if (s < 3) tc::tmem_ld32_issue(tbase + (s + 1) * 32, nxt);
+#pragma unroll
+          for (int q = 0; q < 32; q += 8) {
+            const float4 b0 = *reinterpret_cast<const float4 *>(bias + s * 32 + q);
+            const float4 b1 = *reinterpret_cast<const float4 *>(bias + s * 32 + q + 4);
+            const uint32_t p0 = gelu2_bf16(__uint_as_float(cur[q]) + b0.x, __uint_as_float(cur[q + 1]) + b0.y);
+            const uint32_t p1 = gelu2_bf16(__uint_as_float(cur[q + 2]) + b0.z, __uint_as_float(cur[q + 3]) + b0.w);
+            const uint32_t p2 = gelu2_bf16(__uint_as_float(cur[q + 4]) + b1.x, __uint_as_float(cur[q + 5]) + b1.y);
+            const uint32_t p3 = gelu2_bf16(__uint_as_float(cur[q + 6]) + b1.z, __uint_as_float(cur[q + 7]) + b1.w);
+            *reinterpret_cast<uint4 *>(out + tc::tile_offset(row, half * 128 + s * 32 + q, kSurHidden)) =
+                make_uint4(p0, p1, p2, p3);
+          }
+          if (s < 3) tc::tmem_ld_wait(nxt);
+          if (s == 2) {
+            // this warp has read all its accumulator columns
+            tc::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) bar_arrive(&acc_free[p]);
+          }
+          if (s & 1) {
+            // 64 columns written: release them to the next layer's MMAs
+            tc::fence_async_smem();
+            __syncwarp();
+            if (lane == 0) bar_arrive(&act_ready[half * 2 + (s >> 1)]);
+          }
+        }
+      }
+    }
+  } else {
+    // ---- features of the next tile, outputs of the current one
+    const int quarter = warp & 3, row = quarter * 32 + lane;
+    bool ok = true;
+    if (my_tiles > 0) {
+      tile_features<C>(B, P, static_cast<int64_t>(blockIdx.x) * kCells, row, x0);
+      tc::fence_async_smem();
+      __syncwarp();
+      if (lane == 0) bar_arrive(&feat_full[0]);
+    }
+    for (int it = 0; it < my_tiles && ok; ++it) {
+      const int64_t tile = blockIdx.x + static_cast<int64_t>(it) * gridDim.x;
+      if (it + 1 < my_tiles) {
+        const int nb = (it + 1) & 1;
+        if (it + 1 >= 2) ok = __all_sync(0xffffffffu, wait_bar(&x0_free[nb], (((it + 1) >> 1) - 1) & 1, abort));
+        if (!ok) break;
+        tile_features<C>(B, P, (tile + gridDim.x) * kCells, row, x0 + nb * kX0Bytes);
+        tc::fence_async_smem();
+        __syncwarp();
+        if (lane == 0) bar_arrive(&feat_full[nb]);
+      }
+      const int g = it * 5 + 4, p = g & 1;
+      ok = __all_sync(0xffffffffu, wait_bar(mma_out, it & 1, abort));
+      if (!ok) break;
+      tc::fence_after_sync();
+      float o[kSurOutPad];
+      tc::tmem_ld16(tmem + p * kSurHidden + (static_cast<uint32_t>(quarter * 32) << 16), o);
+      tc::fence_before_sync();
+      __syncwarp();
+      if (lane == 0) bar_arrive(&acc_free[p], 2);  // four warps stand for the eight epilogue warps
+      tile_apply<C, MODE, NE>(B, P, tile * kCells + row, o, sbias + 4 * kSurHidden, fb_count, fb_list, stats);
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, 512);
+  if (tid == 0 && *abort) atomicExch(err, 1);
 }
 
 // EPI fallback for the listed cells of block b (grid-stride over the list).

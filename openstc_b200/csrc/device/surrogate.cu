@@ -666,7 +666,8 @@ __global__ void k_decode(const float *z, const double *states, int64_t n, Surrog
   float o[NS];
   for (int k = 0; k < NS; ++k) o[k] = z[i * kSurOutPad + k];
   double d[NS];
-  const bool ok = sur::decode<NS>(gd, o, s[0], log10(s[1]), log10(s[11]), s + 2, d);
+  const bool ok = sur::decode<NS>(gd, o, static_cast<float>(s[0]), log10f(static_cast<float>(s[1])),
+                                  log10f(static_cast<float>(s[11])), s + 2, d);
   for (int k = 0; k < NS; ++k) dy[i * NS + k] = d[k];
   accepted[i] = ok ? 1 : 0;
 }
