@@ -64,6 +64,7 @@ class EngineT final : public Engine {
     tiles0_ = make_tiles(0);
     tiles1_ = make_tiles(1);
     tilesg_ = make_tiles(ngg);
+    col_tiles_ = make_col_tiles();
     cuda_check(cudaMalloc(&d_partial_, sizeof(double) * 4 * tiles0_.begin[tiles0_.nblk]), "cudaMalloc partial");
     cuda_check(cudaMalloc(&d_res_, sizeof(double) * 4), "cudaMalloc res");
     cuda_check(cudaMalloc(&d_bad_, sizeof(unsigned int)), "cudaMalloc bad");
@@ -391,6 +392,22 @@ class EngineT final : public Engine {
                                " values, caller passed " + std::to_string(count));
   }
 
+  // columns of kTX x kTY cells over kFluxKC planes (the k-marching flux kernel)
+  Tiles make_col_tiles() const {
+    Tiles t{};
+    t.nblk = static_cast<int>(blocks_.size());
+    int acc = 0;
+    for (int b = 0; b < t.nblk; ++b) {
+      const DevBlock &B = blocks_[b];
+      t.begin[b] = acc;
+      t.ntx[b] = (B.mx + kTX - 1) / kTX;
+      t.nty[b] = (B.my + kTY - 1) / kTY;
+      acc += t.ntx[b] * t.nty[b] * ((B.mz + kFluxKC - 1) / kFluxKC);
+    }
+    t.begin[t.nblk] = acc;
+    return t;
+  }
+
   Tiles make_tiles(int halo) const {
     Tiles t{};
     t.nblk = static_cast<int>(blocks_.size());
@@ -420,7 +437,7 @@ class EngineT final : public Engine {
 
   void launch_flux() {
     if constexpr (C::mixed)
-      k_flux_mx<C><<<grid(tiles0_), block3(), flux_smem_, stream_>>>(d_blocks_, tiles0_);
+      k_flux_mx_col<C><<<grid(col_tiles_), kFluxThreads, 0, stream_>>>(d_blocks_, col_tiles_);
     else
       k_flux<C><<<grid(tiles0_), block3(), flux_smem_, stream_>>>(d_blocks_, tiles0_);
   }
@@ -657,7 +674,7 @@ class EngineT final : public Engine {
   double *d_partial_ = nullptr, *d_res_ = nullptr, *h_res_ = nullptr, *d_wall_ = nullptr;
   unsigned int *d_bad_ = nullptr;
   std::vector<void *> allocations_;
-  Tiles tiles0_, tiles1_, tilesg_;
+  Tiles tiles0_, tiles1_, tilesg_, col_tiles_;
   size_t source_smem_ = 0, flux_smem_ = 0;
   int final_dq_ = 0;
   cudaGraphExec_t graphs_[4] = {nullptr, nullptr, nullptr, nullptr};

@@ -459,6 +459,42 @@ __global__ void __launch_bounds__(kCta) k_source_mx(const DevBlock *__restrict__
   OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq[l * szd + nd] = dq[l];
 }
 
+// Local time step of cell (i, j, k) in FP32 (local_time_step,
+// src/TimeAdvanceFunc.cuh:21-71); also stores the spectral radii the DPLUR
+// sweeps use.
+template <class C>
+__device__ __forceinline__ void local_time_step_mx(const DevBlock &B, int i, int j, int k, int64_t n, int64_t nd) {
+  const int64_t szd = B.D.size;
+  const bool three_d = B.mz > 1;
+  const int64_t sz = B.G.size;
+  const double *m = B.metric;
+  using fp32::ldf;
+  const float m11 = ldf(m + n), m12 = ldf(m + sz + n), m13 = ldf(m + 2 * sz + n);
+  const float m21 = ldf(m + 3 * sz + n), m22 = ldf(m + 4 * sz + n), m23 = ldf(m + 5 * sz + n);
+  const float m31 = ldf(m + 6 * sz + n), m32 = ldf(m + 7 * sz + n), m33 = ldf(m + 8 * sz + n);
+  const float grad_xi = sqrtf(m11 * m11 + m12 * m12 + m13 * m13);
+  const float grad_eta = sqrtf(m21 * m21 + m22 * m22 + m23 * m23);
+  const float grad_zeta = sqrtf(m31 * m31 + m32 * m32 + m33 * m33);
+  const float u = ldf(B.bv + sz + n), v = ldf(B.bv + 2 * sz + n), w = ldf(B.bv + 3 * sz + n);
+  const float a = ldf(B.acoustic + n);
+  const float s0 = fabsf(u * m11 + v * m12 + w * m13) + a * grad_xi;
+  const float s1 = fabsf(u * m21 + v * m22 + w * m23) + a * grad_eta;
+  const float s2 = three_d ? fabsf(u * m31 + v * m32 + w * m33) + a * grad_zeta : 0.f;
+  B.inv_spec[nd] = s0;
+  B.inv_spec[szd + nd] = s1;
+  B.inv_spec[2 * szd + nd] = s2;
+  float gamma = 1.4f;
+  if constexpr (C::mix != 0) gamma = ldf(B.gamma + n);
+  const float coeff_1 = fmaxf(gamma, 4.f / 3.f) / ldf(B.bv + n);
+  float coeff_2 = ldf(B.mul + n) / cF.Pr;
+  if constexpr (C::turb) coeff_2 += ldf(B.mut + n) / cF.Prt;
+  float srv = grad_xi * grad_xi + grad_eta * grad_eta;
+  if (three_d) srv += grad_zeta * grad_zeta;
+  srv *= coeff_1 * coeff_2;
+  B.visc_spec[nd] = srv;
+  B.dt_local[B.Z.at(i, j, k)] = cF.cfl / (s0 + s1 + s2 + srv);
+}
+
 // Inviscid + viscous flux differences in FP32 (accumulated in FP32 and added
 // to the FP64 source terms), then the local time step.
 template <class C>
@@ -503,34 +539,142 @@ __global__ void __launch_bounds__(kCta, 4) k_flux_mx(const DevBlock *__restrict_
     }
   }
   OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq[l * szd + nd] += static_cast<double>(acc[l]);
+  local_time_step_mx<C>(B, i, j, k, n, nd);
+}
 
-  const int64_t sz = B.G.size;
-  const double *m = B.metric;
-  using fp32::ldf;
-  const float m11 = ldf(m + n), m12 = ldf(m + sz + n), m13 = ldf(m + 2 * sz + n);
-  const float m21 = ldf(m + 3 * sz + n), m22 = ldf(m + 4 * sz + n), m23 = ldf(m + 5 * sz + n);
-  const float m31 = ldf(m + 6 * sz + n), m32 = ldf(m + 7 * sz + n), m33 = ldf(m + 8 * sz + n);
-  const float grad_xi = sqrtf(m11 * m11 + m12 * m12 + m13 * m13);
-  const float grad_eta = sqrtf(m21 * m21 + m22 * m22 + m23 * m23);
-  const float grad_zeta = sqrtf(m31 * m31 + m32 * m32 + m33 * m33);
-  const float u = ldf(B.bv + sz + n), v = ldf(B.bv + 2 * sz + n), w = ldf(B.bv + 3 * sz + n);
-  const float a = ldf(B.acoustic + n);
-  const float s0 = fabsf(u * m11 + v * m12 + w * m13) + a * grad_xi;
-  const float s1 = fabsf(u * m21 + v * m22 + w * m23) + a * grad_eta;
-  const float s2 = three_d ? fabsf(u * m31 + v * m32 + w * m33) + a * grad_zeta : 0.f;
-  B.inv_spec[nd] = s0;
-  B.inv_spec[szd + nd] = s1;
-  B.inv_spec[2 * szd + nd] = s2;
-  float gamma = 1.4f;
-  if constexpr (C::mix != 0) gamma = ldf(B.gamma + n);
-  const float coeff_1 = fmaxf(gamma, 4.f / 3.f) / ldf(B.bv + n);
-  float coeff_2 = ldf(B.mul + n) / cF.Pr;
-  if constexpr (C::turb) coeff_2 += ldf(B.mut + n) / cF.Prt;
-  float srv = grad_xi * grad_xi + grad_eta * grad_eta;
-  if (three_d) srv += grad_zeta * grad_zeta;
-  srv *= coeff_1 * coeff_2;
-  B.visc_spec[nd] = srv;
-  B.dt_local[B.Z.at(i, j, k)] = cF.cfl / (s0 + s1 + s2 + srv);
+// The same flux differences with every face evaluated once.  A CTA owns a
+// column of 32 x 4 cells (i, j) over kFluxKC planes of k and marches in k:
+// the four compute warps (warp = j offset, lane = i offset) evaluate the
+// plus faces of their cells in x, y and z; the fifth warp evaluates the
+// minus faces on the column's low i and low j sides; the low-k face of a
+// plane is the high-k face of the plane before, carried in shared memory.
+// Each face value is the one k_flux_mx computes for it, and the per-cell
+// sums run in the same order, so the result is bit-identical.
+constexpr int kFluxKC = 8;                  // k planes per column
+constexpr int kFluxThreads = kCta + 32;    // 4 compute warps + the minus-face warp
+
+__device__ __forceinline__ void col_tile(const Tiles &T, int &b, int &i0, int &j0, int &k0) {
+  int t = blockIdx.x;
+  b = 0;
+  while (b + 1 < T.nblk && t >= T.begin[b + 1]) ++b;
+  t -= T.begin[b];
+  const int tx = t % T.ntx[b];
+  t /= T.ntx[b];
+  const int ty = t % T.nty[b];
+  const int tz = t / T.nty[b];
+  i0 = tx * kTX;
+  j0 = ty * kTY;
+  k0 = tz * kFluxKC;
+}
+
+// Shared-memory plan of the column kernel (floats): x faces [NV][kTY][kTX+1]
+// (face i0 - 1/2 + f), y faces [NV][kTY+1][kTX] (face j0 - 1/2 + f), the
+// low-k faces carried between planes [2][NV][kCta] (inviscid, viscous) and
+// the high-k faces of the current plane [NV][kCta].
+template <int NV>
+struct ColSmem {
+  static constexpr int xs = 0, ys = xs + NV * kTY * (kTX + 1), zs = ys + NV * (kTY + 1) * kTX,
+                       zp = zs + 2 * NV * kCta, size = zp + NV * kCta;
+};
+
+// One face type (VISC 0: inviscid, 1: viscous) of plane k of a column: every
+// face into shared memory (one inlined face evaluation, looped over the
+// thread's faces), then each cell's differences in the order x, y, z,
+// subtracted (inviscid) or added (viscous).
+template <class C, int VISC>
+__device__ __forceinline__ void col_faces(const DevBlock &B, int i0, int j0, int k, bool first, bool cell,
+                                          float *sm, float *acc) {
+  constexpr int NV = C::nv;
+  using S = ColSmem<NV>;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
+  const int i = i0 + lane, j = j0 + warp;
+  const int64_t sx = B.G.sx, sxy = B.G.sxy;
+  const bool three_d = B.mz > 1;
+  float *zs = sm + S::zs + VISC * NV * kCta;
+  const int ntask = cell ? (three_d ? (first ? 4 : 3) : 2) : (warp == kTY ? 2 : 0);
+#pragma unroll 1
+  for (int q = 0; q < ntask; ++q) {
+    int64_t nl = 0, s = 1;
+    int d = 0, off = 0, stride = kCta;
+    bool valid = true;
+    if (cell) {
+      const int64_t n = B.G.at(i, j, k);
+      const int task = (q >= 2 && !first) ? q + 1 : q;  // x, y, low z (first plane), high z
+      if (task == 0) {
+        nl = n; d = 0; s = 1; off = S::xs + warp * (kTX + 1) + lane + 1; stride = kTY * (kTX + 1);
+      } else if (task == 1) {
+        nl = n; d = 1; s = sx; off = S::ys + (warp + 1) * kTX + lane; stride = (kTY + 1) * kTX;
+      } else if (task == 2) {
+        nl = n - sxy; d = 2; s = sxy; off = static_cast<int>(zs - sm) + tid;
+      } else {
+        nl = n; d = 2; s = sxy; off = S::zp + tid;
+      }
+    } else if (q == 0) {  // low-i faces of the column's rows
+      valid = lane < kTY && j0 + lane < B.my && i0 < B.mx;
+      if (valid) nl = B.G.at(i0, j0 + lane, k) - 1;
+      d = 0; s = 1; off = S::xs + lane * (kTX + 1); stride = kTY * (kTX + 1);
+    } else {  // low-j faces of the column's i
+      valid = i < B.mx && j0 < B.my;
+      if (valid) nl = B.G.at(i, j0, k) - sx;
+      d = 1; s = sx; off = S::ys + lane; stride = (kTY + 1) * kTX;
+    }
+    if (!valid) continue;
+    float t[NV];
+    if constexpr (VISC == 0)
+      fp32::inviscid_face<C>(B, nl, d, s, t);
+    else
+      fp32::viscous_face<C>(B, nl, d, s, t);
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) sm[off + l * stride] = t[l];
+  }
+  __syncthreads();
+  if (cell) {
+    const float *xs = sm + S::xs + warp * (kTX + 1) + lane, *ys = sm + S::ys + warp * kTX + lane;
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) {
+      const float dx = xs[l * kTY * (kTX + 1) + 1] - xs[l * kTY * (kTX + 1)];
+      const float dy = ys[l * (kTY + 1) * kTX + kTX] - ys[l * (kTY + 1) * kTX];
+      if constexpr (VISC == 0) {
+        acc[l] -= dx;
+        acc[l] -= dy;
+      } else {
+        acc[l] += dx;
+        acc[l] += dy;
+      }
+      if (three_d) {
+        const float zp = sm[S::zp + l * kCta + tid];
+        const float dz = zp - zs[l * kCta + tid];
+        zs[l * kCta + tid] = zp;
+        if constexpr (VISC == 0)
+          acc[l] -= dz;
+        else
+          acc[l] += dz;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+template <class C>
+__global__ void __launch_bounds__(kFluxThreads, 3) k_flux_mx_col(const DevBlock *__restrict__ blks, Tiles T) {
+  constexpr int NV = C::nv;
+  __shared__ float sm[ColSmem<NV>::size];
+  int b, i0, j0, k0;
+  col_tile(T, b, i0, j0, k0);
+  const DevBlock &B = blks[b];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = i0 + lane, j = j0 + warp;
+  const bool cell = warp < kTY && i < B.mx && j < B.my;
+  const int64_t szd = B.D.size;
+  const int k1 = min(k0 + kFluxKC, B.mz);
+  for (int k = k0; k < k1; ++k) {
+    float acc[NV];
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) acc[l] = 0;
+    col_faces<C, 0>(B, i0, j0, k, k == k0, cell, sm, acc);
+    if (cP.viscous_order != 0) col_faces<C, 1>(B, i0, j0, k, k == k0, cell, sm, acc);
+    if (!cell) continue;
+    const int64_t n = B.G.at(i, j, k), nd = B.D.at(i, j, k);
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq[l * szd + nd] += static_cast<double>(acc[l]);
+    local_time_step_mx<C>(B, i, j, k, n, nd);
+  }
 }
 
 // DPLUR sweep with FP32 flux-Jacobian products; the update of the point
