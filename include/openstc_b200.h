@@ -233,10 +233,10 @@ int ostc_surrogate_set_params(ostc_surrogate *s, const float *flat);
 int ostc_surrogate_normalisation(const ostc_surrogate *s, float *in_mu, float *in_sig, float *out_c, float *out_scale);
 /* The per-cell trust gate: inputs in the training box, |network output| <=
    out_max, element defect <= defect_tol of the element totals, |dY_k| <=
-   rel_max (Y_k + 1e-10); other cells take the EPI fallback.  Takes effect
-   for drivers at their next ostc_driver_set_surrogate. */
+   rel_max (Y_k + max(y_floor, 1e-10)); other cells take the EPI fallback.
+   Takes effect for drivers at their next ostc_driver_set_surrogate. */
 typedef struct ostc_surrogate_gate {
-  float t_min, t_max, lp_min, lp_max, ldt_min, ldt_max, defect_tol, rel_max, out_max;
+  float t_min, t_max, lp_min, lp_max, ldt_min, ldt_max, defect_tol, rel_max, out_max, y_floor;
 } ostc_surrogate_gate;
 int ostc_surrogate_get_gate(const ostc_surrogate *s, ostc_surrogate_gate *g);
 int ostc_surrogate_set_gate(ostc_surrogate *s, const ostc_surrogate_gate *g);

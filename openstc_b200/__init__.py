@@ -46,7 +46,7 @@ class SurrogateEval(C.Structure):
 
 class SurrogateGate(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("t_min", "t_max", "lp_min", "lp_max", "ldt_min", "ldt_max", "defect_tol",
-                                         "rel_max", "out_max")]
+                                         "rel_max", "out_max", "y_floor")]
 
 
 class Info(C.Structure):

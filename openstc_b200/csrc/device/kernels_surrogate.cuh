@@ -52,7 +52,8 @@ __device__ inline void epi_increment(double T, double rho, const double *Y, doub
 // (weighted least squares, weights |dY_k| + 1e-3 Y_k).  The cell is accepted
 // when the inputs lie in the training box, every output is within
 // gate.out_max, the raw element defect is below gate.defect_tol of the
-// element totals, no increment exceeds gate.rel_max (Y_k + eps), and no mass
+// element totals, no increment exceeds gate.rel_max (Y_k + gate.y_floor)
+// (species below the floor are judged by their absolute change), and no mass
 // fraction is driven below -1e-9: the network is trusted where the chemistry
 // changes the composition little, the EPI step takes the reacting cells.
 // NE is a compile-time bound on the element count (elements past p.n_elem
@@ -70,7 +71,7 @@ __device__ __forceinline__ bool decode_ne(const SurrogateDev &p, const float *o,
     ok = ok && fabsf(o[k]) <= g.out_max;
     const float oc = fminf(fmaxf(o[k], -g.out_max), g.out_max);
     dy[k] = (Y[k] + kSurYEps) * static_cast<double>(p.out_c[k] * sinhf(oc * p.out_s[k]));
-    if (fabs(dy[k]) > g.rel_max * (Y[k] + kSurYEps)) ok = false;
+    if (fabs(dy[k]) > g.rel_max * (Y[k] + fmax(kSurYEps, static_cast<double>(g.y_floor)))) ok = false;
     w[k] = static_cast<float>(fabs(dy[k]) + 1e-3 * Y[k]) + 1e-30f;
   }
   // normal equations (E W E^T) lambda = E dy, E[e][k] = a_ek / W_k

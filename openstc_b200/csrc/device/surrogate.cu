@@ -817,7 +817,7 @@ const SurrogateDev &Surrogate::device_params() {
 void Surrogate::save(const std::string &path) const {
   std::ofstream f(path, std::ios::binary);
   if (!f) throw std::runtime_error("cannot write " + path);
-  const char magic[8] = {'O', 'S', 'T', 'C', 'M', 'L', 'P', '3'};
+  const char magic[8] = {'O', 'S', 'T', 'C', 'M', 'L', 'P', '4'};
   f.write(magic, 8);
   f.write(reinterpret_cast<const char *>(in_mu.data()), sizeof(in_mu));
   f.write(reinterpret_cast<const char *>(in_sig.data()), sizeof(in_sig));
@@ -832,7 +832,7 @@ void Surrogate::load(const std::string &path) {
   if (!f) throw std::runtime_error("cannot open " + path);
   char magic[8];
   f.read(magic, 8);
-  if (std::memcmp(magic, "OSTCMLP3", 8) != 0) throw std::runtime_error(path + " is not a surrogate file");
+  if (std::memcmp(magic, "OSTCMLP4", 8) != 0) throw std::runtime_error(path + " is not a surrogate file");
   f.read(reinterpret_cast<char *>(in_mu.data()), sizeof(in_mu));
   f.read(reinterpret_cast<char *>(in_sig.data()), sizeof(in_sig));
   f.read(reinterpret_cast<char *>(out_c.data()), sizeof(out_c));

@@ -36,8 +36,9 @@ struct SurrogateGate {
   float lp_min = 4.5f, lp_max = 6.0f;      // log10 p [Pa]
   float ldt_min = -9.0f, ldt_max = -6.0f;  // log10 dt [s]
   float defect_tol = 1e-3f;                // element-conservation defect (relative)
-  float rel_max = 0.01f;                   // largest accepted |dY_k| / (Y_k + eps)
+  float rel_max = 0.01f;                   // largest accepted |dY_k| / (Y_k + y_floor)
   float out_max = 6.f;                     // largest accepted |network output|
+  float y_floor = 1e-10f;                  // mass fraction below which changes count as absolute
 };
 
 // Parameters the fused inference kernel reads (device memory).
