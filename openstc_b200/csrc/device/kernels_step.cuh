@@ -41,11 +41,11 @@ __global__ void __launch_bounds__(kCta) k_source(const DevBlock *__restrict__ bl
   }
   if constexpr (C::mix == 2) {
     if (B.chem_quiet && B.chem_quiet[nz]) {
-      // judged chemically quiet by the surrogate: its rate, no Jacobian
+      // judged chemically quiet by the surrogate: its rate and no Jacobian
+      // (the implicit stages treat the cell's species diagonally and never
+      // read its chem_jac)
       const double jac = ld(B.jac + n);
       OSTC_UNROLL for (int l = 0; l < NS; ++l) dq[l + 5] = jac * B.chem_rate[l * sz0 + nz];
-      const int nj = cP.chem_src_method == 1 ? NS * NS : (cP.chem_src_method == 2 ? NS : 0);
-      for (int q = 0; q < nj; ++q) B.chem_jac[q * sz0 + nz] = 0;
     } else {
     const int tid = threadIdx.x + kTX * (threadIdx.y + kTY * threadIdx.z);
     double *q1 = sq + tid, *q2 = sq + cP.nr * kCta + tid;
@@ -253,7 +253,9 @@ __global__ void __launch_bounds__(kCta) k_point_implicit(const DevBlock *__restr
   const int64_t nd = B.D.at(i, j, k), nz = B.Z.at(i, j, k), szd = B.D.size, sz0 = B.Z.size;
   const double dt = B.dt_local[nz];
   if constexpr (C::mix == 2) {
-    if (cP.chem_src_method == 1) {
+    // a chemically quiet cell has no chemistry Jacobian: I x = dq leaves dq
+    if (B.chem_quiet && B.chem_quiet[nz]) {
+    } else if (cP.chem_src_method == 1) {
       double lhs[NS * NS];
       int piv[NS];
       OSTC_UNROLL for (int m = 0; m < NS; ++m)
@@ -302,7 +304,11 @@ __global__ void __launch_bounds__(kCta) k_dq0(const DevBlock *__restrict__ blks,
   } else {
     OSTC_UNROLL for (int l = 0; l < 5; ++l) dq[l] /= diag;
     const int method = cP.chem_src_method;
-    if (method == 1) {
+    if (B.chem_quiet && B.chem_quiet[nz]) {
+      // no chemistry Jacobian: the factorisation of diag I is diag I, and
+      // its solve divides by diag (bit for bit)
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) dq[5 + l] /= diag;
+    } else if (method == 1) {
       double lhs[NS * NS];
       int piv[NS];
       OSTC_UNROLL for (int m = 0; m < NS; ++m)
@@ -420,7 +426,10 @@ __global__ void __launch_bounds__(kCta, OSTC_SWEEP_MIN_BLOCKS) k_sweep(const Dev
   } else {
     OSTC_UNROLL for (int l = 0; l < 5; ++l) out[l] = B.dq0[l * szd + nd] + dt * tot[l] / diag;
     const int method = cP.chem_src_method;
-    if (method == 1) {
+    if (B.chem_quiet && B.chem_quiet[nz]) {
+      // chemically quiet: the stored factors would be diag I
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) out[5 + l] = B.dq0[(5 + l) * szd + nd] + dt * tot[5 + l] / diag;
+    } else if (method == 1) {
       double lhs[NS * NS];
       int piv[NS];
       OSTC_UNROLL for (int q = 0; q < NS * NS; ++q) lhs[q] = B.chem_jac[q * sz0 + nz];
