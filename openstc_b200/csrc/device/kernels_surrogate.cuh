@@ -132,17 +132,18 @@ __device__ __forceinline__ bool decode(const SurrogateDev &p, const float *o, fl
 // ------------------------------------------------------------ fused kernel
 // A persistent kernel, one CTA per SM, that runs the tiles of 128 cells of a
 // block through the network as a software pipeline on mbarriers:
-//   * warp 9 (one lane) streams the hidden layers' weights through a ring of
-//     kStages shared-memory stages, one 32 KB stage (K = 64) per 64-column
-//     activation group, in the order the MMAs consume them; the first and
-//     output layers' weights (8 KB each) stay resident;
-//   * warp 8 issues the tcgen05 MMAs of global layer g (tile g / 5, layer
+//   * warp 17 (one lane) streams the hidden layers' weights through a ring
+//     of kStages shared-memory stages of 32 KB (K = 64), in the order the MMAs
+//     consume them; the first and output layers' weights (8 KB each) stay
+//     resident;
+//   * warp 16 issues the tcgen05 MMAs of global layer g (tile g / 5, layer
 //     g % 5) into accumulator g % 2 (2 x 256 TMEM columns);
-//   * warps 0-7 (TMEM lane quarter w % 4, column half w / 4) run the hidden
-//     epilogues: accumulator + bias -> GELU -> bf16 activations, each 64-
-//     column group released to the MMA of the next layer as soon as it is
-//     written, so that MMA overlaps this epilogue;
-//   * warps 10-13 (lane quarters 2, 3, 0, 1) compute the features of the
+//   * warps 0-15 (TMEM lane quarter w % 4, column group w / 4) run the hidden
+//     epilogues: accumulator + bias -> GELU -> bf16 activations in two steps,
+//     step s covering columns 32 (w / 4) + 128 s; each step's 128 columns are
+//     released to the MMAs of the next layer as soon as all sixteen warps have
+//     written them, so that MMA overlaps the second half of this epilogue;
+//   * warps 18-21 (lane quarters 2, 3, 0, 1) compute the features of the
 //     next tile and decode / gate / apply the outputs of the current one.
 // One activation buffer serves every layer (the epilogue of layer L only
 // starts once the MMAs of layer L, its last readers, have completed), and
@@ -151,9 +152,9 @@ __device__ __forceinline__ bool decode(const SurrogateDev &p, const float *o, fl
 // out raises the CTA's abort flag, every role then leaves its loop, the MMAs
 // and copies in flight are drained, and the kernel reports the error.
 constexpr int kCells = 128;
-constexpr int kEpiWarps = 8;
-constexpr int kMmaWarp = 8, kLoadWarp = 9, kIoWarp0 = 10;
-constexpr int kThreads = 32 * 14;
+constexpr int kEpiWarps = 16;
+constexpr int kMmaWarp = 16, kLoadWarp = 17, kIoWarp0 = 18;
+constexpr int kThreads = 32 * 22;
 constexpr int kStageChunks = 4;  // weight chunks per ring stage
 constexpr int kStages = 4;       // ring stages
 constexpr int kFusedElem = 4;  // largest element count of the fused kernel's conservation gate
@@ -165,25 +166,21 @@ constexpr int kTileStages = 3 * 4;  // streamed stages per tile: 3 hidden layers
 constexpr uint32_t kActBytes = 128 * kSurHidden * 2;
 constexpr uint32_t kStageBytes = kStageChunks * kChunkBytes;
 constexpr uint32_t kX0Bytes = 128 * kSurInPad * 2;
-// barriers: full[S], empty[S], feat_full[2], x0_free[2], mma_epi[2], mma_out, acc_free[2], act_ready[4], res,
+// barriers: full[S], empty[S], feat_full[2], x0_free[2], mma_epi[2], mma_out, acc_free[2], act_ready[2], res,
 // drain.  Each barrier has waiters that are never more than one phase behind
 // its arrivals, which is what parity waits need: the hidden layers' MMAs
 // signal the epilogue through mma_epi (by epilogue index), the output layer's
 // the decode through mma_out (by tile).
-constexpr int kBars = 2 * kStages + 2 + 2 + 2 + 1 + 2 + 4 + 1 + 1;
+constexpr int kBars = 2 * kStages + 2 + 2 + 2 + 1 + 2 + 2 + 1 + 1;
 constexpr uint32_t kBiasBytes = (4 * kSurHidden + kSurOutPad) * 4;  // every layer's bias, staged once per CTA
 constexpr uint32_t kSmem = kActBytes + 2 * kX0Bytes + 2 * kChunkBytes + kStages * kStageBytes + kBiasBytes + kBars * 8 + 16;
 static_assert(kSmem <= 232448, "shared memory of one CTA");
 
-// A hidden layer's K is consumed in the order the epilogue releases its
-// 64-column activation groups (group j = 2 * half + step / 2 holds K chunks
-// 4j..4j+3, and the two column halves run side by side): groups 0, 2, 1, 3.
-__host__ __device__ constexpr int group_order(int gq) { return gq == 1 ? 2 : (gq == 2 ? 1 : gq); }
-
-// Source of streamed stage s (0..kTileStages-1) of a tile: 4 contiguous K
-// chunks of a hidden layer's packed weights
+// Source of streamed stage s (0..kTileStages-1) of a tile: K chunks
+// 4 (s % 4) .. 4 (s % 4) + 3 of hidden layer 1 + s / 4, contiguous in its
+// packed weights
 __device__ __forceinline__ const uint8_t *stage_src(const SurrogateDev &P, int s) {
-  return P.w_packed[1 + s / 4] + static_cast<size_t>(group_order(s % 4)) * kStageBytes;
+  return P.w_packed[1 + s / 4] + static_cast<size_t>(s % 4) * kStageBytes;
 }
 
 // Asynchronous bulk copies into shared memory: the stage's mbarrier is told
@@ -367,7 +364,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sur_infer(const DevBlock *__res
   uint64_t *bars = reinterpret_cast<uint64_t *>(reinterpret_cast<uint8_t *>(sbias) + kBiasBytes);
   uint64_t *full = bars, *empty = full + kStages, *feat_full = empty + kStages, *x0_free = feat_full + 2,
            *mma_epi = x0_free + 2, *mma_out = mma_epi + 2, *acc_free = mma_out + 1, *act_ready = acc_free + 2,
-           *drain = act_ready + 4, *res_full = drain + 1;
+           *drain = act_ready + 2, *res_full = drain + 1;
   uint32_t *tslot = reinterpret_cast<uint32_t *>(drain + 1);
   volatile int *abort = reinterpret_cast<volatile int *>(tslot + 1);
   const DevBlock &B = blks[b];
@@ -389,7 +386,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sur_infer(const DevBlock *__res
       tc::mbar_init(&mma_epi[q], 1);
       tc::mbar_init(&acc_free[q], kEpiWarps);
     }
-    for (int q = 0; q < 4; ++q) tc::mbar_init(&act_ready[q], 4);
+    for (int q = 0; q < 2; ++q) tc::mbar_init(&act_ready[q], kEpiWarps);
     tc::mbar_init(mma_out, 1);
     tc::mbar_init(drain, 1);
     tc::mbar_init(res_full, 1);
@@ -448,21 +445,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_sur_infer(const DevBlock *__res
           tc::commit_warp(&x0_free[tb]);
         } else if (L < 4) {
           for (int gq = 0; gq < 4 && ok; ++gq, ++si) {
-            const int j = group_order(gq), slot = si % kStages;
-            ok = __all_sync(0xffffffffu, wait_bar(&act_ready[j], e_prev & 1, abort));
+            const int slot = si % kStages;
+            if ((gq & 1) == 0) ok = __all_sync(0xffffffffu, wait_bar(&act_ready[gq >> 1], e_prev & 1, abort));
             if (ok) ok = __all_sync(0xffffffffu, wait_bar(&full[slot], (si / kStages) & 1, abort));
             if (!ok) break;
             tc::fence_after_sync();
             const uint32_t wb = tc::smem_u32(stages + slot * kStageBytes);
 #pragma unroll
             for (int c = 0; c < 4; ++c)
-              tc::mma_bf16_warp(acc, tc::desc_kmajor(in + (4 * j + c) * 16 * 16, 128, kSboAct),
+              tc::mma_bf16_warp(acc, tc::desc_kmajor(in + (4 * gq + c) * 16 * 16, 128, kSboAct),
                                 tc::desc_kmajor(wb + c * kChunkBytes, 128, kSbo16), kIdHidden,
                                 (gq > 0 || c > 0) ? 1u : 0u);
             tc::commit_warp(&empty[slot]);
           }
         } else {
-          for (int j = 0; j < 4 && ok; ++j) ok = __all_sync(0xffffffffu, wait_bar(&act_ready[j], e_prev & 1, abort));
+          for (int j = 0; j < 2 && ok; ++j) ok = __all_sync(0xffffffffu, wait_bar(&act_ready[j], e_prev & 1, abort));
           if (!ok) break;
           tc::fence_after_sync();
 #pragma unroll 4
@@ -483,7 +480,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sur_infer(const DevBlock *__res
     tc::mbar_wait(drain, 0);
   } else if (warp < kEpiWarps) {
     // ---- hidden epilogues
-    const int quarter = warp & 3, half = warp >> 2, row = quarter * 32 + lane;
+    const int quarter = warp & 3, cg = warp >> 2, row = quarter * 32 + lane;
     bool ok = true;
     for (int it = 0; it < my_tiles && ok; ++it) {
       for (int L = 0; L < 4 && ok; ++L) {
@@ -491,42 +488,34 @@ __global__ void __launch_bounds__(kThreads, 1) k_sur_infer(const DevBlock *__res
         ok = __all_sync(0xffffffffu, wait_bar(&mma_epi[e & 1], (e >> 1) & 1, abort));
         if (!ok) break;
         tc::fence_after_sync();
-        const uint32_t tbase = tmem + p * kSurHidden + (static_cast<uint32_t>(quarter * 32) << 16) + half * 128;
-        const float *bias = sbias + L * kSurHidden + half * 128;
-        uint8_t *out = act;
-        // the load of the next 32 columns overlaps the GELU of these
-        uint32_t ra[32], rb[32];
-        tc::tmem_ld32_issue(tbase, ra);
-        tc::tmem_ld_wait(ra);
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-          uint32_t(&cur)[32] = (s & 1) ? rb : ra;
-          uint32_t(&nxt)[32] = (s & 1) ? ra : rb;
-          if (s < 3) tc::tmem_ld32_issue(tbase + (s + 1) * 32, nxt);
+        const uint32_t tbase = tmem + p * kSurHidden + (static_cast<uint32_t>(quarter * 32) << 16) + cg * 32;
+        const float *bias = sbias + L * kSurHidden + cg * 32;
+#pragma unroll 1
+        for (int s = 0; s < 2; ++s) {
+          uint32_t cur[32];
+          tc::tmem_ld32_issue(tbase + s * 128, cur);
+          tc::tmem_ld_wait(cur);
 #pragma unroll
           for (int q = 0; q < 32; q += 8) {
-            const float4 b0 = *reinterpret_cast<const float4 *>(bias + s * 32 + q);
-            const float4 b1 = *reinterpret_cast<const float4 *>(bias + s * 32 + q + 4);
+            const float4 b0 = *reinterpret_cast<const float4 *>(bias + s * 128 + q);
+            const float4 b1 = *reinterpret_cast<const float4 *>(bias + s * 128 + q + 4);
             const uint32_t p0 = gelu2_bf16(__uint_as_float(cur[q]) + b0.x, __uint_as_float(cur[q + 1]) + b0.y);
             const uint32_t p1 = gelu2_bf16(__uint_as_float(cur[q + 2]) + b0.z, __uint_as_float(cur[q + 3]) + b0.w);
             const uint32_t p2 = gelu2_bf16(__uint_as_float(cur[q + 4]) + b1.x, __uint_as_float(cur[q + 5]) + b1.y);
             const uint32_t p3 = gelu2_bf16(__uint_as_float(cur[q + 6]) + b1.z, __uint_as_float(cur[q + 7]) + b1.w);
-            *reinterpret_cast<uint4 *>(out + tc::tile_offset(row, half * 128 + s * 32 + q, kSurHidden)) =
+            *reinterpret_cast<uint4 *>(act + tc::tile_offset(row, s * 128 + cg * 32 + q, kSurHidden)) =
                 make_uint4(p0, p1, p2, p3);
           }
-          if (s < 3) tc::tmem_ld_wait(nxt);
-          if (s == 2) {
+          if (s == 1) {
             // this warp has read all its accumulator columns
             tc::fence_before_sync();
             __syncwarp();
             if (lane == 0) bar_arrive(&acc_free[p]);
           }
-          if (s & 1) {
-            // 64 columns written: release them to the next layer's MMAs
-            tc::fence_async_smem();
-            __syncwarp();
-            if (lane == 0) bar_arrive(&act_ready[half * 2 + (s >> 1)]);
-          }
+          // columns 128 s .. 128 s + 127 written by all epilogue warps: release them
+          tc::fence_async_smem();
+          __syncwarp();
+          if (lane == 0) bar_arrive(&act_ready[s]);
         }
       }
     }
@@ -559,7 +548,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sur_infer(const DevBlock *__res
       tc::tmem_ld16(tmem + p * kSurHidden + (static_cast<uint32_t>(quarter * 32) << 16), o);
       tc::fence_before_sync();
       __syncwarp();
-      if (lane == 0) bar_arrive(&acc_free[p], 2);  // four warps stand for the eight epilogue warps
+      if (lane == 0) bar_arrive(&acc_free[p], kEpiWarps / 4);  // four warps stand for the epilogue warps
       tile_apply<C, MODE, NE>(B, P, tile * kCells + row, o, sbias + 4 * kSurHidden, fb_count, fb_list, stats);
     }
   }
