@@ -392,7 +392,7 @@ __device__ __forceinline__ void sst_source(const DevBlock &B, int64_t n, double 
 // dq = source terms: SST in FP32, finite-rate chemistry and its EPI Jacobian
 // in FP64 (the same code as the FP64 path).
 template <class C>
-__global__ void __launch_bounds__(kCta) k_source_mx(const DevBlock *__restrict__ blks, Tiles T) {
+__global__ void __launch_bounds__(kCta, 4) k_source_mx(const DevBlock *__restrict__ blks, Tiles T) {
   constexpr int NS = C::ns, NV = C::nv;
   extern __shared__ double sq[];
   int b, i, j, k;

@@ -12,7 +12,7 @@ constexpr int kCta = kTX * kTY * kTZ;
 // compute_source (src/SourceTerm.cuh:11-40) fused with the reset of dq:
 // writes every dq component of an interior cell (zero + source).
 template <class C>
-__global__ void __launch_bounds__(kCta) k_source(const DevBlock *__restrict__ blks, Tiles T) {
+__global__ void __launch_bounds__(kCta, 4) k_source(const DevBlock *__restrict__ blks, Tiles T) {
   constexpr int NS = C::ns, NV = C::nv;
   extern __shared__ double sq[];  // q1, q2: 2 * n_reac * kCta doubles
   int b, i, j, k;
