@@ -194,14 +194,20 @@ int ostc_tc_gemm_bf16(const void *A, int lda, const void *B, int ldb, float *D, 
    weights, Adam. */
 typedef struct ostc_surrogate ostc_surrogate;
 
+/* Held-out statistics against the FP64 EPI labels.  rel = max_k |dY_k -
+   dY_EPI,k| / max_k |dY_EPI,k| per sample, over samples with max |dY_EPI| > 1e-6
+   (smaller increments change nothing the solver resolves). */
 typedef struct ostc_surrogate_eval {
-  double mean_rel;    /* mean over samples of max_k |dY - dY_EPI| / max_k |dY_EPI| (samples with max |dY_EPI| > 1e-8) */
-  double max_rel;
-  double mean_abs;    /* mean |dY - dY_EPI| */
-  double max_defect;  /* element-conservation defect, max over elements of |sum_k a_ek dY_k/W_k| / sum_k a_ek Y_k/W_k */
+  double mean_rel, max_rel; /* over the samples the trust gate accepts */
+  double mean_abs;          /* accepted: mean |dY - dY_EPI| */
+  double max_defect;        /* accepted: element defect of the applied (projected) dY, max over elements of
+                               |sum_k a_ek dY_k/W_k| / sum_k a_ek Y_k/W_k */
   double mean_defect;
-  double gate_pass;   /* fraction of samples the trust gate accepts */
+  double median_rel_all;    /* every sample: median and 90th percentile of rel */
+  double p90_rel_all;
+  double gate_pass;         /* fraction of samples the trust gate accepts */
   long long count;
+  long long nonfinite;      /* samples whose (rejected) prediction was not finite */
 } ostc_surrogate_eval;
 
 /* Mechanism and device from the driver (9-species finite-rate case). */

@@ -40,8 +40,9 @@ class Options(C.Structure):
 
 class SurrogateEval(C.Structure):
     _fields_ = [("mean_rel", C.c_double), ("max_rel", C.c_double), ("mean_abs", C.c_double),
-                ("max_defect", C.c_double), ("mean_defect", C.c_double), ("gate_pass", C.c_double),
-                ("count", C.c_longlong)]
+                ("max_defect", C.c_double), ("mean_defect", C.c_double), ("median_rel_all", C.c_double),
+                ("p90_rel_all", C.c_double), ("gate_pass", C.c_double), ("count", C.c_longlong),
+                ("nonfinite", C.c_longlong)]
 
 
 class SurrogateGate(C.Structure):

@@ -438,8 +438,11 @@ int ostc_surrogate_evaluate(ostc_surrogate *s, long long begin, long long count,
     out->mean_abs = e.mean_abs;
     out->max_defect = e.max_defect;
     out->mean_defect = e.mean_defect;
+    out->median_rel_all = e.median_rel_all;
+    out->p90_rel_all = e.p90_rel_all;
     out->gate_pass = e.gate_pass;
     out->count = e.count;
+    out->nonfinite = e.nonfinite;
     return OSTC_OK;
   });
 }

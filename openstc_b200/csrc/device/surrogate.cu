@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <limits>
 #include <algorithm>
 #include <random>
 #include <stdexcept>
@@ -747,6 +748,11 @@ double Surrogate::grad_host(const double *states, const double *dy, int64_t n, s
   return loss;
 }
 
+// Relative errors are taken over samples whose EPI increment reaches 1e-6 in
+// some species: below that the chemistry changes nothing the solver resolves,
+// and the gate bounds the network's increment by rel_max (Y_k + y_floor).
+constexpr double kRelFloor = 1e-6;
+
 SurrogateEval Surrogate::evaluate(int64_t begin, int64_t count) {
   if (begin < 0 || count <= 0 || begin + count > n_) throw std::runtime_error("evaluation range outside the data set");
   std::vector<double> st(count * kSurIn), lab(count * NS), pred(count * NS);
@@ -761,16 +767,30 @@ SurrogateEval Surrogate::evaluate(int64_t begin, int64_t count) {
   SurrogateEval e{};
   e.count = count;
   double rel_sum = 0;
-  int64_t rel_n = 0;
+  int64_t rel_n = 0, n_acc = 0;
+  std::vector<double> rel_all;
+  rel_all.reserve(static_cast<size_t>(count));
   for (int64_t i = 0; i < count; ++i) {
-    double nrm = 0, err = 0;
+    double nrm = 0, err = 0, abs_sum = 0;
+    bool finite = true;
     for (int k = 0; k < NS; ++k) {
+      const double d = pred[i * NS + k] - lab[i * NS + k];
+      finite = finite && std::isfinite(d);
       nrm = std::max(nrm, std::fabs(lab[i * NS + k]));
-      err = std::max(err, std::fabs(pred[i * NS + k] - lab[i * NS + k]));
-      e.mean_abs += std::fabs(pred[i * NS + k] - lab[i * NS + k]) / (count * NS);
+      err = std::max(err, std::fabs(d));
+      abs_sum += std::fabs(d);
     }
-    if (nrm > 1e-8) {
-      const double r = err / nrm;
+    if (!finite) {
+      ++e.nonfinite;
+      if (nrm > kRelFloor) rel_all.push_back(std::numeric_limits<double>::infinity());
+      continue;
+    }
+    const double r = nrm > kRelFloor ? err / nrm : -1;
+    if (r >= 0) rel_all.push_back(r);
+    if (!acc[i]) continue;
+    ++n_acc;
+    e.mean_abs += abs_sum / NS;
+    if (r >= 0) {
       rel_sum += r;
       ++rel_n;
       e.max_rel = std::max(e.max_rel, r);
@@ -786,10 +806,23 @@ SurrogateEval Surrogate::evaluate(int64_t begin, int64_t count) {
       if (total > 0) dmax = std::max(dmax, std::fabs(defect) / total);
     }
     e.max_defect = std::max(e.max_defect, dmax);
-    e.mean_defect += dmax / count;
-    e.gate_pass += acc[i] / static_cast<double>(count);
+    e.mean_defect += dmax;
   }
+  e.gate_pass = static_cast<double>(n_acc) / static_cast<double>(count);
   e.mean_rel = rel_n ? rel_sum / rel_n : 0;
+  if (n_acc) {
+    e.mean_abs /= n_acc;
+    e.mean_defect /= n_acc;
+  }
+  if (!rel_all.empty()) {
+    auto at = [&](double q) {
+      const size_t k = static_cast<size_t>(q * (rel_all.size() - 1));
+      std::nth_element(rel_all.begin(), rel_all.begin() + k, rel_all.end());
+      return rel_all[k];
+    };
+    e.median_rel_all = at(0.5);
+    e.p90_rel_all = at(0.9);
+  }
   return e;
 }
 

@@ -51,9 +51,16 @@ struct SurrogateDev {
   SurrogateGate gate;
 };
 
+// Held-out statistics against the FP64 EPI labels.  rel = max_k |dY_k -
+// dY_EPI,k| / max_k |dY_EPI,k| per sample (samples with max_k |dY_EPI,k| >=
+// 1e-6); the defect is that of the prediction the solver would apply (after
+// the element projection), relative to the element totals.
 struct SurrogateEval {
-  double mean_rel, max_rel, mean_abs, max_defect, mean_defect, gate_pass;
-  int64_t count;
+  double mean_rel, max_rel, mean_abs;  // the samples the trust gate accepts
+  double max_defect, mean_defect;      // accepted samples
+  double median_rel_all, p90_rel_all;  // every sample
+  double gate_pass;                    // fraction accepted
+  int64_t count, nonfinite;            // samples; predictions that were not finite
 };
 
 class Surrogate {
