@@ -256,9 +256,11 @@ int ostc_surrogate_load(ostc_surrogate *s, const char *path);
    the coupled DPLUR step -- the fallback.  s = NULL returns to EPI everywhere.
    The surrogate must stay alive while set; its weights are read at each step. */
 int ostc_driver_set_surrogate(ostc_driver *d, ostc_surrogate *s);
-/* Cell evaluations accepted by the trust gate and sent to the point-implicit
-   fallback since the surrogate was set. */
-int ostc_driver_chemistry_stats(ostc_driver *d, long long *accepted, long long *fallback);
+/* Since the surrogate was set: cell-steps whose chemistry the trust gate
+   accepted, cell-steps that took the point-implicit fallback, and cell
+   evaluations of the network (a rejected cell is evaluated again within a few
+   steps, in between it keeps EPI; evaluated may be NULL). */
+int ostc_driver_chemistry_stats(ostc_driver *d, long long *accepted, long long *fallback, long long *evaluated);
 
 /* No counterpart in the reference.  Recomputes, from the device state, the
    normalised residuals of rho, |V|, p, T of the last step that stored its

@@ -146,7 +146,8 @@ def library() -> C.CDLL:
         "ostc_driver_set_surrogate": ([P, P], C.c_int),
         "ostc_surrogate_get_gate": ([P, C.POINTER(SurrogateGate)], C.c_int),
         "ostc_surrogate_set_gate": ([P, C.POINTER(SurrogateGate)], C.c_int),
-        "ostc_driver_chemistry_stats": ([P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], C.c_int),
+        "ostc_driver_chemistry_stats": ([P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                                         C.POINTER(C.c_longlong)], C.c_int),
         "ostc_driver_run_phase": ([P, C.c_int], C.c_int),
         "ostc_driver_get_field": ([P, C.c_int, C.c_int, D, I64], C.c_int),
         "ostc_driver_set_field": ([P, C.c_int, C.c_int, D, I64], C.c_int),
@@ -285,10 +286,16 @@ class Driver:
         _check(library().ostc_driver_set_surrogate(self._h, sur._h if sur is not None else None))
 
     def chemistry_stats(self) -> tuple[int, int]:
-        """(cells accepted by the trust gate, cells sent to the EPI fallback)."""
-        a, f = C.c_longlong(), C.c_longlong()
-        _check(library().ostc_driver_chemistry_stats(self._h, C.byref(a), C.byref(f)))
+        """(cell-steps accepted by the trust gate, cell-steps sent to the EPI fallback)."""
+        a, f, e = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        _check(library().ostc_driver_chemistry_stats(self._h, C.byref(a), C.byref(f), C.byref(e)))
         return a.value, f.value
+
+    def surrogate_evaluations(self) -> int:
+        """Cell evaluations of the network since the surrogate was set."""
+        a, f, e = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        _check(library().ostc_driver_chemistry_stats(self._h, C.byref(a), C.byref(f), C.byref(e)))
+        return e.value
 
     def residual_noalloc(self) -> np.ndarray:
         """The residual of the last stored step recomputed on the device in

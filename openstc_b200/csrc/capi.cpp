@@ -528,14 +528,15 @@ int ostc_driver_set_surrogate(ostc_driver *d, ostc_surrogate *s) {
   });
 }
 
-int ostc_driver_chemistry_stats(ostc_driver *d, long long *accepted, long long *fallback) {
+int ostc_driver_chemistry_stats(ostc_driver *d, long long *accepted, long long *fallback, long long *evaluated) {
   if (!d || !accepted || !fallback) return fail(OSTC_ERR_INPUT, "null argument");
   if (!d->drv.initialized()) return fail(OSTC_ERR_STATE, "initialize first");
   return guarded([&] {
-    unsigned long long st[2];
+    unsigned long long st[3];
     d->drv.engine().surrogate_stats(st);
     *accepted = static_cast<long long>(st[0]);
     *fallback = static_cast<long long>(st[1]);
+    if (evaluated) *evaluated = static_cast<long long>(st[2]);
     return OSTC_OK;
   });
 }

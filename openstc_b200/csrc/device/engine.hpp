@@ -83,7 +83,8 @@ class Engine {
   virtual void set_surrogate(const SurrogateDev *p) = 0;
   // cells accepted by the trust gate and cells sent to the EPI fallback
   // since the surrogate was set
-  virtual void surrogate_stats(unsigned long long out[2]) = 0;
+  // accepted, sent to the EPI fallback, evaluated by the network
+  virtual void surrogate_stats(unsigned long long out[3]) = 0;
 };
 
 // Largest grid ostc_driver_residual_noalloc accepts, in residual tiles

@@ -100,6 +100,7 @@ class EngineT final : public Engine {
     cudaFree(d_fb_list_);
     cudaFree(d_sur_stats_);
     cudaFree(d_sur_err_);
+    cudaFree(d_sur_phase_);
     for (void *p : allocations_) cudaFree(p);
     cudaFree(d_blocks_);
     cudaFree(d_bcs_);
@@ -261,6 +262,7 @@ class EngineT final : public Engine {
     n += 1;  // properties
     if (store_last) n += 1;
     if (residual) n += 2;
+    if (sur_on_) n += 2 * static_cast<int>(blocks_.size());  // candidates + inference per block
     return n;
   }
 
@@ -455,10 +457,17 @@ class EngineT final : public Engine {
       for (int b = 0; b < static_cast<int>(blocks_.size()); ++b) {
         const DevBlock &B = blocks_[b];
         const int64_t cells = static_cast<int64_t>(B.mx) * B.my * B.mz;
+        // the cells to evaluate (quiet last step, plus a rotating 1/kRecheckEvery)
+        cuda_check(cudaMemsetAsync(d_fb_count_, 0, sizeof(int), stream_), "memset candidates");
+        const unsigned cgrid = static_cast<unsigned>(std::min<int64_t>((cells + 255) / 256, 8 * num_sms_));
+        sur::k_sur_candidates<C><<<cgrid, 256, 0, stream_>>>(d_blocks_, b, sur::kRecheckEvery, d_sur_phase_,
+                                                             d_fb_list_, d_fb_count_, d_sur_stats_);
         auto *fn = sur_.n_elem <= 3 ? sur::k_sur_infer<C, 1, 3> : sur::k_sur_infer<C, 1, 4>;
         const int64_t tiles = (cells + sur::kCells - 1) / sur::kCells;
+        const bool last = b + 1 == static_cast<int>(blocks_.size());
         fn<<<static_cast<unsigned>(std::min<int64_t>(tiles, num_sms_)), sur::kThreads, sur::kSmem, stream_>>>(
-            d_blocks_, b, sur_, d_fb_count_, d_fb_list_, d_sur_stats_, d_sur_err_);
+            d_blocks_, b, sur_, d_fb_count_, d_fb_list_, d_sur_stats_, d_sur_err_, d_fb_list_, d_fb_count_,
+            last ? d_sur_phase_ : nullptr);
         mark("surrogate");
       }
     }
@@ -512,9 +521,11 @@ class EngineT final : public Engine {
         for (const auto &B : blocks_) most = std::max<int64_t>(most, static_cast<int64_t>(B.mx) * B.my * B.mz);
         cuda_check(cudaMalloc(&d_fb_count_, sizeof(int)), "cudaMalloc fallback count");
         cuda_check(cudaMalloc(&d_fb_list_, sizeof(int) * most), "cudaMalloc fallback list");
-        cuda_check(cudaMalloc(&d_sur_stats_, 2 * sizeof(unsigned long long)), "cudaMalloc surrogate stats");
+        cuda_check(cudaMalloc(&d_sur_stats_, 3 * sizeof(unsigned long long)), "cudaMalloc surrogate stats");
         cuda_check(cudaMalloc(&d_sur_err_, sizeof(int)), "cudaMalloc surrogate err");
         cuda_check(cudaMemset(d_sur_err_, 0, sizeof(int)), "memset surrogate err");
+        cuda_check(cudaMalloc(&d_sur_phase_, sizeof(int)), "cudaMalloc surrogate phase");
+        cuda_check(cudaMemset(d_sur_phase_, 0, sizeof(int)), "memset surrogate phase");
         for (auto *fn : {sur::k_sur_infer<C, 0, 3>, sur::k_sur_infer<C, 1, 3>, sur::k_sur_infer<C, 0, 4>,
                          sur::k_sur_infer<C, 1, 4>})
           cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sur::kSmem)),
@@ -526,7 +537,7 @@ class EngineT final : public Engine {
           cuda_check(cudaFuncSetAttribute(sur::k_sur_fallback<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, fb_smem),
                      "fallback smem");
       }
-      if (sur_on_) cuda_check(cudaMemset(d_sur_stats_, 0, 2 * sizeof(unsigned long long)), "memset stats");
+      if (sur_on_) cuda_check(cudaMemset(d_sur_stats_, 0, 3 * sizeof(unsigned long long)), "memset stats");
       for (auto &B : blocks_) {
         if (sur_on_ && !B.chem_quiet) {
           void *q = nullptr;
@@ -556,10 +567,10 @@ class EngineT final : public Engine {
     upload_params();
   }
 
-  void surrogate_stats(unsigned long long out[2]) override {
-    out[0] = out[1] = 0;
+  void surrogate_stats(unsigned long long out[3]) override {
+    out[0] = out[1] = out[2] = 0;
     if (!d_sur_stats_) return;
-    cuda_check(cudaMemcpy(out, d_sur_stats_, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost), "stats");
+    cuda_check(cudaMemcpy(out, d_sur_stats_, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost), "stats");
     int err = 0;
     cuda_check(cudaMemcpy(&err, d_sur_err_, sizeof(int), cudaMemcpyDeviceToHost), "surrogate err");
     if (err) throw std::runtime_error("CUDA error in the surrogate kernel: a tensor-core wait timed out");
@@ -576,7 +587,7 @@ class EngineT final : public Engine {
         auto *fn = sur_.n_elem <= 3 ? sur::k_sur_infer<C, 0, 3> : sur::k_sur_infer<C, 0, 4>;
         const int64_t tiles = (cells + sur::kCells - 1) / sur::kCells;
         fn<<<static_cast<unsigned>(std::min<int64_t>(tiles, num_sms_)), sur::kThreads, sur::kSmem, stream_>>>(
-            d_blocks_, b, sur_, d_fb_count_, d_fb_list_, d_sur_stats_, d_sur_err_);
+            d_blocks_, b, sur_, d_fb_count_, d_fb_list_, d_sur_stats_, d_sur_err_, nullptr, nullptr, nullptr);
         mark("surrogate");
         sur::k_sur_fallback<C><<<148 * 4, 128, fb_smem, stream_>>>(d_blocks_, b, d_fb_count_, d_fb_list_);
         mark("epi_fallback");
@@ -681,7 +692,7 @@ class EngineT final : public Engine {
   bool sur_on_ = false;
   SurrogateDev sur_{};
   int num_sms_ = 148;
-  int *d_fb_count_ = nullptr, *d_fb_list_ = nullptr, *d_sur_err_ = nullptr;
+  int *d_fb_count_ = nullptr, *d_fb_list_ = nullptr, *d_sur_err_ = nullptr, *d_sur_phase_ = nullptr;
   unsigned long long *d_sur_stats_ = nullptr;
   std::vector<void *> sur_arrays_;
   std::vector<unsigned char *> quiet_store_;

@@ -158,6 +158,7 @@ constexpr int kThreads = 32 * 22;
 constexpr int kStageChunks = 4;  // weight chunks per ring stage
 constexpr int kStages = 4;       // ring stages
 constexpr int kFusedElem = 4;  // largest element count of the fused kernel's conservation gate
+constexpr int kRecheckEvery = 4;  // a cell the gate rejected is evaluated again within this many steps
 // Every weight chunk is 8 KB: one K=16 slice [256 x 16] of a hidden layer,
 // the whole first layer [256 x 16] or the whole output layer [16 x 256],
 // all packed K-major canonical with 16-column tiles.
@@ -252,14 +253,13 @@ __device__ __forceinline__ uint32_t gelu2_bf16(float x0, float x1) {
   return r;
 }
 
-// Features of the cell in row `row` of the tile starting at cell0 -> bf16
-// row of the first layer's input (zeros past the last cell).
+// Features of cell c -> bf16 row `row` of the first layer's input (zeros
+// for c past the last cell).
 template <class C>
-__device__ __forceinline__ void tile_features(const DevBlock &B, const SurrogateDev &P, int64_t cell0, int row,
+__device__ __forceinline__ void tile_features(const DevBlock &B, const SurrogateDev &P, int64_t c, int row,
                                               uint8_t *x0) {
   constexpr int NS = C::ns;
   const int64_t cells = static_cast<int64_t>(B.mx) * B.my * B.mz, sz = B.G.size;
-  const int64_t c = cell0 + row;
   float f[kSurInPad];
 #pragma unroll
   for (int q = 0; q < kSurInPad; ++q) f[q] = 0.f;
@@ -349,12 +349,16 @@ __device__ __forceinline__ void tile_apply(const DevBlock &B, const SurrogateDev
 // are marked chemically quiet and get the rate rho dY / dt, the others keep
 // the point-implicit chemistry.  MODE 0 (a split step): accepted increments
 // go into cv (rho Y_k) with the primitives recomputed, rejected cells are
-// listed for the EPI fallback.  stats[0] += accepted, stats[1] += rejected.
-// NE (3 or 4) bounds the element count of the conservation gate.
+// listed for the EPI fallback.  stats[0] += accepted, stats[1] += rejected,
+// stats[2] += cells evaluated.
+// NE (3 or 4) bounds the element count of the conservation gate.  With a
+// candidate list (cand, *cand_count; k_sur_candidates) only the listed cells
+// are evaluated, and the CTA of block index 0 advances *phase_ctr at the end.
 template <class C, int MODE, int NE>
 __global__ void __launch_bounds__(kThreads, 1) k_sur_infer(const DevBlock *__restrict__ blks, int b, SurrogateDev P,
                                                            int *fb_count, int *fb_list, unsigned long long *stats,
-                                                           int *err) {
+                                                           int *err, const int *__restrict__ cand,
+                                                           const int *cand_count, int *phase_ctr) {
   extern __shared__ __align__(128) uint8_t smem[];
   uint8_t *act = smem;                     // 64 KB
   uint8_t *x0 = smem + kActBytes;          // 2 x 4 KB, by tile
@@ -365,12 +369,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_sur_infer(const DevBlock *__res
   uint64_t *full = bars, *empty = full + kStages, *feat_full = empty + kStages, *x0_free = feat_full + 2,
            *mma_epi = x0_free + 2, *mma_out = mma_epi + 2, *acc_free = mma_out + 1, *act_ready = acc_free + 2,
            *drain = act_ready + 2, *res_full = drain + 1;
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(drain + 1);
+  static_assert(kBars == 2 * kStages + 2 + 2 + 2 + 1 + 2 + 2 + 1 + 1, "one slot per barrier");
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(res_full + 1);
   volatile int *abort = reinterpret_cast<volatile int *>(tslot + 1);
   const DevBlock &B = blks[b];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t cells = static_cast<int64_t>(B.mx) * B.my * B.mz;
-  const int64_t ntiles = (cells + kCells - 1) / kCells;
+  const int64_t n_items = cand ? static_cast<int64_t>(*cand_count) : cells;
+  // the cell of item idx (past the end: an invalid cell)
+  auto cell_of = [&](int64_t idx) -> int64_t { return cand ? (idx < n_items ? cand[idx] : cells) : idx; };
+  const int64_t ntiles = (n_items + kCells - 1) / kCells;
   // this CTA's tiles: blockIdx.x, blockIdx.x + gridDim.x, ...
   const int my_tiles =
       blockIdx.x < ntiles ? static_cast<int>((ntiles - 1 - blockIdx.x) / gridDim.x + 1) : 0;
@@ -524,7 +532,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sur_infer(const DevBlock *__res
     const int quarter = warp & 3, row = quarter * 32 + lane;
     bool ok = true;
     if (my_tiles > 0) {
-      tile_features<C>(B, P, static_cast<int64_t>(blockIdx.x) * kCells, row, x0);
+      tile_features<C>(B, P, cell_of(static_cast<int64_t>(blockIdx.x) * kCells + row), row, x0);
       tc::fence_async_smem();
       __syncwarp();
       if (lane == 0) bar_arrive(&feat_full[0]);
@@ -535,7 +543,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_sur_infer(const DevBlock *__res
         const int nb = (it + 1) & 1;
         if (it + 1 >= 2) ok = __all_sync(0xffffffffu, wait_bar(&x0_free[nb], (((it + 1) >> 1) - 1) & 1, abort));
         if (!ok) break;
-        tile_features<C>(B, P, (tile + gridDim.x) * kCells, row, x0 + nb * kX0Bytes);
+        tile_features<C>(B, P, cell_of((tile + gridDim.x) * kCells + row), row, x0 + nb * kX0Bytes);
         tc::fence_async_smem();
         __syncwarp();
         if (lane == 0) bar_arrive(&feat_full[nb]);
@@ -549,13 +557,54 @@ __global__ void __launch_bounds__(kThreads, 1) k_sur_infer(const DevBlock *__res
       tc::fence_before_sync();
       __syncwarp();
       if (lane == 0) bar_arrive(&acc_free[p], kEpiWarps / 4);  // four warps stand for the epilogue warps
-      tile_apply<C, MODE, NE>(B, P, tile * kCells + row, o, sbias + 4 * kSurHidden, fb_count, fb_list, stats);
+      tile_apply<C, MODE, NE>(B, P, cell_of(tile * kCells + row), o, sbias + 4 * kSurHidden, fb_count, fb_list,
+                              stats);
     }
   }
   tc::fence_before_sync();
   __syncthreads();
   if (warp == 0) tc::tmem_dealloc(tmem, 512);
   if (tid == 0 && *abort) atomicExch(err, 1);
+  if (tid == 0 && blockIdx.x == 0) {
+    if (phase_ctr) atomicAdd(phase_ctr, 1);
+    atomicAdd(&stats[2], static_cast<unsigned long long>(n_items));
+  }
+}
+
+// Cells the inference evaluates this step: those it judged quiet the step
+// before, and every cell whose linear index is the step's phase modulo
+// `every` (a reacting cell is looked at again within `every` steps; in
+// between it keeps the point-implicit chemistry, so no decision goes stale).
+// Clears chem_quiet; the cells left out count as EPI fallbacks in stats[1].
+template <class C>
+__global__ void __launch_bounds__(256) k_sur_candidates(const DevBlock *__restrict__ blks, int b, int every,
+                                                        const int *phase_ctr, int *list, int *count,
+                                                        unsigned long long *stats) {
+  const DevBlock &B = blks[b];
+  const int64_t cells = static_cast<int64_t>(B.mx) * B.my * B.mz;
+  const int phase = *phase_ctr % every;
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x; base < cells; base += stride) {
+    const int64_t c = base + threadIdx.x;
+    bool pick = false, valid = c < cells;
+    if (valid) {
+      const int i = static_cast<int>(c % B.mx), j = static_cast<int>((c / B.mx) % B.my),
+                k = static_cast<int>(c / (static_cast<int64_t>(B.mx) * B.my));
+      const int64_t nz = B.Z.at(i, j, k);
+      pick = B.chem_quiet[nz] != 0 || c % every == phase;
+      B.chem_quiet[nz] = 0;
+    }
+    // one atomic per warp for the list and one for the left-out cells
+    const unsigned m = __ballot_sync(0xffffffffu, pick), skip = __ballot_sync(0xffffffffu, valid && !pick);
+    int at = 0;
+    if (lane == 0) {
+      if (m) at = atomicAdd(count, __popc(m));
+      if (skip) atomicAdd(&stats[1], static_cast<unsigned long long>(__popc(skip)));
+    }
+    at = __shfl_sync(0xffffffffu, at, 0);
+    if (pick) list[at + __popc(m & ((1u << lane) - 1u))] = static_cast<int>(c);
+  }
 }
 
 // EPI fallback for the listed cells of block b (grid-stride over the list).
