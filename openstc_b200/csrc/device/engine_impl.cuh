@@ -41,7 +41,11 @@ class EngineT final : public Engine {
     }
     for (int b = 0; b < static_cast<int>(blocks_.size()); ++b) allocate(blocks_[b]);
     cuda_check(cudaMalloc(&d_blocks_, sizeof(DevBlock) * blocks_.size()), "cudaMalloc blocks");
-    cuda_check(cudaMemcpy(d_blocks_, blocks_.data(), sizeof(DevBlock) * blocks_.size(), cudaMemcpyHostToDevice),
+    // uploads go through the engine's own (non-blocking) stream: a copy on the
+    // legacy default stream from pageable memory may still be in flight when
+    // a kernel on this stream starts
+    cuda_check(cudaMemcpyAsync(d_blocks_, blocks_.data(), sizeof(DevBlock) * blocks_.size(), cudaMemcpyHostToDevice,
+                               stream_),
                "copy blocks");
     // boundary and inner faces
     std::vector<DevBc> bcs;
@@ -53,12 +57,15 @@ class EngineT final : public Engine {
     static_assert(sizeof(DevBc) == sizeof(HostBc), "DevBc / HostBc layouts differ");
     if (!bcs.empty()) {
       cuda_check(cudaMalloc(&d_bcs_, sizeof(DevBc) * bcs.size()), "cudaMalloc bcs");
-      cuda_check(cudaMemcpy(d_bcs_, bcs.data(), sizeof(DevBc) * bcs.size(), cudaMemcpyHostToDevice), "copy bcs");
+      cuda_check(cudaMemcpyAsync(d_bcs_, bcs.data(), sizeof(DevBc) * bcs.size(), cudaMemcpyHostToDevice, stream_),
+                 "copy bcs");
+      cuda_check(cudaStreamSynchronize(stream_), "copy bcs");
     }
     static_assert(sizeof(DevInner) == sizeof(HostInner), "DevInner / HostInner layouts differ");
     if (!s.inner.empty()) {
       cuda_check(cudaMalloc(&d_inner_, sizeof(DevInner) * s.inner.size()), "cudaMalloc inner");
-      cuda_check(cudaMemcpy(d_inner_, s.inner.data(), sizeof(DevInner) * s.inner.size(), cudaMemcpyHostToDevice),
+      cuda_check(cudaMemcpyAsync(d_inner_, s.inner.data(), sizeof(DevInner) * s.inner.size(), cudaMemcpyHostToDevice,
+                                 stream_),
                  "copy inner");
     }
     tiles0_ = make_tiles(0);
@@ -72,12 +79,17 @@ class EngineT final : public Engine {
     cuda_check(cudaMallocHost(&h_res_, sizeof(double) * 4), "cudaMallocHost res");
     if (!s.wall_points.empty()) {
       cuda_check(cudaMalloc(&d_wall_, sizeof(double) * s.wall_points.size()), "cudaMalloc wall");
-      cuda_check(cudaMemcpy(d_wall_, s.wall_points.data(), sizeof(double) * s.wall_points.size(),
-                            cudaMemcpyHostToDevice),
+      cuda_check(cudaMemcpyAsync(d_wall_, s.wall_points.data(), sizeof(double) * s.wall_points.size(),
+                                 cudaMemcpyHostToDevice, stream_),
                  "copy wall");
     }
     source_smem_ = C::mix == 2 ? 2 * std::max(1, s.params.nr) * kCta * sizeof(double) : 0;
     flux_smem_ = C::nv * kCta * (C::mixed ? sizeof(float) : sizeof(double));
+    col_smem_ = sizeof(double) * ColSmem<C::nv>::size;
+    if (col_smem_ > 48 * 1024)
+      cuda_check(cudaFuncSetAttribute(k_flux_col<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(col_smem_)),
+                 "column flux smem");
     if (source_smem_ > 48 * 1024) {
       if constexpr (C::mixed)
         cuda_check(cudaFuncSetAttribute(k_source_mx<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -90,6 +102,9 @@ class EngineT final : public Engine {
     }
     cuda_check(cudaEventCreate(&ev0_), "event");
     cuda_check(cudaEventCreate(&ev1_), "event");
+    // the cudaMemset / staged copies above ran on the legacy default stream,
+    // which the engine's non-blocking stream does not wait for
+    cuda_check(cudaDeviceSynchronize(), "engine setup");
   }
 
   ~EngineT() override {
@@ -277,10 +292,13 @@ class EngineT final : public Engine {
     // device; re-upload when another engine of this configuration ran last.
     const void *&owner = static_owner();
     if (owner != this) {
-      cuda_check(cudaMemcpyToSymbol(cP, &setup_.params, sizeof(DevParams)), "upload params");
+      cuda_check(cudaMemcpyToSymbolAsync(cP, &setup_.params, sizeof(DevParams), 0, cudaMemcpyHostToDevice, stream_),
+                 "upload params");
       if constexpr (C::mixed) {
         const MixParams f = make_mix_params(setup_.params);
-        cuda_check(cudaMemcpyToSymbol(cF, &f, sizeof(MixParams)), "upload float params");
+        cuda_check(cudaMemcpyToSymbolAsync(cF, &f, sizeof(MixParams), 0, cudaMemcpyHostToDevice, stream_),
+                   "upload float params");
+        cuda_check(cudaStreamSynchronize(stream_), "upload float params");
       }
       owner = this;
     }
@@ -441,7 +459,7 @@ class EngineT final : public Engine {
     if constexpr (C::mixed)
       k_flux_mx_col<C><<<grid(col_tiles_), kFluxThreads, 0, stream_>>>(d_blocks_, col_tiles_);
     else
-      k_flux<C><<<grid(tiles0_), block3(), flux_smem_, stream_>>>(d_blocks_, tiles0_);
+      k_flux_col<C><<<grid(col_tiles_), kFluxThreads, col_smem_, stream_>>>(d_blocks_, col_tiles_);
   }
 
   void launch_props() {
@@ -554,7 +572,8 @@ class EngineT final : public Engine {
         blocks_[b].chem_quiet = sur_on_ ? quiet_store_.at(b) : nullptr;
         blocks_[b].chem_rate = sur_on_ ? rate_store_.at(b) : nullptr;
       }
-      cuda_check(cudaMemcpy(d_blocks_, blocks_.data(), sizeof(DevBlock) * blocks_.size(), cudaMemcpyHostToDevice),
+      cuda_check(cudaMemcpyAsync(d_blocks_, blocks_.data(), sizeof(DevBlock) * blocks_.size(), cudaMemcpyHostToDevice,
+                                 stream_),
                  "copy blocks");
     }
     // the step graphs and the parameter block change
@@ -565,14 +584,18 @@ class EngineT final : public Engine {
       }
     static_owner() = nullptr;
     upload_params();
+    // the cudaMemset calls above ran on the legacy default stream
+    cuda_check(cudaDeviceSynchronize(), "surrogate setup");
   }
 
   void surrogate_stats(unsigned long long out[3]) override {
     out[0] = out[1] = out[2] = 0;
     if (!d_sur_stats_) return;
-    cuda_check(cudaMemcpy(out, d_sur_stats_, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost), "stats");
     int err = 0;
-    cuda_check(cudaMemcpy(&err, d_sur_err_, sizeof(int), cudaMemcpyDeviceToHost), "surrogate err");
+    cuda_check(cudaMemcpyAsync(out, d_sur_stats_, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_),
+               "stats");
+    cuda_check(cudaMemcpyAsync(&err, d_sur_err_, sizeof(int), cudaMemcpyDeviceToHost, stream_), "surrogate err");
+    cuda_check(cudaStreamSynchronize(stream_), "stats");
     if (err) throw std::runtime_error("CUDA error in the surrogate kernel: a tensor-core wait timed out");
   }
 
@@ -686,7 +709,7 @@ class EngineT final : public Engine {
   unsigned int *d_bad_ = nullptr;
   std::vector<void *> allocations_;
   Tiles tiles0_, tiles1_, tilesg_, col_tiles_;
-  size_t source_smem_ = 0, flux_smem_ = 0;
+  size_t source_smem_ = 0, flux_smem_ = 0, col_smem_ = 0;
   int final_dq_ = 0;
   cudaGraphExec_t graphs_[4] = {nullptr, nullptr, nullptr, nullptr};
   bool sur_on_ = false;

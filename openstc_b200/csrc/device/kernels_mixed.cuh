@@ -542,40 +542,10 @@ __global__ void __launch_bounds__(kCta, 4) k_flux_mx(const DevBlock *__restrict_
   local_time_step_mx<C>(B, i, j, k, n, nd);
 }
 
-// The same flux differences with every face evaluated once.  A CTA owns a
-// column of 32 x 4 cells (i, j) over kFluxKC planes of k and marches in k:
-// the four compute warps (warp = j offset, lane = i offset) evaluate the
-// plus faces of their cells in x, y and z; the fifth warp evaluates the
-// minus faces on the column's low i and low j sides; the low-k face of a
-// plane is the high-k face of the plane before, carried in shared memory.
-// Each face value is the one k_flux_mx computes for it, and the per-cell
-// sums run in the same order, so the result is bit-identical.
-constexpr int kFluxKC = 8;                  // k planes per column
-constexpr int kFluxThreads = kCta + 32;    // 4 compute warps + the minus-face warp
-
-__device__ __forceinline__ void col_tile(const Tiles &T, int &b, int &i0, int &j0, int &k0) {
-  int t = blockIdx.x;
-  b = 0;
-  while (b + 1 < T.nblk && t >= T.begin[b + 1]) ++b;
-  t -= T.begin[b];
-  const int tx = t % T.ntx[b];
-  t /= T.ntx[b];
-  const int ty = t % T.nty[b];
-  const int tz = t / T.nty[b];
-  i0 = tx * kTX;
-  j0 = ty * kTY;
-  k0 = tz * kFluxKC;
-}
-
-// Shared-memory plan of the column kernel (floats): x faces [NV][kTY][kTX+1]
-// (face i0 - 1/2 + f), y faces [NV][kTY+1][kTX] (face j0 - 1/2 + f), the
-// low-k faces carried between planes [2][NV][kCta] (inviscid, viscous) and
-// the high-k faces of the current plane [NV][kCta].
-template <int NV>
-struct ColSmem {
-  static constexpr int xs = 0, ys = xs + NV * kTY * (kTX + 1), zs = ys + NV * (kTY + 1) * kTX,
-                       zp = zs + 2 * NV * kCta, size = zp + NV * kCta;
-};
+// k_flux_mx_col (below): the same flux differences with every face evaluated
+// once, on the columns of k_flux_col (kernels_step.cuh).  Each face value is
+// the one k_flux_mx computes for it, and the per-cell sums run in the same
+// order, so the result is bit-identical.
 
 // One face type (VISC 0: inviscid, 1: viscous) of plane k of a column: every
 // face into shared memory (one inlined face evaluation, looped over the

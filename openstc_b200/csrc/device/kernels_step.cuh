@@ -95,6 +95,44 @@ __global__ void __launch_bounds__(kCta, 4) k_source(const DevBlock *__restrict__
 #define OSTC_SWEEP_MIN_BLOCKS 4
 #endif
 
+// local_time_step, src/TimeAdvanceFunc.cuh:21-71: the spectral radii the
+// DPLUR stages use and the cell's local time step.
+template <class C>
+__device__ __forceinline__ void local_time_step(const DevBlock &B, int i, int j, int k, int64_t n, int64_t nd) {
+  const int64_t szd = B.D.size;
+  const bool three_d = B.mz > 1;
+  const int64_t sz = B.G.size;
+  const double *m = B.metric;
+  const double m11 = ld(m + n), m12 = ld(m + sz + n), m13 = ld(m + 2 * sz + n);
+  const double m21 = ld(m + 3 * sz + n), m22 = ld(m + 4 * sz + n), m23 = ld(m + 5 * sz + n);
+  const double m31 = ld(m + 6 * sz + n), m32 = ld(m + 7 * sz + n), m33 = ld(m + 8 * sz + n);
+  const double grad_xi = sqrt(m11 * m11 + m12 * m12 + m13 * m13);
+  const double grad_eta = sqrt(m21 * m21 + m22 * m22 + m23 * m23);
+  const double grad_zeta = sqrt(m31 * m31 + m32 * m32 + m33 * m33);
+  const double u = ld(B.bv + sz + n), v = ld(B.bv + 2 * sz + n), w = ld(B.bv + 3 * sz + n);
+  const double U = u * m11 + v * m12 + w * m13;
+  const double V = u * m21 + v * m22 + w * m23;
+  const double W = u * m31 + v * m32 + w * m33;
+  const double a = ld(B.acoustic + n);
+  const double s0 = fabs(U) + a * grad_xi, s1 = fabs(V) + a * grad_eta;
+  double s2 = 0;
+  if (three_d) s2 = fabs(W) + a * grad_zeta;
+  B.inv_spec[nd] = s0;
+  B.inv_spec[szd + nd] = s1;
+  B.inv_spec[2 * szd + nd] = s2;
+  const double sri = s0 + s1 + s2;
+  double gamma = kDGammaAir;
+  if constexpr (C::mix != 0) gamma = ld(B.gamma + n);
+  const double coeff_1 = fmax(gamma, 4.0 / 3.0) / ld(B.bv + n);
+  double coeff_2 = ld(B.mul + n) / cP.Pr;
+  if constexpr (C::turb) coeff_2 += ld(B.mut + n) / cP.Prt;
+  double srv = grad_xi * grad_xi + grad_eta * grad_eta;
+  if (three_d) srv += grad_zeta * grad_zeta;
+  srv *= coeff_1 * coeff_2;
+  B.visc_spec[nd] = srv;
+  B.dt_local[B.Z.at(i, j, k)] = cP.cfl / (sri + srv);
+}
+
 // ---------------------------------------------------------------- fluxes
 // Inviscid (AUSM+/MUSCL) then viscous (central) flux differences in the
 // reference's accumulation order, plus local_time_step
@@ -146,38 +184,156 @@ __global__ void __launch_bounds__(kCta, OSTC_FLUX_MIN_BLOCKS) k_flux(const DevBl
     }
   }
   OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq[l * szd + nd] = dq[l];
+  local_time_step<C>(B, i, j, k, n, nd);
+}
 
-  // local time step
-  const int64_t sz = B.G.size;
-  const double *m = B.metric;
-  const double m11 = ld(m + n), m12 = ld(m + sz + n), m13 = ld(m + 2 * sz + n);
-  const double m21 = ld(m + 3 * sz + n), m22 = ld(m + 4 * sz + n), m23 = ld(m + 5 * sz + n);
-  const double m31 = ld(m + 6 * sz + n), m32 = ld(m + 7 * sz + n), m33 = ld(m + 8 * sz + n);
-  const double grad_xi = sqrt(m11 * m11 + m12 * m12 + m13 * m13);
-  const double grad_eta = sqrt(m21 * m21 + m22 * m22 + m23 * m23);
-  const double grad_zeta = sqrt(m31 * m31 + m32 * m32 + m33 * m33);
-  const double u = ld(B.bv + sz + n), v = ld(B.bv + 2 * sz + n), w = ld(B.bv + 3 * sz + n);
-  const double U = u * m11 + v * m12 + w * m13;
-  const double V = u * m21 + v * m22 + w * m23;
-  const double W = u * m31 + v * m32 + w * m33;
-  const double a = ld(B.acoustic + n);
-  const double s0 = fabs(U) + a * grad_xi, s1 = fabs(V) + a * grad_eta;
-  double s2 = 0;
-  if (three_d) s2 = fabs(W) + a * grad_zeta;
-  B.inv_spec[nd] = s0;
-  B.inv_spec[szd + nd] = s1;
-  B.inv_spec[2 * szd + nd] = s2;
-  const double sri = s0 + s1 + s2;
-  double gamma = kDGammaAir;
-  if constexpr (C::mix != 0) gamma = ld(B.gamma + n);
-  const double coeff_1 = fmax(gamma, 4.0 / 3.0) / ld(B.bv + n);
-  double coeff_2 = ld(B.mul + n) / cP.Pr;
-  if constexpr (C::turb) coeff_2 += ld(B.mut + n) / cP.Prt;
-  double srv = grad_xi * grad_xi + grad_eta * grad_eta;
-  if (three_d) srv += grad_zeta * grad_zeta;
-  srv *= coeff_1 * coeff_2;
-  B.visc_spec[nd] = srv;
-  B.dt_local[B.Z.at(i, j, k)] = cP.cfl / (sri + srv);
+// The same flux differences with every face evaluated once: a CTA owns a
+// column of 32 x 4 cells (i, j) over kFluxKC planes of k and marches in k;
+// the four compute warps evaluate the plus faces of their cells in x, y and
+// z, the fifth warp the column's low-i and low-j faces, and the low-k face of
+// a plane is the high-k face of the plane before (shared memory).  Each face
+// value is the one k_flux computes for it and the per-cell sums run in the
+// same order (dq -= f(+) - f(-) per direction, inviscid then viscous), so the
+// result is bit-identical.
+constexpr int kFluxKC = 8;                  // k planes per column
+constexpr int kFluxThreads = kCta + 32;     // 4 compute warps + the minus-face warp
+
+__device__ __forceinline__ void col_tile(const Tiles &T, int &b, int &i0, int &j0, int &k0) {
+  int t = blockIdx.x;
+  b = 0;
+  while (b + 1 < T.nblk && t >= T.begin[b + 1]) ++b;
+  t -= T.begin[b];
+  const int tx = t % T.ntx[b];
+  t /= T.ntx[b];
+  const int ty = t % T.nty[b];
+  const int tz = t / T.nty[b];
+  i0 = tx * kTX;
+  j0 = ty * kTY;
+  k0 = tz * kFluxKC;
+}
+
+// Shared-memory plan of a column kernel (elements): x faces [NV][kTY][kTX+1]
+// (face i0 - 1/2 + f), y faces [NV][kTY+1][kTX] (face j0 - 1/2 + f), the
+// low-k faces carried between planes [2][NV][kCta] (inviscid, viscous) and
+// the high-k faces of the current plane [NV][kCta].
+template <int NV>
+struct ColSmem {
+  static constexpr int xs = 0, ys = xs + NV * kTY * (kTX + 1), zs = ys + NV * (kTY + 1) * kTX,
+                       zp = zs + 2 * NV * kCta, size = zp + NV * kCta;
+};
+
+// The faces of plane k of a column and the task that evaluates each: for a
+// compute thread 0 x-plus, 1 y-plus, 2 z-minus (first plane only), 3 z-plus;
+// for the minus-face warp 0 the low-i face of row lane, 1 the low-j face of
+// column lane.  Returns false when the thread has no face for the task.
+template <int NV>
+__device__ __forceinline__ bool col_task(const DevBlock &B, int i0, int j0, int k, bool first, bool cell, int q,
+                                         int zs_off, int64_t &nl, int &d, int64_t &s, int &off, int &stride) {
+  using S = ColSmem<NV>;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
+  const int i = i0 + lane, j = j0 + warp;
+  const int64_t sx = B.G.sx, sxy = B.G.sxy;
+  stride = kCta;
+  if (cell) {
+    const int64_t n = B.G.at(i, j, k);
+    const int task = (q >= 2 && !first) ? q + 1 : q;  // x, y, low z (first plane), high z
+    if (task == 0) {
+      nl = n; d = 0; s = 1; off = S::xs + warp * (kTX + 1) + lane + 1; stride = kTY * (kTX + 1);
+    } else if (task == 1) {
+      nl = n; d = 1; s = sx; off = S::ys + (warp + 1) * kTX + lane; stride = (kTY + 1) * kTX;
+    } else if (task == 2) {
+      nl = n - sxy; d = 2; s = sxy; off = zs_off + tid;
+    } else {
+      nl = n; d = 2; s = sxy; off = S::zp + tid;
+    }
+    return true;
+  }
+  if (q == 0) {
+    d = 0; s = 1; off = S::xs + lane * (kTX + 1); stride = kTY * (kTX + 1);
+    if (!(lane < kTY && j0 + lane < B.my && i0 < B.mx)) return false;
+    nl = B.G.at(i0, j0 + lane, k) - 1;
+    return true;
+  }
+  d = 1; s = sx; off = S::ys + lane; stride = (kTY + 1) * kTX;
+  if (!(i < B.mx && j0 < B.my)) return false;
+  nl = B.G.at(i, j0, k) - sx;
+  return true;
+}
+
+template <class C, int VISC>
+__device__ __forceinline__ void col_faces64(const DevBlock &B, int i0, int j0, int k, bool first, bool cell,
+                                            double *sm, double *dq) {
+  constexpr int NV = C::nv;
+  using S = ColSmem<NV>;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
+  const bool three_d = B.mz > 1;
+  const int zs_off = S::zs + VISC * NV * kCta;
+  const int ntask = cell ? (three_d ? (first ? 4 : 3) : 2) : (warp == kTY ? 2 : 0);
+#pragma unroll 1
+  for (int q = 0; q < ntask; ++q) {
+    int64_t nl = 0, s = 1;
+    int d = 0, off = 0, stride = kCta;
+    if (!col_task<NV>(B, i0, j0, k, first, cell, q, zs_off, nl, d, s, off, stride)) continue;
+    double t[NV];
+    if constexpr (VISC == 0)
+      inviscid_face<C>(B, nl, d, s, t);
+    else
+      viscous_face<C>(B, nl, d, s, t);
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) sm[off + l * stride] = t[l];
+  }
+  __syncthreads();
+  if (cell) {
+    const double *xs = sm + S::xs + warp * (kTX + 1) + lane, *ys = sm + S::ys + warp * kTX + lane;
+    double *zs = sm + zs_off;
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) {
+      const double px = xs[l * kTY * (kTX + 1) + 1], mx = xs[l * kTY * (kTX + 1)];
+      const double py = ys[l * (kTY + 1) * kTX + kTX], my = ys[l * (kTY + 1) * kTX];
+      if constexpr (VISC == 0) {
+        dq[l] -= px - mx;
+        dq[l] -= py - my;
+      } else {
+        dq[l] += px - mx;
+        dq[l] += py - my;
+      }
+      if (three_d) {
+        const double pz = sm[S::zp + l * kCta + tid], mz = zs[l * kCta + tid];
+        zs[l * kCta + tid] = pz;
+        if constexpr (VISC == 0)
+          dq[l] -= pz - mz;
+        else
+          dq[l] += pz - mz;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+template <class C>
+__global__ void __launch_bounds__(kFluxThreads, 2) k_flux_col(const DevBlock *__restrict__ blks, Tiles T) {
+  constexpr int NV = C::nv;
+  extern __shared__ double sm64[];
+  int b, i0, j0, k0;
+  col_tile(T, b, i0, j0, k0);
+  const DevBlock &B = blks[b];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = i0 + lane, j = j0 + warp;
+  const bool cell = warp < kTY && i < B.mx && j < B.my;
+  const int64_t szd = B.D.size;
+  const int k1 = min(k0 + kFluxKC, B.mz);
+  for (int k = k0; k < k1; ++k) {
+    double dq[NV];
+    int64_t n = 0, nd = 0;
+    if (cell) {
+      n = B.G.at(i, j, k);
+      nd = B.D.at(i, j, k);
+      OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] = B.dq[l * szd + nd];
+    }
+    col_faces64<C, 0>(B, i0, j0, k, k == k0, cell, sm64, dq);
+    if (cP.viscous_order != 0) col_faces64<C, 1>(B, i0, j0, k, k == k0, cell, sm64, dq);
+    if (!cell) continue;
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq[l * szd + nd] = dq[l];
+    local_time_step<C>(B, i, j, k, n, nd);
+  }
 }
 
 // ---------------------------------------------------------------- implicit

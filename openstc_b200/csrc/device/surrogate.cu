@@ -22,6 +22,15 @@
 
 namespace ostc {
 
+// Device-to-host copy ordered after the work on stream_ (a plain cudaMemcpy
+// runs on the legacy default stream, which does not wait for this
+// non-blocking stream).
+#define d2h(dst, src, bytes, what)                                                              \
+  do {                                                                                          \
+    ck(cudaMemcpyAsync((dst), (src), (bytes), cudaMemcpyDeviceToHost, stream_), what);          \
+    ck(cudaStreamSynchronize(stream_), what);                                                   \
+  } while (0)
+
 // ------------------------------------------------------------------ GEMM
 template <int BN>
 static cudaError_t launch_gemm_bn(const uint16_t *A, int lda, const uint16_t *B, int ldb, float *D, int ldd, int M,
@@ -348,7 +357,7 @@ Surrogate::Surrogate(const DevParams &chem, const std::vector<int> &elem_comp, i
     auto alloc = [&](size_t bytes) {
       void *p = nullptr;
       ck(cudaMalloc(&p, bytes), "cudaMalloc surrogate");
-      ck(cudaMemset(p, 0, bytes), "memset surrogate");
+      ck(cudaMemsetAsync(p, 0, bytes, stream_), "memset surrogate");
       allocs_.push_back(p);
       return p;
     };
@@ -361,15 +370,16 @@ Surrogate::Surrogate(const DevParams &chem, const std::vector<int> &elem_comp, i
     wb_[l] = static_cast<uint16_t *>(alloc(nw * 2));
     wbt_[l] = static_cast<uint16_t *>(alloc(nw * 2));
     wpack_[l] = static_cast<uint8_t *>(alloc(nw * 2));
-    ck(cudaMemcpy(w_[l], w.data(), nw * 4, cudaMemcpyHostToDevice), "upload weights");
-    ck(cudaMemcpy(b_[l], b.data(), dout_[l] * 4, cudaMemcpyHostToDevice), "upload bias");
+    ck(cudaMemcpyAsync(w_[l], w.data(), nw * 4, cudaMemcpyHostToDevice, stream_), "upload weights");
+    ck(cudaMemcpyAsync(b_[l], b.data(), dout_[l] * 4, cudaMemcpyHostToDevice, stream_), "upload bias");
+    ck(cudaStreamSynchronize(stream_), "upload weights");
   }
   void *p = nullptr;
   ck(cudaMalloc(&p, sizeof(double)), "loss");
   allocs_.push_back(p);
   loss_ = static_cast<double *>(p);
   ck(cudaMalloc(&p, sizeof(int)), "err");
-  ck(cudaMemset(p, 0, sizeof(int)), "err");
+  ck(cudaMemsetAsync(p, 0, sizeof(int), stream_), "err");
   allocs_.push_back(p);
   err_ = static_cast<int *>(p);
   for (int q = 0; q < kSurIn; ++q) {
@@ -391,7 +401,11 @@ Surrogate::~Surrogate() {
   cudaStreamDestroy(stream_);
 }
 
-void Surrogate::upload_chem() { ck(cudaMemcpyToSymbol(cP, &chem_, sizeof(DevParams)), "upload mechanism"); }
+// Stream-ordered: a copy on the legacy default stream from pageable memory
+// may still be in flight when a kernel on this non-blocking stream starts.
+void Surrogate::upload_chem() {
+  ck(cudaMemcpyToSymbolAsync(cP, &chem_, sizeof(DevParams), 0, cudaMemcpyHostToDevice, stream_), "upload mechanism");
+}
 
 void Surrogate::pack() {
   for (int l = 0; l < kSurLayers; ++l) {
@@ -449,8 +463,8 @@ void Surrogate::generate(int64_t n, uint64_t seed, const DevBlock *field, double
     // asinh(r_k / c_k), r_k = dY_k / (Y_k + eps)
     const int64_t m = std::min<int64_t>(n, 1 << 18);
     std::vector<double> lab(static_cast<size_t>(m) * NS), st(static_cast<size_t>(m) * kSurIn);
-    ck(cudaMemcpy(lab.data(), labels_, lab.size() * 8, cudaMemcpyDeviceToHost), "labels copy");
-    ck(cudaMemcpy(st.data(), states_, st.size() * 8, cudaMemcpyDeviceToHost), "states copy");
+    d2h(lab.data(), labels_, lab.size() * 8, "labels copy");
+    d2h(st.data(), states_, st.size() * 8, "states copy");
     for (int64_t i = 0; i < m; ++i)
       for (int q = 0; q < NS; ++q) lab[i * NS + q] /= st[i * kSurIn + 2 + q] + kSurYEps;
     // the trust region in dt follows the data (field samples carry the
@@ -596,7 +610,7 @@ double Surrogate::train(int steps, int batch, double lr, int64_t n_train, float 
     if (losses) losses[s] = static_cast<float>(loss_host);
   }
   int err = 0;
-  ck(cudaMemcpy(&err, err_, sizeof(int), cudaMemcpyDeviceToHost), "err copy");
+  d2h(&err, err_, sizeof(int), "err copy");
   if (err) throw std::runtime_error("tensor-core wait timed out during training");
   return last;
 }
@@ -605,8 +619,8 @@ std::vector<std::vector<float>> Surrogate::params() const {
   std::vector<std::vector<float>> out;
   for (int l = 0; l < kSurLayers; ++l) {
     std::vector<float> w(static_cast<size_t>(dout_[l]) * din_[l]), b(dout_[l]);
-    ck(cudaMemcpy(w.data(), w_[l], w.size() * 4, cudaMemcpyDeviceToHost), "params");
-    ck(cudaMemcpy(b.data(), b_[l], b.size() * 4, cudaMemcpyDeviceToHost), "params");
+    d2h(w.data(), w_[l], w.size() * 4, "params");
+    d2h(b.data(), b_[l], b.size() * 4, "params");
     out.push_back(std::move(w));
     out.push_back(std::move(b));
   }
@@ -618,8 +632,9 @@ void Surrogate::set_params(const std::vector<std::vector<float>> &p) {
   for (int l = 0; l < kSurLayers; ++l) {
     if (p[2 * l].size() != static_cast<size_t>(dout_[l]) * din_[l] || p[2 * l + 1].size() != static_cast<size_t>(dout_[l]))
       throw std::runtime_error("parameter shape mismatch");
-    ck(cudaMemcpy(w_[l], p[2 * l].data(), p[2 * l].size() * 4, cudaMemcpyHostToDevice), "set params");
-    ck(cudaMemcpy(b_[l], p[2 * l + 1].data(), p[2 * l + 1].size() * 4, cudaMemcpyHostToDevice), "set params");
+    ck(cudaMemcpyAsync(w_[l], p[2 * l].data(), p[2 * l].size() * 4, cudaMemcpyHostToDevice, stream_), "set params");
+    ck(cudaMemcpyAsync(b_[l], p[2 * l + 1].data(), p[2 * l + 1].size() * 4, cudaMemcpyHostToDevice, stream_),
+       "set params");
   }
   pack();
   ck(cudaStreamSynchronize(stream_), "set params");
@@ -681,7 +696,7 @@ void Surrogate::predict_host(const double *states, int64_t n, double *dy, int *a
   double *s = nullptr, *d = nullptr;
   int *acc = nullptr;
   ck(cudaMalloc(&s, static_cast<size_t>(batch) * kSurIn * 8), "predict alloc");
-  ck(cudaMemset(s, 0, static_cast<size_t>(batch) * kSurIn * 8), "predict memset");
+  ck(cudaMemsetAsync(s, 0, static_cast<size_t>(batch) * kSurIn * 8, stream_), "predict memset");
   ck(cudaMalloc(&d, n * NS * 8), "predict alloc");
   ck(cudaMalloc(&acc, n * sizeof(int)), "predict alloc");
   ck(cudaMemcpyAsync(s, states, n * kSurIn * 8, cudaMemcpyHostToDevice, stream_), "predict upload");
@@ -757,8 +772,8 @@ SurrogateEval Surrogate::evaluate(int64_t begin, int64_t count) {
   if (begin < 0 || count <= 0 || begin + count > n_) throw std::runtime_error("evaluation range outside the data set");
   std::vector<double> st(count * kSurIn), lab(count * NS), pred(count * NS);
   std::vector<int> acc(count);
-  ck(cudaMemcpy(st.data(), states_ + begin * kSurIn, st.size() * 8, cudaMemcpyDeviceToHost), "eval copy");
-  ck(cudaMemcpy(lab.data(), labels_ + begin * NS, lab.size() * 8, cudaMemcpyDeviceToHost), "eval copy");
+  d2h(st.data(), states_ + begin * kSurIn, st.size() * 8, "eval copy");
+  d2h(lab.data(), labels_ + begin * NS, lab.size() * 8, "eval copy");
   const int64_t chunk = 1 << 18;
   for (int64_t q = 0; q < count; q += chunk) {
     const int64_t m = std::min(chunk, count - q);
