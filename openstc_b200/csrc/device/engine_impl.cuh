@@ -86,19 +86,28 @@ class EngineT final : public Engine {
     source_smem_ = C::mix == 2 ? 2 * std::max(1, s.params.nr) * kCta * sizeof(double) : 0;
     flux_smem_ = C::nv * kCta * (C::mixed ? sizeof(float) : sizeof(double));
     col_smem_ = sizeof(double) * ColSmem<C::nv>::size;
+    dq0_smem_ = (C::mix == 2 && s.params.chem_src_method == 1) ? sizeof(double) * C::ns * C::ns * kCta : 0;
+    if (dq0_smem_ > 48 * 1024)
+      cuda_check(cudaFuncSetAttribute(k_dq0<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(dq0_smem_)),
+                 "dq0 smem");
     if (col_smem_ > 48 * 1024)
       cuda_check(cudaFuncSetAttribute(k_flux_col<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(col_smem_)),
                  "column flux smem");
     if (source_smem_ > 48 * 1024) {
-      if constexpr (C::mixed)
+      if constexpr (C::mixed) {
         cuda_check(cudaFuncSetAttribute(k_source_mx<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(source_smem_)),
                    "smem attribute");
-      else
+        cuda_check(cudaFuncSetAttribute(k_chem_list<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(source_smem_)),
+                   "smem attribute");
+      } else {
         cuda_check(cudaFuncSetAttribute(k_source<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(source_smem_)),
                    "smem attribute");
+      }
     }
     cuda_check(cudaEventCreate(&ev0_), "event");
     cuda_check(cudaEventCreate(&ev1_), "event");
@@ -277,7 +286,7 @@ class EngineT final : public Engine {
     n += 1;  // properties
     if (store_last) n += 1;
     if (residual) n += 2;
-    if (sur_on_) n += 2 * static_cast<int>(blocks_.size());  // candidates + inference per block
+    if (sur_on_) n += (C::mixed ? 4 : 2) * static_cast<int>(blocks_.size());  // candidates + inference (+ chemistry list)
     return n;
   }
 
@@ -449,10 +458,26 @@ class EngineT final : public Engine {
   static dim3 block3() { return dim3(kTX, kTY, kTZ); }
 
   void launch_source() {
-    if constexpr (C::mixed)
+    if constexpr (C::mixed) {
       k_source_mx<C><<<grid(tiles0_), block3(), source_smem_, stream_>>>(d_blocks_, tiles0_);
-    else
+      if constexpr (C::mix == 2) {
+        if (sur_on_) {
+          // the chemistry of the cells the surrogate did not take, compacted
+          // (the candidate list of this step's inference is no longer needed)
+          for (int b = 0; b < static_cast<int>(blocks_.size()); ++b) {
+            const DevBlock &B = blocks_[b];
+            const int64_t cells = static_cast<int64_t>(B.mx) * B.my * B.mz;
+            cuda_check(cudaMemsetAsync(d_fb_count_, 0, sizeof(int), stream_), "memset chemistry list");
+            const unsigned cgrid = static_cast<unsigned>(std::min<int64_t>((cells + 255) / 256, 8 * num_sms_));
+            k_chem_compact<C><<<cgrid, 256, 0, stream_>>>(d_blocks_, b, d_fb_list_, d_fb_count_);
+            const unsigned lgrid = static_cast<unsigned>((cells + kCta - 1) / kCta);
+            k_chem_list<C><<<lgrid, kCta, source_smem_, stream_>>>(d_blocks_, b, d_fb_list_, d_fb_count_);
+          }
+        }
+      }
+    } else {
       k_source<C><<<grid(tiles0_), block3(), source_smem_, stream_>>>(d_blocks_, tiles0_);
+    }
   }
 
   void launch_flux() {
@@ -503,7 +528,7 @@ class EngineT final : public Engine {
   int launch_implicit() {
     const auto &p = setup_.params;
     if (p.implicit_method == 1) {
-      k_dq0<C><<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_);
+      k_dq0<C><<<grid(tiles0_), block3(), dq0_smem_, stream_>>>(d_blocks_, tiles0_);
       mark("dq0");
       int in = 1;
       for (int s = 0; s < p.dplur_inner_step; ++s) {
@@ -709,7 +734,7 @@ class EngineT final : public Engine {
   unsigned int *d_bad_ = nullptr;
   std::vector<void *> allocations_;
   Tiles tiles0_, tiles1_, tilesg_, col_tiles_;
-  size_t source_smem_ = 0, flux_smem_ = 0, col_smem_ = 0;
+  size_t source_smem_ = 0, flux_smem_ = 0, col_smem_ = 0, dq0_smem_ = 0;
   int final_dq_ = 0;
   cudaGraphExec_t graphs_[4] = {nullptr, nullptr, nullptr, nullptr};
   bool sur_on_ = false;

@@ -389,8 +389,51 @@ __device__ __forceinline__ void sst_source(const DevBlock &B, int64_t n, double 
 
 }  // namespace fp32
 
+// Finite-rate chemistry of one cell in FP64 (the code of the FP64 path):
+// returns dq species = J omega and writes the EPI / DA Jacobian.  q1, q2:
+// this thread's column of the CTA's shared rate arrays (stride kCta).
+template <class C>
+__device__ __forceinline__ void chem_cell(const DevBlock &B, int64_t n, int64_t nz, double *q1, double *q2,
+                                          double *dq_spec) {
+  constexpr int NS = C::ns;
+  const int64_t sz = B.G.size, sz0 = B.Z.size;
+  double Y[NS], omega[NS], omega_d[NS];
+  OSTC_UNROLL for (int l = 0; l < NS; ++l) Y[l] = ld(B.sv + l * sz + n);
+  const double density = ld(B.bv + n), t = ld(B.bv + 5 * sz + n);
+  chemistry<NS>(density, t, Y, omega, omega_d, q1, q2, kCta);
+  const double jac = ld(B.jac + n);
+  OSTC_UNROLL for (int l = 0; l < NS; ++l) dq_spec[l] = jac * omega[l];
+  const int method = cP.chem_src_method;
+  if (method == 1) {
+    const int nr = cP.nr;
+    OSTC_UNROLL for (int m = 0; m < NS; ++m) {
+      OSTC_UNROLL for (int q = 0; q < NS; ++q) {
+        double zz = 0;
+        if (Y[q] > 1e-25) {
+          for (int r = 0; r < nr; ++r) {
+            const int dn = cP.sb[r * NS + m] - cP.sf[r * NS + m];
+            if (dn == 0) continue;
+            zz += dn * (cP.sf[r * NS + q] * q1[r * kCta] - cP.sb[r * NS + q] * q2[r * kCta]);
+          }
+          zz /= density * Y[q];
+        }
+        B.chem_jac[(m * NS + q) * sz0 + nz] = cP.mw[m] * zz * 1e+3;
+      }
+    }
+  } else if (method == 2) {
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) {
+      double v = 0;
+      if (Y[l] > 1e-25) v = -omega_d[l] / (Y[l] * density);
+      B.chem_jac[l * sz0 + nz] = v;
+    }
+  }
+}
+
 // dq = source terms: SST in FP32, finite-rate chemistry and its EPI Jacobian
-// in FP64 (the same code as the FP64 path).
+// in FP64 (the same code as the FP64 path).  With the surrogate on
+// (chem_quiet set) the chemistry of the cells it did not judge quiet runs in
+// k_chem_list over a compacted list instead, with every lane of a warp busy;
+// here those cells get zero species source, which k_chem_list overwrites.
 template <class C>
 __global__ void __launch_bounds__(kCta, 4) k_source_mx(const DevBlock *__restrict__ blks, Tiles T) {
   constexpr int NS = C::ns, NV = C::nv;
@@ -399,7 +442,7 @@ __global__ void __launch_bounds__(kCta, 4) k_source_mx(const DevBlock *__restric
   if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
   const DevBlock &B = blks[b];
   const int64_t n = B.G.at(i, j, k), nd = B.D.at(i, j, k), nz = B.Z.at(i, j, k);
-  const int64_t sz = B.G.size, szd = B.D.size, sz0 = B.Z.size;
+  const int64_t szd = B.D.size, sz0 = B.Z.size;
   double dq[NV];
   OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] = 0;
   if constexpr (C::turb) {
@@ -415,48 +458,63 @@ __global__ void __launch_bounds__(kCta, 4) k_source_mx(const DevBlock *__restric
     B.turb_cond[n] = static_cast<float>(mut) * fp32::ldf(B.cp + n) / cF.Prt;
   }
   if constexpr (C::mix == 2) {
-    if (B.chem_quiet && B.chem_quiet[nz]) {
-      // judged chemically quiet by the surrogate: its rate and no Jacobian
-      // (the implicit stages treat the cell's species diagonally and never
-      // read its chem_jac)
-      const double jac = ld(B.jac + n);
-      OSTC_UNROLL for (int l = 0; l < NS; ++l) dq[l + 5] = jac * B.chem_rate[l * sz0 + nz];
+    if (B.chem_quiet) {
+      if (B.chem_quiet[nz]) {
+        // judged chemically quiet by the surrogate: its rate and no Jacobian
+        // (the implicit stages treat the cell's species diagonally and never
+        // read its chem_jac)
+        const double jac = ld(B.jac + n);
+        OSTC_UNROLL for (int l = 0; l < NS; ++l) dq[l + 5] = jac * B.chem_rate[l * sz0 + nz];
+      }
     } else {
-    const int tid = threadIdx.x + kTX * (threadIdx.y + kTY * threadIdx.z);
-    double *q1 = sq + tid, *q2 = sq + cP.nr * kCta + tid;
-    double Y[NS], omega[NS], omega_d[NS];
-    OSTC_UNROLL for (int l = 0; l < NS; ++l) Y[l] = ld(B.sv + l * sz + n);
-    const double density = ld(B.bv + n), t = ld(B.bv + 5 * sz + n);
-    chemistry<NS>(density, t, Y, omega, omega_d, q1, q2, kCta);
-    const double jac = ld(B.jac + n);
-    OSTC_UNROLL for (int l = 0; l < NS; ++l) dq[l + 5] = jac * omega[l];
-    const int method = cP.chem_src_method;
-    if (method == 1) {
-      const int nr = cP.nr;
-      OSTC_UNROLL for (int m = 0; m < NS; ++m) {
-        OSTC_UNROLL for (int q = 0; q < NS; ++q) {
-          double zz = 0;
-          if (Y[q] > 1e-25) {
-            for (int r = 0; r < nr; ++r) {
-              const int dn = cP.sb[r * NS + m] - cP.sf[r * NS + m];
-              if (dn == 0) continue;
-              zz += dn * (cP.sf[r * NS + q] * q1[r * kCta] - cP.sb[r * NS + q] * q2[r * kCta]);
-            }
-            zz /= density * Y[q];
-          }
-          B.chem_jac[(m * NS + q) * sz0 + nz] = cP.mw[m] * zz * 1e+3;
-        }
-      }
-    } else if (method == 2) {
-      OSTC_UNROLL for (int l = 0; l < NS; ++l) {
-        double v = 0;
-        if (Y[l] > 1e-25) v = -omega_d[l] / (Y[l] * density);
-        B.chem_jac[l * sz0 + nz] = v;
-      }
-    }
+      const int tid = threadIdx.x + kTX * (threadIdx.y + kTY * threadIdx.z);
+      chem_cell<C>(B, n, nz, sq + tid, sq + cP.nr * kCta + tid, dq + 5);
     }
   }
   OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq[l * szd + nd] = dq[l];
+}
+
+// The cells of block b the surrogate did not judge quiet, listed (any order).
+template <class C>
+__global__ void __launch_bounds__(256) k_chem_compact(const DevBlock *__restrict__ blks, int b, int *list,
+                                                      int *count) {
+  const DevBlock &B = blks[b];
+  const int64_t cells = static_cast<int64_t>(B.mx) * B.my * B.mz;
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x; base < cells; base += stride) {
+    const int64_t c = base + threadIdx.x;
+    bool pick = false;
+    if (c < cells) {
+      const int i = static_cast<int>(c % B.mx), j = static_cast<int>((c / B.mx) % B.my),
+                k = static_cast<int>(c / (static_cast<int64_t>(B.mx) * B.my));
+      pick = B.chem_quiet[B.Z.at(i, j, k)] == 0;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, pick);
+    int at = 0;
+    if (lane == 0 && m) at = atomicAdd(count, __popc(m));
+    at = __shfl_sync(0xffffffffu, at, 0);
+    if (pick) list[at + __popc(m & ((1u << lane) - 1u))] = static_cast<int>(c);
+  }
+}
+
+// Chemistry of the listed cells (k_chem_compact), one thread per entry, full
+// warps; launched for the block's cell count, entries past the list return.
+template <class C>
+__global__ void __launch_bounds__(kCta, 4) k_chem_list(const DevBlock *__restrict__ blks, int b,
+                                                       const int *__restrict__ list, const int *count) {
+  constexpr int NS = C::ns;
+  extern __shared__ double sq[];
+  const int q = blockIdx.x * kCta + threadIdx.x;
+  if (q >= *count) return;
+  const DevBlock &B = blks[b];
+  const int64_t c = list[q];
+  const int i = static_cast<int>(c % B.mx), j = static_cast<int>((c / B.mx) % B.my),
+            k = static_cast<int>(c / (static_cast<int64_t>(B.mx) * B.my));
+  const int64_t n = B.G.at(i, j, k), nz = B.Z.at(i, j, k), nd = B.D.at(i, j, k), szd = B.D.size;
+  double dqs[NS];
+  chem_cell<C>(B, n, nz, sq + threadIdx.x, sq + cP.nr * kCta + threadIdx.x, dqs);
+  OSTC_UNROLL for (int l = 0; l < NS; ++l) B.dq[(5 + l) * szd + nd] = dqs[l];
 }
 
 // Local time step of cell (i, j, k) in FP32 (local_time_step,

@@ -341,14 +341,16 @@ __global__ void __launch_bounds__(kFluxThreads, 2) k_flux_col(const DevBlock *__
 // src/FiniteRateChem.cu:286-342.  Factor and permutation are stored so that
 // the DPLUR sweeps reuse them: the reference re-factors the identical matrix
 // in every sweep, which yields the same factor bit for bit.
-template <int NS>
+// Element (r, c) of the matrix sits at lhs[((r * NS + c) * ST) * ST]: ST = 1 for a
+// per-thread array, the CTA size for a per-thread slice of shared memory.
+template <int NS, int ST = 1>
 __device__ __forceinline__ void lu_factor(double *lhs, int *ipiv) {
   OSTC_UNROLL for (int n = 0; n < NS; ++n) {
     int ik = n;
     double amax = 0;  // |lhs[ik][n]|: entries of column n above row m are final
     OSTC_UNROLL for (int m = n; m < NS; ++m) {
-      OSTC_UNROLL for (int t = 0; t < n; ++t) lhs[m * NS + n] -= lhs[m * NS + t] * lhs[t * NS + n];
-      const double a = fabs(lhs[m * NS + n]);
+      OSTC_UNROLL for (int t = 0; t < n; ++t) lhs[(m * NS + n) * ST] -= lhs[(m * NS + t) * ST] * lhs[(t * NS + n) * ST];
+      const double a = fabs(lhs[(m * NS + n) * ST]);
       if (m == n) {
         amax = a;
       } else if (a > amax) {
@@ -360,22 +362,22 @@ __device__ __forceinline__ void lu_factor(double *lhs, int *ipiv) {
     if (ik != n) {
       OSTC_UNROLL for (int t = 0; t < NS; ++t) {
         // swap rows n and ik; ik is data dependent, so select row by row
-        double rowk = lhs[n * NS + t];
+        double rowk = lhs[(n * NS + t) * ST];
         double other = 0;
         OSTC_UNROLL for (int q = n + 1; q < NS; ++q)
-          if (q == ik) other = lhs[q * NS + t];
+          if (q == ik) other = lhs[(q * NS + t) * ST];
         OSTC_UNROLL for (int q = n + 1; q < NS; ++q)
-          if (q == ik) lhs[q * NS + t] = rowk;
-        lhs[n * NS + t] = other;
+          if (q == ik) lhs[(q * NS + t) * ST] = rowk;
+        lhs[(n * NS + t) * ST] = other;
       }
     }
     OSTC_UNROLL for (int p = n + 1; p < NS; ++p)
-      OSTC_UNROLL for (int t = 0; t < n; ++t) lhs[n * NS + p] -= lhs[n * NS + t] * lhs[t * NS + p];
-    OSTC_UNROLL for (int m = n + 1; m < NS; ++m) lhs[m * NS + n] /= lhs[n * NS + n];
+      OSTC_UNROLL for (int t = 0; t < n; ++t) lhs[(n * NS + p) * ST] -= lhs[(n * NS + t) * ST] * lhs[(t * NS + p) * ST];
+    OSTC_UNROLL for (int m = n + 1; m < NS; ++m) lhs[(m * NS + n) * ST] /= lhs[(n * NS + n) * ST];
   }
 }
 
-template <int NS>
+template <int NS, int ST = 1>
 __device__ __forceinline__ void lu_solve(const double *lhs, const int *ipiv, double *rhs) {
   OSTC_UNROLL for (int m = 0; m < NS; ++m) {
     const int t = ipiv[m];
@@ -389,11 +391,11 @@ __device__ __forceinline__ void lu_solve(const double *lhs, const int *ipiv, dou
     }
   }
   OSTC_UNROLL for (int m = 1; m < NS; ++m)
-    OSTC_UNROLL for (int t = 0; t < m; ++t) rhs[m] -= lhs[m * NS + t] * rhs[t];
-  rhs[NS - 1] /= lhs[NS * NS - 1];
+    OSTC_UNROLL for (int t = 0; t < m; ++t) rhs[m] -= lhs[(m * NS + t) * ST] * rhs[t];
+  rhs[NS - 1] /= lhs[(NS * NS - 1) * ST];
   OSTC_UNROLL for (int m = NS - 2; m >= 0; --m) {
-    OSTC_UNROLL for (int t = m + 1; t < NS; ++t) rhs[m] -= lhs[m * NS + t] * rhs[t];
-    rhs[m] /= lhs[m * NS + m];
+    OSTC_UNROLL for (int t = m + 1; t < NS; ++t) rhs[m] -= lhs[(m * NS + t) * ST] * rhs[t];
+    rhs[m] /= lhs[(m * NS + m) * ST];
   }
 }
 
@@ -465,16 +467,18 @@ __global__ void __launch_bounds__(kCta) k_dq0(const DevBlock *__restrict__ blks,
       // its solve divides by diag (bit for bit)
       OSTC_UNROLL for (int l = 0; l < NS; ++l) dq[5 + l] /= diag;
     } else if (method == 1) {
-      double lhs[NS * NS];
+      // the matrix lives in this thread's slice of shared memory (stride kCta)
+      extern __shared__ double sdq[];
+      double *lhs = sdq + threadIdx.x + kTX * (threadIdx.y + kTY * threadIdx.z);
       int piv[NS];
       OSTC_UNROLL for (int m = 0; m < NS; ++m)
         OSTC_UNROLL for (int q = 0; q < NS; ++q) {
           const double J = B.chem_jac[(m * NS + q) * sz0 + nz];
-          lhs[m * NS + q] = (m == q) ? diag - dt * J : -dt * J;
+          lhs[(m * NS + q) * kCta] = (m == q) ? diag - dt * J : -dt * J;
         }
-      lu_factor<NS>(lhs, piv);
-      lu_solve<NS>(lhs, piv, dq + 5);
-      OSTC_UNROLL for (int q = 0; q < NS * NS; ++q) B.chem_jac[q * sz0 + nz] = lhs[q];
+      lu_factor<NS, kCta>(lhs, piv);
+      lu_solve<NS, kCta>(lhs, piv, dq + 5);
+      OSTC_UNROLL for (int q = 0; q < NS * NS; ++q) B.chem_jac[q * sz0 + nz] = lhs[q * kCta];
       OSTC_UNROLL for (int q = 0; q < NS; ++q) B.lu_piv[q * sz0 + nz] = static_cast<unsigned char>(piv[q]);
     } else if (method == 2) {
       OSTC_UNROLL for (int l = 0; l < NS; ++l) dq[5 + l] /= diag - dt * B.chem_jac[l * sz0 + nz];
