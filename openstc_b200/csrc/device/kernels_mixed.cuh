@@ -682,7 +682,7 @@ __device__ __forceinline__ void col_faces(const DevBlock &B, int i0, int j0, int
 }
 
 template <class C>
-__global__ void __launch_bounds__(kFluxThreads, 3) k_flux_mx_col(const DevBlock *__restrict__ blks, Tiles T) {
+__global__ void __launch_bounds__(kFluxThreads, 4) k_flux_mx_col(const DevBlock *__restrict__ blks, Tiles T) {
   constexpr int NV = C::nv;
   __shared__ float sm[ColSmem<NV>::size];
   int b, i0, j0, k0;
