@@ -405,19 +405,22 @@ __device__ __forceinline__ void chem_cell(const DevBlock &B, int64_t n, int64_t 
   OSTC_UNROLL for (int l = 0; l < NS; ++l) dq_spec[l] = jac * omega[l];
   const int method = cP.chem_src_method;
   if (method == 1) {
+    // compute_chem_src_jacobian with the reaction loop outside the species
+    // loop: each row m visits only the reactions that change species m once,
+    // and every (m, q) entry still sums its terms in reaction order
     const int nr = cP.nr;
     OSTC_UNROLL for (int m = 0; m < NS; ++m) {
+      double zz[NS];
+      OSTC_UNROLL for (int q = 0; q < NS; ++q) zz[q] = 0;
+      for (int r = 0; r < nr; ++r) {
+        const int dn = cP.sb[r * NS + m] - cP.sf[r * NS + m];
+        if (dn == 0) continue;
+        const double a1 = q1[r * kCta], a2 = q2[r * kCta];
+        OSTC_UNROLL for (int q = 0; q < NS; ++q) zz[q] += dn * (cP.sf[r * NS + q] * a1 - cP.sb[r * NS + q] * a2);
+      }
       OSTC_UNROLL for (int q = 0; q < NS; ++q) {
-        double zz = 0;
-        if (Y[q] > 1e-25) {
-          for (int r = 0; r < nr; ++r) {
-            const int dn = cP.sb[r * NS + m] - cP.sf[r * NS + m];
-            if (dn == 0) continue;
-            zz += dn * (cP.sf[r * NS + q] * q1[r * kCta] - cP.sb[r * NS + q] * q2[r * kCta]);
-          }
-          zz /= density * Y[q];
-        }
-        B.chem_jac[(m * NS + q) * sz0 + nz] = cP.mw[m] * zz * 1e+3;
+        const double v = Y[q] > 1e-25 ? zz[q] / (density * Y[q]) : 0.0;
+        B.chem_jac[(m * NS + q) * sz0 + nz] = cP.mw[m] * v * 1e+3;
       }
     }
   } else if (method == 2) {

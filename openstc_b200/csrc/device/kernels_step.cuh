@@ -58,19 +58,23 @@ __global__ void __launch_bounds__(kCta, 4) k_source(const DevBlock *__restrict__
     const int method = cP.chem_src_method;
     if (method == 1) {
       // compute_chem_src_jacobian, src/FiniteRateChem.cu:173-194
+      // the reaction loop sits outside the species loop: each row m visits
+      // only the reactions that change species m (the others add an exact
+      // zero in the reference), and every (m, q) entry still sums its terms
+      // in reaction order, so the entries are the reference's bit for bit
       const int nr = cP.nr;
       OSTC_UNROLL for (int m = 0; m < NS; ++m) {
+        double zz[NS];
+        OSTC_UNROLL for (int q = 0; q < NS; ++q) zz[q] = 0;
+        for (int r = 0; r < nr; ++r) {
+          const int dn = cP.sb[r * NS + m] - cP.sf[r * NS + m];
+          if (dn == 0) continue;
+          const double a1 = q1[r * kCta], a2 = q2[r * kCta];
+          OSTC_UNROLL for (int q = 0; q < NS; ++q) zz[q] += dn * (cP.sf[r * NS + q] * a1 - cP.sb[r * NS + q] * a2);
+        }
         OSTC_UNROLL for (int q = 0; q < NS; ++q) {
-          double zz = 0;
-          if (Y[q] > 1e-25) {
-            for (int r = 0; r < nr; ++r) {
-              const int dn = cP.sb[r * NS + m] - cP.sf[r * NS + m];
-              if (dn == 0) continue;  // adds an exact zero in the reference
-              zz += dn * (cP.sf[r * NS + q] * q1[r * kCta] - cP.sb[r * NS + q] * q2[r * kCta]);
-            }
-            zz /= density * Y[q];
-          }
-          B.chem_jac[(m * NS + q) * sz0 + nz] = cP.mw[m] * zz * 1e+3;
+          const double v = Y[q] > 1e-25 ? zz[q] / (density * Y[q]) : 0.0;
+          B.chem_jac[(m * NS + q) * sz0 + nz] = cP.mw[m] * v * 1e+3;
         }
       }
     } else if (method == 2) {

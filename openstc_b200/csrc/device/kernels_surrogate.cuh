@@ -25,17 +25,19 @@ __device__ inline void epi_increment(double T, double rho, const double *Y, doub
   double lhs[NS * NS];
   const int nr = cP.nr;
   for (int m = 0; m < NS; ++m) {
+    // reactions outside the species loop (each (m, q) still sums in reaction
+    // order), as in k_source
+    double zz[NS];
+    for (int q = 0; q < NS; ++q) zz[q] = 0;
+    for (int r = 0; r < nr; ++r) {
+      const int dn = cP.sb[r * NS + m] - cP.sf[r * NS + m];
+      if (dn == 0) continue;
+      const double a1 = q1[r * stride], a2 = q2[r * stride];
+      for (int q = 0; q < NS; ++q) zz[q] += dn * (cP.sf[r * NS + q] * a1 - cP.sb[r * NS + q] * a2);
+    }
     for (int q = 0; q < NS; ++q) {
-      double zz = 0;
-      if (Y[q] > 1e-25) {
-        for (int r = 0; r < nr; ++r) {
-          const int dn = cP.sb[r * NS + m] - cP.sf[r * NS + m];
-          if (dn == 0) continue;
-          zz += dn * (cP.sf[r * NS + q] * q1[r * stride] - cP.sb[r * NS + q] * q2[r * stride]);
-        }
-        zz /= rho * Y[q];
-      }
-      const double J = cP.mw[m] * zz * 1e+3;
+      const double v = Y[q] > 1e-25 ? zz[q] / (rho * Y[q]) : 0.0;
+      const double J = cP.mw[m] * v * 1e+3;
       lhs[m * NS + q] = (m == q ? 1.0 : 0.0) - dt * J;
     }
   }
