@@ -41,6 +41,7 @@ struct DevParams {
   int label[kMaxReac], order[kMaxReac];
   signed char sf[kMaxReac * kMaxSpec], sb[kMaxReac * kMaxSpec];
   double A[kMaxReac], b[kMaxReac], Ea[kMaxReac], A2[kMaxReac], b2[kMaxReac], Ea2[kMaxReac];
+  double lnA[kMaxReac], lnA2[kMaxReac];  // ln |A|, ln |A2| (0 where A is 0): the FP32-bulk path's rates
   double tb[kMaxReac * kMaxSpec];
   double troe_a[kMaxReac], troe_t3[kMaxReac], troe_t1[kMaxReac], troe_t2[kMaxReac];
 };

@@ -160,11 +160,25 @@ __device__ __forceinline__ double arrhenius(double t, double A, double b, double
 #define OSTC_DUP_FMA 1
 #endif
 
+// The same rate as one exponential, sign(A) exp(ln|A| + b ln T - Ea / T), for
+// the FP32-bulk path (FP64 throughout, within a few ulps of arrhenius).
+__device__ __forceinline__ double arrhenius_exp(double A, double lnA, double b, double Ea, double ln_t, double t_inv) {
+  return A == 0 ? 0.0 : copysign(std::exp(lnA + b * ln_t - Ea * t_inv), A);
+}
+
 // finite_rate_chemistry, src/FiniteRateChem.cu:7-63 with the rate helpers
 // :65-171.  q1/q2 live in shared memory with stride `st` (CTA size).
-template <int NS>
+// FAST (the FP32-bulk path): every Arrhenius rate as one exponential
+// (arrhenius_exp) instead of a pow and an exponential; the FP64 path keeps the
+// reference's form bit for bit.
+template <int NS, bool FAST = false>
 __device__ __forceinline__ void chemistry(double density, double t, const double *Y, double *omega, double *omega_d,
                                          double *q1, double *q2, int st) {
+  const double ln_t = FAST ? std::log(t) : 0.0, t_inv = FAST ? 1.0 / t : 0.0;
+  auto rate1 = [&](int r) { return FAST ? arrhenius_exp(cP.A[r], cP.lnA[r], cP.b[r], cP.Ea[r], ln_t, t_inv)
+                                        : arrhenius(t, cP.A[r], cP.b[r], cP.Ea[r]); };
+  auto rate2 = [&](int r) { return FAST ? arrhenius_exp(cP.A2[r], cP.lnA2[r], cP.b2[r], cP.Ea2[r], ln_t, t_inv)
+                                        : arrhenius(t, cP.A2[r], cP.b2[r], cP.Ea2[r]); };
   double c[NS];
   OSTC_UNROLL for (int l = 0; l < NS; ++l) c[l] = density * Y[l] / cP.mw[l] * 1e-3;
   double g[NS];
@@ -174,16 +188,20 @@ __device__ __forceinline__ void chemistry(double density, double t, const double
   const int nr = cP.nr;
   for (int r = 0; r < nr; ++r) {
     const int type = cP.label[r];
-    double kf = arrhenius(t, cP.A[r], cP.b[r], cP.Ea[r]);
+    double kf = rate1(r);
     if (type == 3) {
-      // duplicate reaction: the reference adds the second rate in a new basic
-      // block, so only its last product can fuse into the sum
+      if constexpr (FAST) {
+        kf += rate2(r);
+      } else {
+        // duplicate reaction: the reference adds the second rate in a new
+        // basic block, so only its last product can fuse into the sum
 #if OSTC_DUP_FMA
-      const double e2 = cP.Ea2[r] != 0 ? std::exp(-cP.Ea2[r] / t) : 1.0;
-      kf = __fma_rn(arrhenius_pow(t, cP.A2[r], cP.b2[r]), e2, kf);
+        const double e2 = cP.Ea2[r] != 0 ? std::exp(-cP.Ea2[r] / t) : 1.0;
+        kf = __fma_rn(arrhenius_pow(t, cP.A2[r], cP.b2[r]), e2, kf);
 #else
-      kf = __dadd_rn(kf, arrhenius(t, cP.A2[r], cP.b2[r], cP.Ea2[r]));
+        kf = __dadd_rn(kf, arrhenius(t, cP.A2[r], cP.b2[r], cP.Ea2[r]));
 #endif
+      }
     }
     if (type > 3) {
       double cc = 0;
@@ -191,7 +209,7 @@ __device__ __forceinline__ void chemistry(double density, double t, const double
       if (type == 4) {
         kf *= cc;
       } else {
-        const double kf_low = arrhenius(t, cP.A2[r], cP.b2[r], cP.Ea2[r]);
+        const double kf_low = rate2(r);
         const double kf_high = kf;
         const double reduced_pressure = kf_low * cc / kf_high;
         double F = 1.0;
@@ -216,7 +234,7 @@ __device__ __forceinline__ void chemistry(double density, double t, const double
       const double kc = std::pow(temp_t, cP.order[r]) * std::exp(-d_gibbs);
       kb = kf / kc;
     } else {
-      kb = arrhenius(t, cP.A2[r], cP.b2[r], cP.Ea2[r]);
+      kb = rate2(r);
     }
     // rate_of_progress: pow(c, 0) is exactly one, so zero exponents are skipped.
     double a1 = 1.0, a2 = 1.0;

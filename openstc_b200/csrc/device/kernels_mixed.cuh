@@ -389,7 +389,8 @@ __device__ __forceinline__ void sst_source(const DevBlock &B, int64_t n, double 
 
 }  // namespace fp32
 
-// Finite-rate chemistry of one cell in FP64 (the code of the FP64 path):
+// Finite-rate chemistry of one cell in FP64 (the FP64 path's code with each
+// Arrhenius rate as one exponential):
 // returns dq species = J omega and writes the EPI / DA Jacobian.  q1, q2:
 // this thread's column of the CTA's shared rate arrays (stride kCta).
 template <class C>
@@ -400,7 +401,7 @@ __device__ __forceinline__ void chem_cell(const DevBlock &B, int64_t n, int64_t 
   double Y[NS], omega[NS], omega_d[NS];
   OSTC_UNROLL for (int l = 0; l < NS; ++l) Y[l] = ld(B.sv + l * sz + n);
   const double density = ld(B.bv + n), t = ld(B.bv + 5 * sz + n);
-  chemistry<NS>(density, t, Y, omega, omega_d, q1, q2, kCta);
+  chemistry<NS, true>(density, t, Y, omega, omega_d, q1, q2, kCta);
   const double jac = ld(B.jac + n);
   OSTC_UNROLL for (int l = 0; l < NS; ++l) dq_spec[l] = jac * omega[l];
   const int method = cP.chem_src_method;

@@ -125,6 +125,8 @@ void Driver::build_dev_params() {
     p.A2[r] = reac.A2[r];
     p.b2[r] = reac.b2[r];
     p.Ea2[r] = reac.Ea2[r];
+    p.lnA[r] = reac.A[r] != 0 ? std::log(std::fabs(reac.A[r])) : 0.0;
+    p.lnA2[r] = reac.A2[r] != 0 ? std::log(std::fabs(reac.A2[r])) : 0.0;
     p.troe_a[r] = reac.troe_alpha[r];
     p.troe_t3[r] = reac.troe_t3[r];
     p.troe_t1[r] = reac.troe_t1[r];
