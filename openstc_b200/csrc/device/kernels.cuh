@@ -166,10 +166,17 @@ __device__ __forceinline__ double arrhenius_exp(double A, double lnA, double b, 
   return A == 0 ? 0.0 : copysign(std::exp(lnA + b * ln_t - Ea * t_inv), A);
 }
 
+// c^e for a stoichiometric exponent: products for 1..3, pow otherwise.
+__device__ __forceinline__ double ipow(double c, int e) {
+  return e == 1 ? c : (e == 2 ? c * c : (e == 3 ? c * c * c : std::pow(c, e)));
+}
+
 // finite_rate_chemistry, src/FiniteRateChem.cu:7-63 with the rate helpers
 // :65-171.  q1/q2 live in shared memory with stride `st` (CTA size).
-// FAST (the FP32-bulk path): every Arrhenius rate as one exponential
-// (arrhenius_exp) instead of a pow and an exponential; the FP64 path keeps the
+// FAST (the FP32-bulk path, FP64 arithmetic within a few ulps of the
+// reference form): every Arrhenius rate and every K_c as one exponential,
+// integer concentration powers as products, the Troe 10^x as an exponential
+// and the Gibbs polynomials without divisions; the FP64 path keeps the
 // reference's form bit for bit.
 template <int NS, bool FAST = false>
 __device__ __forceinline__ void chemistry(double density, double t, const double *Y, double *omega, double *omega_d,
@@ -182,9 +189,14 @@ __device__ __forceinline__ void chemistry(double density, double t, const double
   double c[NS];
   OSTC_UNROLL for (int l = 0; l < NS; ++l) c[l] = density * Y[l] / cP.mw[l] * 1e-3;
   double g[NS];
-  gibbs_rt<NS>(t, g);
+  if constexpr (FAST)
+    gibbs_rt_fast<NS>(t, ln_t, t_inv, g);
+  else
+    gibbs_rt<NS>(t, g);
   constexpr double temp_p = kDP_atm / kDR_u * 1e-3;
   const double temp_t = temp_p / t;
+  // FAST: ln(temp_p / T), for K_c as one exponential
+  const double ln_temp_t = FAST ? std::log(temp_p) - ln_t : 0.0;
   const int nr = cP.nr;
   for (int r = 0; r < nr; ++r) {
     const int type = cP.label[r];
@@ -222,7 +234,7 @@ __device__ __forceinline__ void chemistry(double density, double t, const double
           const double logPr = std::log10(reduced_pressure);
           const double tempo = (logPr + cq) / (nq - 0.14 * (logPr + cq));
           const double pq = logFc / (1.0 + tempo * tempo);
-          F = std::pow(10, pq);
+          F = FAST ? std::exp(pq * 2.302585092994045684) : std::pow(10, pq);
         }
         kf = kf_high * reduced_pressure / (1.0 + reduced_pressure) * F;
       }
@@ -231,8 +243,13 @@ __device__ __forceinline__ void chemistry(double density, double t, const double
     if (type != 2) {
       double d_gibbs = 0;
       OSTC_UNROLL for (int l = 0; l < NS; ++l) d_gibbs += g[l] * (cP.sb[r * NS + l] - cP.sf[r * NS + l]);
-      const double kc = std::pow(temp_t, cP.order[r]) * std::exp(-d_gibbs);
-      kb = kf / kc;
+      if constexpr (FAST) {
+        // kf / K_c with K_c = (p_atm / R T)^order exp(-dG / RT) as one exponential
+        kb = kf * std::exp(d_gibbs - cP.order[r] * ln_temp_t);
+      } else {
+        const double kc = std::pow(temp_t, cP.order[r]) * std::exp(-d_gibbs);
+        kb = kf / kc;
+      }
     } else {
       kb = rate2(r);
     }
@@ -240,8 +257,13 @@ __device__ __forceinline__ void chemistry(double density, double t, const double
     double a1 = 1.0, a2 = 1.0;
     OSTC_UNROLL for (int j = 0; j < NS; ++j) {
       const int ef = cP.sf[r * NS + j], eb = cP.sb[r * NS + j];
-      if (ef != 0) a1 *= std::pow(c[j], ef);
-      if (eb != 0) a2 *= std::pow(c[j], eb);
+      if constexpr (FAST) {  // integer powers by products
+        if (ef != 0) a1 *= ipow(c[j], ef);
+        if (eb != 0) a2 *= ipow(c[j], eb);
+      } else {
+        if (ef != 0) a1 *= std::pow(c[j], ef);
+        if (eb != 0) a2 *= std::pow(c[j], eb);
+      }
     }
     a1 *= kf;
     a2 *= kb;

@@ -92,17 +92,25 @@ __device__ __forceinline__ void thermo(float t, float *h, float *cp) {
 }
 
 // ------------------------------------------------------------ inviscid face
-template <class C>
-__device__ __forceinline__ void inviscid_face(const DevBlock &B, int64_t n, int d, int64_t s, float *fc) {
+// The face functions read the primitive stencil through a reader, so that one
+// copy of the physics serves the kernels that load it from the FP64 arrays
+// and the one that stages it in shared memory.  Primitive index v: 0..5 the
+// basic variables (rho, u, v, w, p, T), 6.. the scalars (Y_k, k, omega);
+// flux variable l is primitive l below 5 and l + 1 from 5 on.
+
+// get(l, q): flux variable l at cell c + q (q = -1..2) of the face between
+// cell c (linear index n) and c + 1 (n + s).
+template <class C, class Get>
+__device__ __forceinline__ void inviscid_face_r(const DevBlock &B, int64_t n, int d, int64_t s, Get &&get,
+                                                float *fc) {
   constexpr int NV = C::nv, NS = C::ns;
   const int64_t sz = B.G.size;
   float pl[NV + 2], pr[NV + 2];
   const int rec = cP.reconstruction;
   OSTC_UNROLL for (int l = 0; l < NV; ++l) {
-    const double *a = l < 5 ? B.bv + l * sz : B.sv + (l - 5) * sz;
-    const float p0 = ldf(a + n), p1 = ldf(a + n + s);
+    const float p0 = get(l, 0), p1 = get(l, 1);
     if (rec == 2 || rec == 3) {
-      const float pm = ldf(a + n - s), p2 = ldf(a + n + 2 * s);
+      const float pm = get(l, -1), p2 = get(l, 2);
       const float d_i = p0 - pm, d_i1 = p1 - p0, d_i2 = p2 - p1;
       if (rec == 2) {
         const float neg_l = minmod(d_i, d_i1), pos_l = minmod(d_i1, d_i);
@@ -191,13 +199,22 @@ __device__ __forceinline__ void inviscid_face(const DevBlock &B, int64_t n, int 
   const float mass_flux_half = c * (rho_l * mach_pos + rho_r * mach_neg);
   const float coeff = mass_flux_half * gk;
   const bool up = mass_flux_half >= 0;
-  const float *q = up ? pl : pr;
+  // upwind state, selected per element so that pl / pr stay in registers
+  auto q = [&](int l) { return up ? pl[l] : pr[l]; };
   fc[0] = coeff;
-  fc[1] = coeff * q[1] + p_coeff * k1;
-  fc[2] = coeff * q[2] + p_coeff * k2;
-  fc[3] = coeff * q[3] + p_coeff * k3;
-  fc[4] = coeff * (q[NV] + q[4]) / q[0];
-  OSTC_UNROLL for (int l = 5; l < NV; ++l) fc[l] = coeff * q[l];
+  fc[1] = coeff * q(1) + p_coeff * k1;
+  fc[2] = coeff * q(2) + p_coeff * k2;
+  fc[3] = coeff * q(3) + p_coeff * k3;
+  fc[4] = coeff * (q(NV) + q(4)) / q(0);
+  OSTC_UNROLL for (int l = 5; l < NV; ++l) fc[l] = coeff * q(l);
+}
+
+template <class C>
+__device__ __forceinline__ void inviscid_face(const DevBlock &B, int64_t n, int d, int64_t s, float *fc) {
+  const int64_t sz = B.G.size;
+  inviscid_face_r<C>(
+      B, n, d, s,
+      [&](int l, int q) { return ldf((l < 5 ? B.bv + l * sz : B.sv + (l - 5) * sz) + n + q * s); }, fc);
 }
 
 // ------------------------------------------------------------- viscous face
@@ -211,10 +228,14 @@ __device__ __forceinline__ void face_grad(const double *a, int64_t n, int64_t n1
                  : 0.25f * (ldf(a + n + sxy) - ldf(a + n - sxy) + ldf(a + n1 + sxy) - ldf(a + n1 - sxy));
 }
 
-template <class C>
-__device__ __forceinline__ void viscous_face(const DevBlock &B, int64_t n, int d, int64_t s, float *fv) {
+// val(v, side): primitive v at cell c (side 0) or c + 1 (side 1) of the face;
+// grad(v, g_xi, g_eta, g_zeta): its computational-space gradient at the face
+// (the face_grad stencil).
+template <class C, class Val, class Grad>
+__device__ __forceinline__ void viscous_face_r(const DevBlock &B, int64_t n, int d, int64_t s, Val &&val,
+                                               Grad &&grad, float *fv) {
   constexpr int NS = C::ns;
-  const int64_t sz = B.G.size, sx = B.G.sx, sxy = B.G.sxy;
+  const int64_t sz = B.G.size;
   const int64_t n1 = n + s;
   const double *m = B.metric;
   float mm[9];
@@ -228,13 +249,13 @@ __device__ __forceinline__ void viscous_face(const DevBlock &B, int64_t n, int d
   };
   float g0, g1, g2;
   float u_x, u_y, u_z, v_x, v_y, v_z, w_x, w_y, w_z, t_x, t_y, t_z;
-  face_grad(B.bv + sz, n, n1, d, sx, sxy, g0, g1, g2);
+  grad(1, g0, g1, g2);
   cart(g0, g1, g2, u_x, u_y, u_z);
-  face_grad(B.bv + 2 * sz, n, n1, d, sx, sxy, g0, g1, g2);
+  grad(2, g0, g1, g2);
   cart(g0, g1, g2, v_x, v_y, v_z);
-  face_grad(B.bv + 3 * sz, n, n1, d, sx, sxy, g0, g1, g2);
+  grad(3, g0, g1, g2);
   cart(g0, g1, g2, w_x, w_y, w_z);
-  face_grad(B.bv + 5 * sz, n, n1, d, sx, sxy, g0, g1, g2);
+  grad(5, g0, g1, g2);
   cart(g0, g1, g2, t_x, t_y, t_z);
   const float mul = 0.5f * (ldf(B.mul + n) + ldf(B.mul + n1));
   float mut = 0;
@@ -248,7 +269,7 @@ __device__ __forceinline__ void viscous_face(const DevBlock &B, int64_t n, int d
   const float tau_xz = viscosity * (u_z + w_x);
   const float tau_yz = viscosity * (v_z + w_y);
   if constexpr (C::turb) {
-    const float tt = -(1.f / 3.f) * (ldf(B.bv + n) * ldf(B.sv + NS * sz + n) + ldf(B.bv + n1) * ldf(B.sv + NS * sz + n1));
+    const float tt = -(1.f / 3.f) * (val(0, 0) * val(6 + NS, 0) + val(0, 1) * val(6 + NS, 1));
     tau_xx += tt;
     tau_yy += tt;
     tau_zz += tt;
@@ -262,9 +283,9 @@ __device__ __forceinline__ void viscous_face(const DevBlock &B, int64_t n, int d
   fv[1] = kx * tau_xx + ky * tau_xy + kz * tau_xz;
   fv[2] = kx * tau_xy + ky * tau_yy + kz * tau_yz;
   fv[3] = kx * tau_xz + ky * tau_yz + kz * tau_zz;
-  const float um = 0.5f * (ldf(B.bv + sz + n) + ldf(B.bv + sz + n1));
-  const float vm = 0.5f * (ldf(B.bv + 2 * sz + n) + ldf(B.bv + 2 * sz + n1));
-  const float wm = 0.5f * (ldf(B.bv + 3 * sz + n) + ldf(B.bv + 3 * sz + n1));
+  const float um = 0.5f * (val(1, 0) + val(1, 1));
+  const float vm = 0.5f * (val(2, 0) + val(2, 1));
+  const float wm = 0.5f * (val(3, 0) + val(3, 1));
   float conductivity = 0.5f * (ldf(B.cond + n) + ldf(B.cond + n1));
   if constexpr (C::turb) conductivity += 0.5f * (ldf(B.turb_cond + n) + ldf(B.turb_cond + n1));
   fv[4] = um * fv[1] + vm * fv[2] + wm * fv[3] + conductivity * (kx * t_x + ky * t_y + kz * t_z);
@@ -272,12 +293,12 @@ __device__ __forceinline__ void viscous_face(const DevBlock &B, int64_t n, int d
     float turb_d = 0;
     if constexpr (C::turb) turb_d = mut / cF.Sct;
     float h[NS], dif[NS], yx[NS], yy[NS], yz[NS];
-    const float tm = 0.5f * (ldf(B.bv + 5 * sz + n) + ldf(B.bv + 5 * sz + n1));
+    const float tm = 0.5f * (val(5, 0) + val(5, 1));
     thermo<NS, true, false>(tm, h, nullptr);
     float rho_uc = 0, rho_vc = 0, rho_wc = 0, hflux = 0;
     OSTC_UNROLL for (int l = 0; l < NS; ++l) {
       dif[l] = 0.5f * (ldf(B.rho_d + l * sz + n) + ldf(B.rho_d + l * sz + n1)) + turb_d;
-      face_grad(B.sv + l * sz, n, n1, d, sx, sxy, g0, g1, g2);
+      grad(6 + l, g0, g1, g2);
       cart(g0, g1, g2, yx[l], yy[l], yz[l]);
       hflux += dif[l] * h[l] * (kx * yx[l] + ky * yy[l] + kz * yz[l]);
       rho_uc += dif[l] * yx[l];
@@ -288,23 +309,22 @@ __device__ __forceinline__ void viscous_face(const DevBlock &B, int64_t n, int d
     const float corr = kx * rho_uc + ky * rho_vc + kz * rho_wc;
     OSTC_UNROLL for (int l = 0; l < NS; ++l) {
       fv[5 + l] = dif[l] * (kx * yx[l] + ky * yy[l] + kz * yz[l]) -
-                  0.5f * (ldf(B.sv + l * sz + n) + ldf(B.sv + l * sz + n1)) * corr;
+                  0.5f * (val(6 + l, 0) + val(6 + l, 1)) * corr;
     }
   }
   if constexpr (C::turb) {
-    const double *tk = B.sv + NS * sz, *tw = B.sv + (NS + 1) * sz;
     float k_x, k_y, k_z, o_x, o_y, o_z;
-    face_grad(tk, n, n1, d, sx, sxy, g0, g1, g2);
+    grad(6 + NS, g0, g1, g2);
     cart(g0, g1, g2, k_x, k_y, k_z);
-    face_grad(tw, n, n1, d, sx, sxy, g0, g1, g2);
+    grad(7 + NS, g0, g1, g2);
     cart(g0, g1, g2, o_x, o_y, o_z);
     const float wall_dist = 0.5f * (ldf(B.wall_dist + n) + ldf(B.wall_dist + n1));
     float f1 = 1;
     if (wall_dist > 1e-25f) {
-      const float km = 0.5f * (ldf(tk + n) + ldf(tk + n1));
-      const float omegam = 0.5f * (ldf(tw + n) + ldf(tw + n1));
+      const float km = 0.5f * (val(6 + NS, 0) + val(6 + NS, 1));
+      const float omegam = 0.5f * (val(7 + NS, 0) + val(7 + NS, 1));
       const float param1 = sqrtf(km) / (0.09f * omegam * wall_dist);
-      const float rhom = 0.5f * (ldf(B.bv + n) + ldf(B.bv + n1));
+      const float rhom = 0.5f * (val(0, 0) + val(0, 1));
       const float d2 = wall_dist * wall_dist;
       const float param2 = 500 * mul / (rhom * d2 * omegam);
       constexpr float so2 = static_cast<float>(sst::sigma_omega2);
@@ -319,6 +339,15 @@ __device__ __forceinline__ void viscous_face(const DevBlock &B, int64_t n, int d
     fv[5 + NS] = (mul + mut * sigma_k) * (kx * k_x + ky * k_y + kz * k_z);
     fv[6 + NS] = (mul + mut * sigma_omega) * (kx * o_x + ky * o_y + kz * o_z);
   }
+}
+
+template <class C>
+__device__ __forceinline__ void viscous_face(const DevBlock &B, int64_t n, int d, int64_t s, float *fv) {
+  const int64_t sz = B.G.size, sx = B.G.sx, sxy = B.G.sxy, n1 = n + s;
+  auto ptr = [&](int v) { return v < 6 ? B.bv + v * sz : B.sv + (v - 6) * sz; };
+  viscous_face_r<C>(
+      B, n, d, s, [&](int v, int side) { return ldf(ptr(v) + (side ? n1 : n)); },
+      [&](int v, float &g0, float &g1, float &g2) { face_grad(ptr(v), n, n1, d, sx, sxy, g0, g1, g2); }, fv);
 }
 
 // ------------------------------------------------------------- SST source
@@ -410,6 +439,10 @@ __device__ __forceinline__ void chem_cell(const DevBlock &B, int64_t n, int64_t 
     // loop: each row m visits only the reactions that change species m once,
     // and every (m, q) entry still sums its terms in reaction order
     const int nr = cP.nr;
+    // 1 / (rho Y_q) once per species (0 below the floor): products, not
+    // NS^2 divisions, within an ulp of the FP64 path's quotients
+    double inv_rho_y[NS];
+    OSTC_UNROLL for (int q = 0; q < NS; ++q) inv_rho_y[q] = Y[q] > 1e-25 ? 1.0 / (density * Y[q]) : 0.0;
     OSTC_UNROLL for (int m = 0; m < NS; ++m) {
       double zz[NS];
       OSTC_UNROLL for (int q = 0; q < NS; ++q) zz[q] = 0;
@@ -420,7 +453,7 @@ __device__ __forceinline__ void chem_cell(const DevBlock &B, int64_t n, int64_t 
         OSTC_UNROLL for (int q = 0; q < NS; ++q) zz[q] += dn * (cP.sf[r * NS + q] * a1 - cP.sb[r * NS + q] * a2);
       }
       OSTC_UNROLL for (int q = 0; q < NS; ++q) {
-        const double v = Y[q] > 1e-25 ? zz[q] / (density * Y[q]) : 0.0;
+        const double v = zz[q] * inv_rho_y[q];
         B.chem_jac[(m * NS + q) * sz0 + nz] = cP.mw[m] * v * 1e+3;
       }
     }

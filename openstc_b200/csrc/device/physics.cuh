@@ -126,6 +126,27 @@ __device__ __forceinline__ void gibbs_rt(double t, double *g) {
   }
 }
 
+// gibbs_rt for the FP32-bulk path: the same polynomials with ln T and 1 / T
+// passed in and the constant divisors as products (within an ulp or two).
+template <int NS>
+__device__ __forceinline__ void gibbs_rt_fast(double t, double log_t, double t_inv, double *g) {
+  constexpr double k6 = 1.0 / 6.0, k12 = 1.0 / 12.0;
+  const double t2 = t * t, t3 = t2 * t, t4 = t3 * t;
+  OSTC_UNROLL for (int i = 0; i < NS; ++i) {
+    if (t < cP.t_low[i]) {
+      const double tt = cP.t_low[i];
+      const double tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt, tt_inv = 1 / tt, log_tt = std::log(tt);
+      const double *c = &cP.low[i * 7];
+      g[i] = c[0] * (1.0 - log_tt) - 0.5 * c[1] * tt - c[2] * tt2 * k6 - c[3] * tt3 * k12 - c[4] * tt4 * 0.05 +
+             c[5] * tt_inv - c[6];
+    } else {
+      const bool lo = t < cP.t_mid[i];
+      g[i] = nasa(i, 0, lo) * (1.0 - log_t) - 0.5 * nasa(i, 1, lo) * t - nasa(i, 2, lo) * t2 * k6 -
+             nasa(i, 3, lo) * t3 * k12 - nasa(i, 4, lo) * t4 * 0.05 + nasa(i, 5, lo) * t_inv - nasa(i, 6, lo);
+    }
+  }
+}
+
 // ------------------------------------------------------------------ transport
 // Sutherland, src/Transport.cu:6-9
 __device__ __forceinline__ double sutherland(double t) {
