@@ -77,6 +77,10 @@ struct DevBlock {
   // chemically quiet take its increment rate rho dY/dt as an explicit source
   unsigned char *chem_quiet;
   double *chem_rate;
+  // FP32-bulk path under DPLUR: the increments in FP32 (layout D, nv
+  // components each): [0] dq0, [1] and [2] the ping-pong of the sweeps; the
+  // last sweep writes the FP64 dq.  Null on the FP64 path.
+  float *dqf[3];
 };
 
 // Work table of a launch: CTA-tiles of every block, in block order.

@@ -397,6 +397,17 @@ class EngineT final : public Engine {
       allocations_.push_back(q);
       B.h_spec = static_cast<double *>(q);
     }
+    for (auto &f : B.dqf) f = nullptr;
+    if (C::mixed && p.implicit_method == 1) {
+      for (auto &f : B.dqf) {
+        void *q = nullptr;
+        const size_t bytes = sizeof(float) * static_cast<size_t>(B.D.size) * C::nv;
+        cuda_check(cudaMalloc(&q, bytes), "cudaMalloc dqf");
+        cuda_check(cudaMemset(q, 0, bytes), "memset dqf");
+        allocations_.push_back(q);
+        f = static_cast<float *>(q);
+      }
+    }
     B.lu_piv = nullptr;
     if (C::mix == 2 && p.chem_src_method == 1) {
       void *q = nullptr;
@@ -530,17 +541,27 @@ class EngineT final : public Engine {
     if (p.implicit_method == 1) {
       k_dq0<C><<<grid(tiles0_), block3(), dq0_smem_, stream_>>>(d_blocks_, tiles0_);
       mark("dq0");
-      int in = 1;
-      for (int s = 0; s < p.dplur_inner_step; ++s) {
-        const int out = (s % 2 == 0) ? 2 : 0;
-        if constexpr (C::mixed)
+      if constexpr (C::mixed) {
+        // FP32 increments dqf[0] (dq0) -> dqf[1] -> dqf[2] -> ..., the last
+        // sweep into the FP64 dq (k_dq0 writes the FP64 dq0 when there is no sweep)
+        int in = 0;
+        for (int s = 0; s < p.dplur_inner_step; ++s) {
+          const int out = s + 1 == p.dplur_inner_step ? -1 : (s % 2 == 0 ? 1 : 2);
           k_sweep_mx<C><<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_, in, out);
-        else
+          mark("dplur_sweep");
+          in = out;
+        }
+        final_dq_ = p.dplur_inner_step > 0 ? 0 : 1;
+      } else {
+        int in = 1;
+        for (int s = 0; s < p.dplur_inner_step; ++s) {
+          const int out = (s % 2 == 0) ? 2 : 0;
           k_sweep<C><<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_, in, out);
-        mark("dplur_sweep");
-        in = out;
+          mark("dplur_sweep");
+          in = out;
+        }
+        final_dq_ = in;
       }
-      final_dq_ = in;
     } else {
       if ((C::mix == 2 && p.chem_src_method != 0) || (C::turb && p.turb_implicit == 1))
         k_point_implicit<C><<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_);

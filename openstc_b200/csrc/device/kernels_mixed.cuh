@@ -743,7 +743,9 @@ __global__ void __launch_bounds__(kFluxThreads, 4) k_flux_mx_col(const DevBlock 
 }
 
 // DPLUR sweep with FP32 flux-Jacobian products; the update of the point
-// implicit blocks (EPI: stored LU factors) in FP64.
+// implicit blocks (EPI: stored LU factors) in FP64.  The increments are FP32
+// arrays: reads dqf[in_sel] (neighbours) and dqf[0] (dq0), writes
+// dqf[out_sel], or the FP64 dq when out_sel < 0 (the last sweep).
 template <class C>
 __global__ void __launch_bounds__(kCta, 4) k_sweep_mx(const DevBlock *__restrict__ blks, Tiles T, int in_sel,
                                                       int out_sel) {
@@ -752,8 +754,8 @@ __global__ void __launch_bounds__(kCta, 4) k_sweep_mx(const DevBlock *__restrict
   int b, i, j, k;
   if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
   const DevBlock &B = blks[b];
-  const double *dqin = in_sel == 0 ? B.dq : (in_sel == 1 ? B.dq0 : B.dqk);
-  double *dqout = out_sel == 0 ? B.dq : B.dqk;
+  const float *dqin = B.dqf[in_sel];
+  const float *dq0 = B.dqf[0];
   const int64_t sz = B.G.size, szd = B.D.size, sz0 = B.Z.size;
   const int64_t n = B.G.at(i, j, k), nd = B.D.at(i, j, k), nz = B.Z.at(i, j, k);
   const int64_t sx = B.G.sx, sxy = B.G.sxy, dsx = B.D.sx, dsxy = B.D.sxy;
@@ -779,7 +781,7 @@ __global__ void __launch_bounds__(kCta, 4) k_sweep_mx(const DevBlock *__restrict
     const float vel = ldf(B.vel + on);
     const float e = 0.5f * vel * vel;
     float d[NV];
-    OSTC_UNROLL for (int l = 0; l < NV; ++l) d[l] = ldf(dqin + l * szd + od);
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) d[l] = __ldg(dqin + l * szd + od);
     float gamma = 1.4f, b3 = 0, b4 = 0, h = 0;
     if constexpr (C::mix != 0) {
       const float t = ldf(B.bv + 5 * sz + on);
@@ -811,39 +813,42 @@ __global__ void __launch_bounds__(kCta, 4) k_sweep_mx(const DevBlock *__restrict
   const double diag = 1 + dt * (isr[nd] + isr[szd + nd] + isr[2 * szd + nd]);
   double out[NV];
   if constexpr (C::mix != 2) {
-    OSTC_UNROLL for (int l = 0; l < 5 + NS; ++l) out[l] = B.dq0[l * szd + nd] + dt * tot[l] / diag;
+    OSTC_UNROLL for (int l = 0; l < 5 + NS; ++l) out[l] = static_cast<double>(dq0[l * szd + nd]) + dt * tot[l] / diag;
   } else {
-    OSTC_UNROLL for (int l = 0; l < 5; ++l) out[l] = B.dq0[l * szd + nd] + dt * tot[l] / diag;
+    OSTC_UNROLL for (int l = 0; l < 5; ++l) out[l] = static_cast<double>(dq0[l * szd + nd]) + dt * tot[l] / diag;
     const int method = cP.chem_src_method;
     if (B.chem_quiet && B.chem_quiet[nz]) {
       // chemically quiet: the stored factors would be diag I
-      OSTC_UNROLL for (int l = 0; l < NS; ++l) out[5 + l] = B.dq0[(5 + l) * szd + nd] + dt * tot[5 + l] / diag;
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) out[5 + l] = static_cast<double>(dq0[(5 + l) * szd + nd]) + dt * tot[5 + l] / diag;
     } else if (method == 1) {
-      double lhs[NS * NS];
       int piv[NS];
-      OSTC_UNROLL for (int q = 0; q < NS * NS; ++q) lhs[q] = B.chem_jac[q * sz0 + nz];
       OSTC_UNROLL for (int q = 0; q < NS; ++q) piv[q] = B.lu_piv[q * sz0 + nz];
       double rhs[NS];
       OSTC_UNROLL for (int l = 0; l < NS; ++l) rhs[l] = static_cast<double>(tot[5 + l]) * dt;
-      lu_solve<NS>(lhs, piv, rhs);
-      OSTC_UNROLL for (int l = 0; l < NS; ++l) out[5 + l] = B.dq0[(5 + l) * szd + nd] + rhs[l];
+      lu_solve_g<NS>(B.chem_jac + nz, sz0, piv, rhs);
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) out[5 + l] = static_cast<double>(dq0[(5 + l) * szd + nd]) + rhs[l];
     } else if (method == 2) {
       OSTC_UNROLL for (int l = 0; l < NS; ++l)
-        out[5 + l] = B.dq0[(5 + l) * szd + nd] + dt * tot[5 + l] / (diag - dt * B.chem_jac[l * sz0 + nz]);
+        out[5 + l] = static_cast<double>(dq0[(5 + l) * szd + nd]) + dt * tot[5 + l] / (diag - dt * B.chem_jac[l * sz0 + nz]);
     } else {
-      OSTC_UNROLL for (int l = 0; l < NS; ++l) out[5 + l] = B.dq0[(5 + l) * szd + nd] + dt * tot[5 + l] / diag;
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) out[5 + l] = static_cast<double>(dq0[(5 + l) * szd + nd]) + dt * tot[5 + l] / diag;
     }
   }
   if constexpr (C::turb) {
     if (cP.turb_implicit == 1) {
-      out[NS + 5] = B.dq0[(NS + 5) * szd + nd] + dt * tot[5 + NS] / (diag - dt * B.turb_src_jac[nz]);
-      out[NS + 6] = B.dq0[(NS + 6) * szd + nd] + dt * tot[6 + NS] / (diag - dt * B.turb_src_jac[sz0 + nz]);
+      out[NS + 5] = static_cast<double>(dq0[(NS + 5) * szd + nd]) + dt * tot[5 + NS] / (diag - dt * B.turb_src_jac[nz]);
+      out[NS + 6] = static_cast<double>(dq0[(NS + 6) * szd + nd]) + dt * tot[6 + NS] / (diag - dt * B.turb_src_jac[sz0 + nz]);
     } else {
-      out[NS + 5] = B.dq0[(NS + 5) * szd + nd] + dt * tot[5 + NS] / diag;
-      out[NS + 6] = B.dq0[(NS + 6) * szd + nd] + dt * tot[6 + NS] / diag;
+      out[NS + 5] = static_cast<double>(dq0[(NS + 5) * szd + nd]) + dt * tot[5 + NS] / diag;
+      out[NS + 6] = static_cast<double>(dq0[(NS + 6) * szd + nd]) + dt * tot[6 + NS] / diag;
     }
   }
-  OSTC_UNROLL for (int l = 0; l < NV; ++l) dqout[l * szd + nd] = out[l];
+  if (out_sel < 0) {
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq[l * szd + nd] = out[l];
+  } else {
+    float *dqout = B.dqf[out_sel];
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) dqout[l * szd + nd] = static_cast<float>(out[l]);
+  }
 }
 
 // Thermodynamic and transport properties in FP32 (update_physical_properties).

@@ -403,6 +403,32 @@ __device__ __forceinline__ void lu_solve(const double *lhs, const int *ipiv, dou
   }
 }
 
+// lu_solve with the factors read from the arrays (entry q of the cell at
+// lhs[q * st]): each factor is used once, so none is held in registers or
+// local memory; same operations in the same order as lu_solve.
+template <int NS>
+__device__ __forceinline__ void lu_solve_g(const double *__restrict__ lhs, int64_t st, const int *ipiv,
+                                           double *rhs) {
+  OSTC_UNROLL for (int m = 0; m < NS; ++m) {
+    const int t = ipiv[m];
+    if (t != m) {
+      double a = rhs[m], other = 0;
+      OSTC_UNROLL for (int q = m + 1; q < NS; ++q)
+        if (q == t) other = rhs[q];
+      OSTC_UNROLL for (int q = m + 1; q < NS; ++q)
+        if (q == t) rhs[q] = a;
+      rhs[m] = other;
+    }
+  }
+  OSTC_UNROLL for (int m = 1; m < NS; ++m)
+    OSTC_UNROLL for (int t = 0; t < m; ++t) rhs[m] -= __ldg(lhs + (m * NS + t) * st) * rhs[t];
+  rhs[NS - 1] /= __ldg(lhs + (NS * NS - 1) * st);
+  OSTC_UNROLL for (int m = NS - 2; m >= 0; --m) {
+    OSTC_UNROLL for (int t = m + 1; t < NS; ++t) rhs[m] -= __ldg(lhs + (m * NS + t) * st) * rhs[t];
+    rhs[m] /= __ldg(lhs + (m * NS + m) * st);
+  }
+}
+
 // Explicit-mode point-implicit treatment: EPI / DA and the SST diagonal,
 // src/ImplicitTreatmentHPP.cuh:14-54, src/FiniteRateChem.cu:211-234, 400-412,
 // src/SST.cu:180-194.
@@ -499,7 +525,13 @@ __global__ void __launch_bounds__(kCta) k_dq0(const DevBlock *__restrict__ blks,
       dq[NS + 6] /= diag;
     }
   }
-  OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq0[l * szd + nd] = dq[l];
+  if constexpr (C::mixed) {
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dqf[0][l * szd + nd] = static_cast<float>(dq[l]);
+    if (cP.dplur_inner_step == 0)
+      OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq0[l * szd + nd] = dq[l];
+  } else {
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq0[l * szd + nd] = dq[l];
+  }
 }
 
 // compute_jacobian_times_dq, src/DPLURHPP.cuh:78-125, accumulated into tot
@@ -594,13 +626,11 @@ __global__ void __launch_bounds__(kCta, OSTC_SWEEP_MIN_BLOCKS) k_sweep(const Dev
       // chemically quiet: the stored factors would be diag I
       OSTC_UNROLL for (int l = 0; l < NS; ++l) out[5 + l] = B.dq0[(5 + l) * szd + nd] + dt * tot[5 + l] / diag;
     } else if (method == 1) {
-      double lhs[NS * NS];
       int piv[NS];
-      OSTC_UNROLL for (int q = 0; q < NS * NS; ++q) lhs[q] = B.chem_jac[q * sz0 + nz];
       OSTC_UNROLL for (int q = 0; q < NS; ++q) piv[q] = B.lu_piv[q * sz0 + nz];
       double rhs[NS];
       OSTC_UNROLL for (int l = 0; l < NS; ++l) rhs[l] = tot[5 + l] * dt;
-      lu_solve<NS>(lhs, piv, rhs);
+      lu_solve_g<NS>(B.chem_jac + nz, sz0, piv, rhs);
       OSTC_UNROLL for (int l = 0; l < NS; ++l) out[5 + l] = B.dq0[(5 + l) * szd + nd] + rhs[l];
     } else if (method == 2) {
       OSTC_UNROLL for (int l = 0; l < NS; ++l)
