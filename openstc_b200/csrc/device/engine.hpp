@@ -85,6 +85,17 @@ class Engine {
   // since the surrogate was set
   // accepted, sent to the EPI fallback, evaluated by the network
   virtual void surrogate_stats(unsigned long long out[3]) = 0;
+  // Output pipeline (.plt written while the next steps run): get_field_async
+  // enqueues the device-to-host copy on the engine stream and returns at once
+  // (asynchronous for host memory made page-locked by pin_host);
+  // record_output_event(slot) marks everything enqueued so far, and
+  // wait_output_event(slot), callable from any host thread, blocks until it
+  // has run.  Two slots.
+  virtual void get_field_async(int b, int field, double *host, int64_t count) = 0;
+  virtual bool pin_host(void *p, size_t bytes) = 0;  // false (and no error left behind) if refused
+  virtual void unpin_host(void *p) = 0;
+  virtual void record_output_event(int slot) = 0;
+  virtual void wait_output_event(int slot) = 0;
 };
 
 // Largest grid ostc_driver_residual_noalloc accepts, in residual tiles

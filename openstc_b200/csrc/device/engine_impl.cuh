@@ -111,6 +111,7 @@ class EngineT final : public Engine {
     }
     cuda_check(cudaEventCreate(&ev0_), "event");
     cuda_check(cudaEventCreate(&ev1_), "event");
+    for (auto &e : out_ev_) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
     // the cudaMemset / staged copies above ran on the legacy default stream,
     // which the engine's non-blocking stream does not wait for
     cuda_check(cudaDeviceSynchronize(), "engine setup");
@@ -136,6 +137,7 @@ class EngineT final : public Engine {
     cudaFreeHost(h_res_);
     cudaEventDestroy(ev0_);
     cudaEventDestroy(ev1_);
+    for (auto e : out_ev_) cudaEventDestroy(e);
     cudaStreamDestroy(stream_);
   }
 
@@ -152,6 +154,29 @@ class EngineT final : public Engine {
     check_count(b, field, count);
     cuda_check(cudaMemcpyAsync(host, p, sizeof(double) * count, cudaMemcpyDeviceToHost, stream_), "get_field");
     cuda_check(cudaStreamSynchronize(stream_), "get_field sync");
+  }
+
+  void get_field_async(int b, int field, double *host, int64_t count) override {
+    double *p = field_ptr(b, field);
+    check_count(b, field, count);
+    cuda_check(cudaMemcpyAsync(host, p, sizeof(double) * count, cudaMemcpyDeviceToHost, stream_), "get_field_async");
+  }
+
+  bool pin_host(void *p, size_t bytes) override {
+    if (cudaHostRegister(p, bytes, cudaHostRegisterDefault) == cudaSuccess) return true;
+    cudaGetLastError();  // not sticky: clear it so that no later check reports it
+    return false;
+  }
+
+  void unpin_host(void *p) override { cuda_check(cudaHostUnregister(p), "cudaHostUnregister"); }
+
+  void record_output_event(int slot) override {
+    cuda_check(cudaEventRecord(out_ev_[slot & 1], stream_), "output event");
+  }
+
+  void wait_output_event(int slot) override {
+    cuda_check(cudaSetDevice(setup_.device), "cudaSetDevice");
+    cuda_check(cudaEventSynchronize(out_ev_[slot & 1]), "output event wait");
   }
 
   int64_t field_count(int b, int field) const override {
@@ -767,6 +792,7 @@ class EngineT final : public Engine {
   std::vector<unsigned char *> quiet_store_;
   std::vector<double *> rate_store_;
   cudaEvent_t ev0_{}, ev1_{};
+  cudaEvent_t out_ev_[2]{};  // output pipeline slots
   double last_ms_ = 0;
 };
 

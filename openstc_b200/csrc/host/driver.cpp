@@ -5,11 +5,165 @@
 #include <cstring>
 #include <filesystem>
 #include <fstream>
+#include <condition_variable>
+#include <deque>
+#include <exception>
 #include <limits>
+#include <mutex>
+#include <thread>
 
 #include "plt_io.hpp"
 
 namespace ostc {
+
+// The .plt output of the steady loop without stalling it: at an output step
+// the device-to-host copies of bv, sv, Mach and mu_t go into one of two
+// page-locked staging sets on the engine stream, behind the step's kernels,
+// and the loop goes on; a writer thread waits for the copies, then writes
+// output/message/step.txt and output/field/flowfield.plt exactly as the
+// synchronous path does.  A third output waits for the older set to be
+// written.  flush() returns when everything enqueued is on disk and rethrows
+// a writer error.
+class PltPipeline {
+ public:
+  PltPipeline(Engine &E, const Mesh &mesh, const std::vector<HostField> &field, const Species &spec, bool rans,
+              std::string case_dir)
+      : E_(E), mesh_(mesh), spec_(spec), rans_(rans), dir_(std::move(case_dir)) {
+    for (auto &st : slots_) {
+      st.field.resize(mesh.n_block);
+      st.mach.resize(mesh.n_block);
+      st.mut.resize(mesh.n_block);
+      for (int b = 0; b < mesh.n_block; ++b) {
+        HostField &F = st.field[b];
+        F.e = field[b].e;
+        F.n_scalar = field[b].n_scalar;
+        F.bv.resize(field[b].bv.size());
+        F.sv.resize(field[b].sv.size());
+        st.mach[b].resize(static_cast<size_t>(F.e.size()));
+        if (rans) st.mut[b].resize(static_cast<size_t>(F.e.size()));
+        // page-locked, so that the copies do not stall the loop; where the
+        // host refuses to lock them the copies are synchronous instead
+        for (auto *v : {&F.bv, &F.sv, &st.mach[b], &st.mut[b]})
+          if (!v->empty() && E_.pin_host(v->data(), sizeof(double) * v->size())) pinned_.push_back(v->data());
+      }
+    }
+    writer_ = std::thread([this] { run(); });
+  }
+
+  ~PltPipeline() {
+    {
+      std::unique_lock<std::mutex> lk(mu_);
+      cv_.wait(lk, [this] { return queue_.empty() && !writing_; });
+      stop_ = true;
+    }
+    cv_.notify_all();
+    writer_.join();
+    for (void *p : pinned_) {
+      try {
+        E_.unpin_host(p);
+      } catch (...) {
+      }
+    }
+  }
+
+  void enqueue(int step) {
+    const int s = next_++ & 1;
+    Slot &st = slots_[s];
+    {
+      std::unique_lock<std::mutex> lk(mu_);
+      cv_.wait(lk, [&] { return !st.busy; });
+      rethrow_locked();
+      st.busy = true;
+    }
+    st.step = step;
+    for (int b = 0; b < mesh_.n_block; ++b) {
+      HostField &F = st.field[b];
+      E_.get_field_async(b, F_BV, F.bv.data(), static_cast<int64_t>(F.bv.size()));
+      if (!F.sv.empty()) E_.get_field_async(b, F_SV, F.sv.data(), static_cast<int64_t>(F.sv.size()));
+      E_.get_field_async(b, F_MACH, st.mach[b].data(), static_cast<int64_t>(st.mach[b].size()));
+      if (rans_) E_.get_field_async(b, F_MUT, st.mut[b].data(), static_cast<int64_t>(st.mut[b].size()));
+    }
+    E_.record_output_event(s);
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      queue_.push_back(s);
+    }
+    cv_.notify_all();
+  }
+
+  void flush() {
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_.wait(lk, [this] { return queue_.empty() && !writing_; });
+    rethrow_locked();
+  }
+
+ private:
+  struct Slot {
+    std::vector<HostField> field;
+    std::vector<std::vector<double>> mach, mut;
+    int step = 0;
+    bool busy = false;
+  };
+
+  void rethrow_locked() {
+    if (error_) {
+      std::exception_ptr e = error_;
+      error_ = nullptr;
+      std::rethrow_exception(e);
+    }
+  }
+
+  void run() {
+    for (;;) {
+      int s;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [this] { return stop_ || !queue_.empty(); });
+        if (queue_.empty()) return;
+        s = queue_.front();
+        queue_.pop_front();
+        writing_ = true;
+      }
+      Slot &st = slots_[s];
+      try {
+        E_.wait_output_event(s);
+        const std::filesystem::path dir = std::filesystem::path(dir_) / "output" / "message";
+        std::filesystem::create_directories(dir);
+        std::ofstream(dir / "step.txt") << st.step;
+        std::vector<PltBlockData> blocks(mesh_.n_block);
+        for (int b = 0; b < mesh_.n_block; ++b)
+          blocks[b] = PltBlockData{&mesh_[b], &st.field[b], &st.mach[b], rans_ ? &st.mut[b] : nullptr};
+        write_plt(dir_ + "/output/field/flowfield.plt", blocks, spec_, rans_);
+      } catch (...) {
+        std::lock_guard<std::mutex> lk(mu_);
+        error_ = std::current_exception();
+      }
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        st.busy = false;
+        writing_ = false;
+      }
+      cv_.notify_all();
+    }
+  }
+
+  Engine &E_;
+  const Mesh &mesh_;
+  const Species &spec_;
+  bool rans_;
+  std::string dir_;
+  Slot slots_[2];
+  std::vector<void *> pinned_;
+  int next_ = 0;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::deque<int> queue_;
+  bool writing_ = false, stop_ = false;
+  std::exception_ptr error_;
+  std::thread writer_;
+};
+
+Driver::~Driver() = default;
 
 Driver::Driver(const std::string &dir, const DriverOptions &o) : case_dir(dir), opt(o), parameter(dir) {
   mesh = Mesh(parameter);
@@ -219,6 +373,7 @@ void Driver::initialize_computation() {
   s.wall_points = wall_points;
   s.device = opt.device;
   s.precision = opt.precision;
+  plt_out_.reset();  // bound to the engine it copies from
   engine_ = make_engine(s);
   for (int b = 0; b < mesh.n_block; ++b) {
     const Block &B = mesh[b];
@@ -307,13 +462,12 @@ void Driver::simulate() {
       }
     }
     if (step % out_file == 0 || converged) {
-      const std::filesystem::path dir = std::filesystem::path(case_dir) / "output" / "message";
-      std::filesystem::create_directories(dir);
-      std::ofstream(dir / "step.txt") << step;
-      write_field(case_dir + "/output/field/flowfield.plt");
+      if (!plt_out_) plt_out_ = std::make_unique<PltPipeline>(E, mesh, field, spec, rans, case_dir);
+      plt_out_->enqueue(step);
     }
   }
   E.synchronize();
+  if (plt_out_) plt_out_->flush();
 }
 
 void Driver::write_field(const std::string &path) {

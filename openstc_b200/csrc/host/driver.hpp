@@ -16,6 +16,8 @@
 
 namespace ostc {
 
+class PltPipeline;
+
 struct DriverOptions {
   int device = 0;
   bool quiet = false;
@@ -28,6 +30,7 @@ class Driver {
   // main + Driver constructor, src/main.cu:7-28, src/Driver.cu:14-40).  No
   // GPU work happens here.
   Driver(const std::string &case_dir, const DriverOptions &opt);
+  ~Driver();
 
   // Driver::initialize_computation: creates the engine, uploads the grid and
   // field and runs the initial boundary / exchange / property passes.
@@ -64,6 +67,9 @@ class Driver {
   void build_dev_params();
   void build_faces();
   std::unique_ptr<Engine> engine_;
+  // the .plt output of simulate(), written by a host thread while the next
+  // steps run; declared after engine_ so that it is finished first
+  std::unique_ptr<PltPipeline> plt_out_;
 };
 
 }  // namespace ostc

@@ -102,6 +102,16 @@ void write_plt(const std::string &path, const std::vector<PltBlockData> &blocks,
     o.i32(0);
   }
   o.f32(357.0f);
+  // The header goes out first; then each zone's data header (with the
+  // variables' interior min / max) and its data, streamed one k-plane of one
+  // variable at a time: interior rows are contiguous in the ghosted layout,
+  // so a plane is mz row copies into one reused buffer.
+  const auto parent = std::filesystem::path(path).parent_path();
+  if (!parent.empty()) std::filesystem::create_directories(parent);
+  std::ofstream f(path, std::ios::binary | std::ios::trunc);
+  if (!f) throw ParameterError("cannot write " + path);
+  f.write(o.buf.data(), static_cast<std::streamsize>(o.buf.size()));
+  std::vector<double> plane;
   for (const auto &bd : blocks) {
     const Block &b = *bd.block;
     const HostField &F = *bd.field;
@@ -115,28 +125,35 @@ void write_plt(const std::string &path, const std::vector<PltBlockData> &blocks,
     vars.push_back({bd.mach->data(), &e});
     for (int l = 0; l < F.n_scalar; ++l) vars.push_back({F.sv.data() + l * e.size(), &e});
     if (rans) vars.push_back({bd.mut->data(), &e});
-    o.f32(299.0f);
-    for (int l = 0; l < nvar; ++l) o.i32(2);
-    o.i32(0);
-    o.i32(0);
-    o.i32(-1);
+    Out z;
+    z.f32(299.0f);
+    for (int l = 0; l < nvar; ++l) z.i32(2);
+    z.i32(0);
+    z.i32(0);
+    z.i32(-1);
     for (const auto &[ptr, ext] : vars) {
       double lo = ptr[ext->at(0, 0, 0)], hi = lo;
-      for_interior(b, [&](int i, int j, int k) {
-        const double v = ptr[ext->at(i, j, k)];
-        lo = std::min(lo, v);
-        hi = std::max(hi, v);
-      });
-      o.f64(lo);
-      o.f64(hi);
+      for (int k = 0; k < b.mz; ++k)
+        for (int j = 0; j < b.my; ++j) {
+          const double *row = ptr + ext->at(0, j, k);
+          for (int i = 0; i < b.mx; ++i) {
+            lo = std::min(lo, row[i]);
+            hi = std::max(hi, row[i]);
+          }
+        }
+      z.f64(lo);
+      z.f64(hi);
     }
-    for (const auto &[ptr, ext] : vars) for_interior(b, [&](int i, int j, int k) { o.f64(ptr[ext->at(i, j, k)]); });
+    f.write(z.buf.data(), static_cast<std::streamsize>(z.buf.size()));
+    plane.resize(static_cast<size_t>(b.mx) * b.my);
+    for (const auto &[ptr, ext] : vars)
+      for (int k = 0; k < b.mz; ++k) {
+        for (int j = 0; j < b.my; ++j)
+          std::memcpy(plane.data() + static_cast<size_t>(j) * b.mx, ptr + ext->at(0, j, k), sizeof(double) * b.mx);
+        f.write(reinterpret_cast<const char *>(plane.data()), static_cast<std::streamsize>(sizeof(double) * plane.size()));
+      }
   }
-  const auto parent = std::filesystem::path(path).parent_path();
-  if (!parent.empty()) std::filesystem::create_directories(parent);
-  std::ofstream f(path, std::ios::binary | std::ios::trunc);
   if (!f) throw ParameterError("cannot write " + path);
-  f.write(o.buf.data(), static_cast<std::streamsize>(o.buf.size()));
 }
 
 bool read_plt_restart(const std::string &path, const Mesh &mesh, const Species &spec, Parameter &parameter,
