@@ -150,7 +150,10 @@ int ostc_driver_get_host_field(const ostc_driver *d, int block, int field, doubl
 /* Driver::initialize_computation (src/Driver.cu:44-104) on the GPU. */
 int ostc_driver_initialize(ostc_driver *d);
 /* Driver::simulate (src/Driver.cu:107-120, 192-289): the steady loop with
-   history.dat, residual_scale.txt, step.txt and flowfield.plt output. */
+   history.dat, residual_scale.txt, step.txt and flowfield.plt output.  The
+   .plt files are written by a host thread while the next steps run (the
+   first output page-locks two staging copies of the output fields); the call
+   returns once every file is written. */
 int ostc_driver_simulate(ostc_driver *d);
 /* n iterations of the steady loop body, no file output.  *err_max receives
    the last normalised residual (or -1 if none was due). */
