@@ -44,8 +44,11 @@ def setup_files(*, dimension: int, total_step: int, output_file: int, output_scr
                 implicit_method: int, dplur_inner_step: int, species: bool, reaction: bool, turbulence: bool,
                 chem_src_method: int = 1, initial: int = 0, convergence: float = 1e-30, reconstruction: int = 2,
                 grid_scale: float = 1.0, inflows: list[dict] | None = None, walls: list[dict] | None = None,
-                default_init: str = "freestream", schmidt: float = 0.5) -> dict[str, list[str]]:
-    """The nine setup files with the keys the reference reads."""
+                default_init: str = "freestream", schmidt: float = 0.5,
+                post_process: list[int] | None = None) -> dict[str, list[str]]:
+    """The nine setup files with the keys the reference reads.  post_process:
+    the reference's post-processing labels (0: skin friction and heat flux of
+    the j = 0 wall of a 2-D case)."""
     inflows = inflows or []
     walls = walls or []
     names = [f["name"] for f in inflows] + [w["name"] for w in walls]
@@ -93,7 +96,8 @@ def setup_files(*, dimension: int, total_step: int, output_file: int, output_scr
             f"bool    turbulence = {int(turbulence)}", f"int     turbulence_method = {1 if turbulence else 0}",
             "int     fluctuate_method = 0", "int     RANS_model = 2", "int     turb_implicit   =   1"],
         "5_boundary_condition.txt": bc,
-        "6_post_process.txt": ["array   int post_process {", "}"],
+        "6_post_process.txt": ["array   int post_process {"] + ([" ".join(map(str, post_process))] if post_process
+                                                                 else []) + ["}"],
         "8_initialization.txt": ["int groups_init = 1", f"string  default_init    =   {default_init}"],
         "9_transport_property.txt": [
             "int diffusivity_method = 1", f"real schmidt_number = {_fmt(float(schmidt))}",
@@ -168,7 +172,7 @@ def _tanh_wall(n: int, first: float, height: float) -> np.ndarray:
 
 
 def ramp_case(case: str | Path, mx: int = 256, my: int = 128, total_step: int = 5000, output_screen: int = 100,
-              output_file: int | None = None) -> Path:
+              output_file: int | None = None, post_process: list[int] | None = None) -> Path:
     """2-D laminar air, Mach 3, p = 2.5 kPa, T = 220 K over a 15 degree
     compression ramp (corner at x = 0.05 m, x in [0, 0.1] m, top at y = 0.03 m),
     first cell 1e-5 m at the isothermal 300 K wall; inflow i = 0, outflow
@@ -194,7 +198,7 @@ def ramp_case(case: str | Path, mx: int = 256, my: int = 128, total_step: int = 
         cfl=0.5, implicit_method=0, dplur_inner_step=3, species=False, reaction=False, turbulence=False,
         inflows=[dict(name="freestream", label=5, temperature=220.0, mach=3.0, pressure=2500.0, u=1.0, v=0.0,
                       w=0.0)],
-        walls=[dict(name="wall", label=2, temperature=300.0)]))
+        walls=[dict(name="wall", label=2, temperature=300.0)], post_process=post_process))
     copy_chemistry(case)
     return case
 

@@ -96,6 +96,11 @@ class Engine {
   virtual void unpin_host(void *p) = 0;
   virtual void record_output_event(int slot) = 0;
   virtual void wait_output_event(int slot) = 0;
+  // Post-processing 0 of the reference (src/PostProcess.cu:6-48): enqueues
+  // the wall skin friction and heat flux of block b (j = 0 wall, mx values
+  // each) and their device-to-host copies into cf / qw; the values are there
+  // once the next output event (or a synchronize) has passed.
+  virtual void wall_friction_heatflux_2d(int b, double dyn_pressure, double *cf, double *qw) = 0;
 };
 
 // Largest grid ostc_driver_residual_noalloc accepts, in residual tiles

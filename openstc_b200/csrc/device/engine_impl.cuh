@@ -138,6 +138,7 @@ class EngineT final : public Engine {
     cudaEventDestroy(ev0_);
     cudaEventDestroy(ev1_);
     for (auto e : out_ev_) cudaEventDestroy(e);
+    cudaFree(d_wall2d_);
     cudaStreamDestroy(stream_);
   }
 
@@ -177,6 +178,19 @@ class EngineT final : public Engine {
   void wait_output_event(int slot) override {
     cuda_check(cudaSetDevice(setup_.device), "cudaSetDevice");
     cuda_check(cudaEventSynchronize(out_ev_[slot & 1]), "output event wait");
+  }
+
+  void wall_friction_heatflux_2d(int b, double dyn_pressure, double *cf, double *qw) override {
+    const int mx = blocks_.at(b).mx;
+    if (!d_wall2d_) {  // once, for the widest block
+      for (const auto &B : blocks_) wall_cap_ = std::max(wall_cap_, B.mx);
+      cuda_check(cudaMalloc(&d_wall2d_, sizeof(double) * 2 * wall_cap_), "cudaMalloc wall2d");
+    }
+    double *dcf = d_wall2d_, *dqw = d_wall2d_ + wall_cap_;
+    k_wall_2d<<<(mx + 127) / 128, 128, 0, stream_>>>(d_blocks_, b, dcf, dqw, dyn_pressure);
+    cuda_check(cudaGetLastError(), "wall_2d launch");
+    cuda_check(cudaMemcpyAsync(cf, dcf, sizeof(double) * mx, cudaMemcpyDeviceToHost, stream_), "wall cf");
+    cuda_check(cudaMemcpyAsync(qw, dqw, sizeof(double) * mx, cudaMemcpyDeviceToHost, stream_), "wall qw");
   }
 
   int64_t field_count(int b, int field) const override {
@@ -793,6 +807,8 @@ class EngineT final : public Engine {
   std::vector<double *> rate_store_;
   cudaEvent_t ev0_{}, ev1_{};
   cudaEvent_t out_ev_[2]{};  // output pipeline slots
+  double *d_wall2d_ = nullptr;  // cf and qw of the 2-D wall post-processing
+  int wall_cap_ = 0;
   double last_ms_ = 0;
 };
 

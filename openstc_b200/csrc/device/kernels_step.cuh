@@ -1280,4 +1280,26 @@ static __global__ void __launch_bounds__(kCta) k_wall_distance(const DevBlock *_
   B.wall_dist[n] = sqrt(wd);
 }
 
+// wall_friction_heatFlux_2d, src/PostProcess.cu:50-73: skin friction and
+// wall heat flux along the j = 0 wall of a 2-D block, at the cells i of the
+// k = 0 plane: cf = mu du_par/dn / q_inf, q_w = lambda dT/dn with the wall
+// normal derivative one-sided over the first cell (|grad eta| spacing).
+static __global__ void __launch_bounds__(128) k_wall_2d(const DevBlock *__restrict__ blks, int b, double *cf,
+                                                       double *qw, double dyn_pressure) {
+  const DevBlock &B = blks[b];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= B.mx) return;
+  const int64_t sz = B.G.size, n0 = B.G.at(i, 0, 0), n1 = B.G.at(i, 1, 0);
+  const double *m = B.metric;
+  const double xi_x = m[n0], xi_y = m[sz + n0];
+  const double eta_x = m[3 * sz + n0], eta_y = m[4 * sz + n0];
+  const double viscosity = B.mul[n0];
+  const double u_parallel_wall = (xi_x * B.bv[sz + n1] + xi_y * B.bv[2 * sz + n1]) / sqrt(xi_x * xi_x + xi_y * xi_y);
+  const double grad_eta = sqrt(eta_x * eta_x + eta_y * eta_y);
+  const double du_normal_wall = u_parallel_wall * grad_eta;
+  cf[i] = viscosity * du_normal_wall / dyn_pressure;
+  const double conductivity = B.cond[n0];
+  qw[i] = conductivity * (B.bv[5 * sz + n1] - B.bv[5 * sz + n0]) * grad_eta;
+}
+
 }  // namespace ostc

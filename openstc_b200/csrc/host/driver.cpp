@@ -26,13 +26,17 @@ namespace ostc {
 // a writer error.
 class PltPipeline {
  public:
+  // wall_dyn_pressure > 0: also the reference's post-processing 0 (skin
+  // friction and heat flux of the j = 0 wall, output/wall/friction_heatflux.dat)
   PltPipeline(Engine &E, const Mesh &mesh, const std::vector<HostField> &field, const Species &spec, bool rans,
-              std::string case_dir)
-      : E_(E), mesh_(mesh), spec_(spec), rans_(rans), dir_(std::move(case_dir)) {
+              std::string case_dir, double wall_dyn_pressure)
+      : E_(E), mesh_(mesh), spec_(spec), rans_(rans), dir_(std::move(case_dir)), wall_q_(wall_dyn_pressure) {
     for (auto &st : slots_) {
       st.field.resize(mesh.n_block);
       st.mach.resize(mesh.n_block);
       st.mut.resize(mesh.n_block);
+      st.cf.resize(mesh.n_block);
+      st.qw.resize(mesh.n_block);
       for (int b = 0; b < mesh.n_block; ++b) {
         HostField &F = st.field[b];
         F.e = field[b].e;
@@ -41,9 +45,13 @@ class PltPipeline {
         F.sv.resize(field[b].sv.size());
         st.mach[b].resize(static_cast<size_t>(F.e.size()));
         if (rans) st.mut[b].resize(static_cast<size_t>(F.e.size()));
+        if (wall_q_ > 0) {
+          st.cf[b].resize(static_cast<size_t>(mesh[b].mx));
+          st.qw[b].resize(static_cast<size_t>(mesh[b].mx));
+        }
         // page-locked, so that the copies do not stall the loop; where the
         // host refuses to lock them the copies are synchronous instead
-        for (auto *v : {&F.bv, &F.sv, &st.mach[b], &st.mut[b]})
+        for (auto *v : {&F.bv, &F.sv, &st.mach[b], &st.mut[b], &st.cf[b], &st.qw[b]})
           if (!v->empty() && E_.pin_host(v->data(), sizeof(double) * v->size())) pinned_.push_back(v->data());
       }
     }
@@ -82,6 +90,7 @@ class PltPipeline {
       if (!F.sv.empty()) E_.get_field_async(b, F_SV, F.sv.data(), static_cast<int64_t>(F.sv.size()));
       E_.get_field_async(b, F_MACH, st.mach[b].data(), static_cast<int64_t>(st.mach[b].size()));
       if (rans_) E_.get_field_async(b, F_MUT, st.mut[b].data(), static_cast<int64_t>(st.mut[b].size()));
+      if (wall_q_ > 0) E_.wall_friction_heatflux_2d(b, wall_q_, st.cf[b].data(), st.qw[b].data());
     }
     E_.record_output_event(s);
     {
@@ -100,10 +109,25 @@ class PltPipeline {
  private:
   struct Slot {
     std::vector<HostField> field;
-    std::vector<std::vector<double>> mach, mut;
+    std::vector<std::vector<double>> mach, mut, cf, qw;
     int step = 0;
     bool busy = false;
   };
+
+  // src/PostProcess.cu:35-42: one file, rewritten for every block in turn
+  // (so a multi-block case keeps the last block's wall), x of the wall
+  // point, cf, q_w, default stream formatting.
+  void write_wall(const Slot &st) const {
+    const std::filesystem::path dir = std::filesystem::path(dir_) / "output" / "wall";
+    std::filesystem::create_directories(dir);
+    for (int b = 0; b < mesh_.n_block; ++b) {
+      std::ofstream f(dir / "friction_heatflux.dat");
+      if (!f) throw ParameterError("cannot write " + (dir / "friction_heatflux.dat").string());
+      f << "variables = \"x\", \"cf\", \"qw\"\n";
+      const Block &blk = mesh_[b];
+      for (int i = 0; i < blk.mx; ++i) f << blk.x(i, 0, 0) << '\t' << st.cf[b][i] << '\t' << st.qw[b][i] << '\n';
+    }
+  }
 
   void rethrow_locked() {
     if (error_) {
@@ -134,6 +158,7 @@ class PltPipeline {
         for (int b = 0; b < mesh_.n_block; ++b)
           blocks[b] = PltBlockData{&mesh_[b], &st.field[b], &st.mach[b], rans_ ? &st.mut[b] : nullptr};
         write_plt(dir_ + "/output/field/flowfield.plt", blocks, spec_, rans_);
+        if (wall_q_ > 0) write_wall(st);
       } catch (...) {
         std::lock_guard<std::mutex> lk(mu_);
         error_ = std::current_exception();
@@ -152,6 +177,7 @@ class PltPipeline {
   const Species &spec_;
   bool rans_;
   std::string dir_;
+  double wall_q_ = 0;  // dynamic pressure of the wall post-processing, 0: off
   Slot slots_[2];
   std::vector<void *> pinned_;
   int next_ = 0;
@@ -462,7 +488,14 @@ void Driver::simulate() {
       }
     }
     if (step % out_file == 0 || converged) {
-      if (!plt_out_) plt_out_ = std::make_unique<PltPipeline>(E, mesh, field, spec, rans, case_dir);
+      if (!plt_out_) {
+        // Driver::post_process, src/Driver.cu:404-415: label 0, the 2-D wall
+        double wall_q = 0;
+        for (int p : parameter.get_int_array("post_process"))
+          if (p == 0)
+            wall_q = 0.5 * parameter.get_real("rho_inf") * parameter.get_real("v_inf") * parameter.get_real("v_inf");
+        plt_out_ = std::make_unique<PltPipeline>(E, mesh, field, spec, rans, case_dir, wall_q);
+      }
       plt_out_->enqueue(step);
     }
   }

@@ -8,7 +8,10 @@ The reference has no CPU path, so this runs on a GPU machine:
 
 Each fixture ``<case>_s<steps>.npz`` holds every variable of the reference's
 output/field/flowfield.plt after <steps> steps (x, y, z dropped) plus the
-history.dat residuals and residual_scale.txt of that run.
+history.dat residuals and residual_scale.txt of that run.  ``ramp_wall_s<steps>.dat``
+is the reference's output/wall/friction_heatflux.dat (post-processing 0: skin
+friction and heat flux along the ramp wall) of the ramp case run with
+post_process = {0}, verbatim.
 """
 from __future__ import annotations
 
@@ -69,6 +72,19 @@ def collect(case: Path) -> dict[str, np.ndarray]:
     return out
 
 
+# the ramp with the reference's 2-D wall post-processing: steps recorded
+WALL_STEPS = (10, 100)
+
+
+def make_wall_fixture(ref: Path, work: Path, out: Path, steps: int) -> None:
+    case = work / f"ramp_wall_s{steps}"
+    if case.exists():
+        shutil.rmtree(case)
+    cases.ramp_case(case, mx=48, my=24, total_step=steps, output_screen=1, output_file=steps, post_process=[0])
+    run_reference(ref, case)
+    shutil.copy(case / "output" / "wall" / "friction_heatflux.dat", out / f"ramp_wall_s{steps}.dat")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=str(ROOT / "oracle" / "_ref" / "openstc_ref"))
@@ -88,6 +104,10 @@ def main() -> None:
             run_reference(Path(a.ref), case)
             np.savez_compressed(out / f"{name}_s{steps}.npz", **collect(case))
             print(f"{name} {steps} steps: ok", flush=True)
+    if not a.only or "ramp_wall" in a.only:
+        for steps in WALL_STEPS:
+            make_wall_fixture(Path(a.ref), work, out, steps)
+            print(f"ramp_wall {steps} steps: ok", flush=True)
 
 
 if __name__ == "__main__":
