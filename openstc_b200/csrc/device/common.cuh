@@ -42,6 +42,11 @@ struct DevParams {
   signed char sf[kMaxReac * kMaxSpec], sb[kMaxReac * kMaxSpec];
   double A[kMaxReac], b[kMaxReac], Ea[kMaxReac], A2[kMaxReac], b2[kMaxReac], Ea2[kMaxReac];
   double lnA[kMaxReac], lnA2[kMaxReac];  // ln |A|, ln |A2| (0 where A is 0): the FP32-bulk path's rates
+  // FP32-bulk path under DPLUR + EPI: ns - 1 when the last species takes
+  // part in no reaction (a third body only, e.g. N2), so that its EPI row and
+  // column are zero; chem_jac / lu_piv then hold only the leading na x na
+  // block (entry (m, q) at m * na + q).  ns everywhere else.
+  int na;
   double tb[kMaxReac * kMaxSpec];
   double troe_a[kMaxReac], troe_t3[kMaxReac], troe_t1[kMaxReac], troe_t2[kMaxReac];
 };

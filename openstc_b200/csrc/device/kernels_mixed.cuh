@@ -438,12 +438,14 @@ __device__ __forceinline__ void chem_cell(const DevBlock &B, int64_t n, int64_t 
     // compute_chem_src_jacobian with the reaction loop outside the species
     // loop: each row m visits only the reactions that change species m once,
     // and every (m, q) entry still sums its terms in reaction order
-    const int nr = cP.nr;
+    const int nr = cP.nr, na = cP.na;
     // 1 / (rho Y_q) once per species (0 below the floor): products, not
     // NS^2 divisions, within an ulp of the FP64 path's quotients
     double inv_rho_y[NS];
     OSTC_UNROLL for (int q = 0; q < NS; ++q) inv_rho_y[q] = Y[q] > 1e-25 ? 1.0 / (density * Y[q]) : 0.0;
+    // only the leading na x na block (the other rows and columns are zero)
     OSTC_UNROLL for (int m = 0; m < NS; ++m) {
+      if (m >= na) break;
       double zz[NS];
       OSTC_UNROLL for (int q = 0; q < NS; ++q) zz[q] = 0;
       for (int r = 0; r < nr; ++r) {
@@ -453,8 +455,9 @@ __device__ __forceinline__ void chem_cell(const DevBlock &B, int64_t n, int64_t 
         OSTC_UNROLL for (int q = 0; q < NS; ++q) zz[q] += dn * (cP.sf[r * NS + q] * a1 - cP.sb[r * NS + q] * a2);
       }
       OSTC_UNROLL for (int q = 0; q < NS; ++q) {
+        if (q >= na) break;
         const double v = zz[q] * inv_rho_y[q];
-        B.chem_jac[(m * NS + q) * sz0 + nz] = cP.mw[m] * v * 1e+3;
+        B.chem_jac[(m * na + q) * sz0 + nz] = cP.mw[m] * v * 1e+3;
       }
     }
   } else if (method == 2) {
@@ -742,6 +745,18 @@ __global__ void __launch_bounds__(kFluxThreads, 4) k_flux_mx_col(const DevBlock 
   }
 }
 
+// EPI solve of a DPLUR sweep with the stored factors of the leading NA x NA
+// block; the trailing species have the single pivot diag, so their solve is
+// rhs / diag, the operation the full factors would do for them.
+template <int NS, int NA>
+__device__ __forceinline__ void epi_solve_block(const DevBlock &B, int64_t nz, int64_t sz0, double diag,
+                                                double *rhs) {
+  int piv[NA];
+  OSTC_UNROLL for (int q = 0; q < NA; ++q) piv[q] = B.lu_piv[q * sz0 + nz];
+  lu_solve_g<NA>(B.chem_jac + nz, sz0, piv, rhs);
+  OSTC_UNROLL for (int l = NA; l < NS; ++l) rhs[l] /= diag;
+}
+
 // DPLUR sweep with FP32 flux-Jacobian products; the update of the point
 // implicit blocks (EPI: stored LU factors) in FP64.  The increments are FP32
 // arrays: reads dqf[in_sel] (neighbours) and dqf[0] (dq0), writes
@@ -821,11 +836,12 @@ __global__ void __launch_bounds__(kCta, 4) k_sweep_mx(const DevBlock *__restrict
       // chemically quiet: the stored factors would be diag I
       OSTC_UNROLL for (int l = 0; l < NS; ++l) out[5 + l] = static_cast<double>(dq0[(5 + l) * szd + nd]) + dt * tot[5 + l] / diag;
     } else if (method == 1) {
-      int piv[NS];
-      OSTC_UNROLL for (int q = 0; q < NS; ++q) piv[q] = B.lu_piv[q * sz0 + nz];
       double rhs[NS];
       OSTC_UNROLL for (int l = 0; l < NS; ++l) rhs[l] = static_cast<double>(tot[5 + l]) * dt;
-      lu_solve_g<NS>(B.chem_jac + nz, sz0, piv, rhs);
+      if (cP.na == NS - 1)
+        epi_solve_block<NS, NS - 1>(B, nz, sz0, diag, rhs);
+      else
+        epi_solve_block<NS, NS>(B, nz, sz0, diag, rhs);
       OSTC_UNROLL for (int l = 0; l < NS; ++l) out[5 + l] = static_cast<double>(dq0[(5 + l) * szd + nd]) + rhs[l];
     } else if (method == 2) {
       OSTC_UNROLL for (int l = 0; l < NS; ++l)

@@ -496,6 +496,23 @@ __global__ void __launch_bounds__(kCta) k_dq0(const DevBlock *__restrict__ blks,
       // no chemistry Jacobian: the factorisation of diag I is diag I, and
       // its solve divides by diag (bit for bit)
       OSTC_UNROLL for (int l = 0; l < NS; ++l) dq[5 + l] /= diag;
+    } else if (method == 1 && C::mixed && cP.na == NS - 1) {
+      // FP32-bulk path: the leading (NS-1) x (NS-1) block, the last species
+      // with its single pivot diag (what the full factorisation gives it)
+      extern __shared__ double sdq[];
+      double *lhs = sdq + threadIdx.x + kTX * (threadIdx.y + kTY * threadIdx.z);
+      constexpr int NA = NS > 1 ? NS - 1 : 1;
+      int piv[NA];
+      OSTC_UNROLL for (int m = 0; m < NA; ++m)
+        OSTC_UNROLL for (int q = 0; q < NA; ++q) {
+          const double J = B.chem_jac[(m * NA + q) * sz0 + nz];
+          lhs[(m * NA + q) * kCta] = (m == q) ? diag - dt * J : -dt * J;
+        }
+      lu_factor<NA, kCta>(lhs, piv);
+      lu_solve<NA, kCta>(lhs, piv, dq + 5);
+      OSTC_UNROLL for (int l = NA; l < NS; ++l) dq[5 + l] /= diag;
+      OSTC_UNROLL for (int q = 0; q < NA * NA; ++q) B.chem_jac[q * sz0 + nz] = lhs[q * kCta];
+      OSTC_UNROLL for (int q = 0; q < NA; ++q) B.lu_piv[q * sz0 + nz] = static_cast<unsigned char>(piv[q]);
     } else if (method == 1) {
       // the matrix lives in this thread's slice of shared memory (stride kCta)
       extern __shared__ double sdq[];

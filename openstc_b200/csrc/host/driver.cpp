@@ -5,6 +5,7 @@
 #include <cstring>
 #include <filesystem>
 #include <fstream>
+#include <algorithm>
 #include <condition_variable>
 #include <deque>
 #include <exception>
@@ -316,6 +317,18 @@ void Driver::build_dev_params() {
       p.sb[r * ns + l] = static_cast<signed char>(reac.stoi_b[r * ns + l]);
       p.tb[r * ns + l] = reac.third_body[r * ns + l];
     }
+  }
+  // FP32-bulk path: when only the last species takes part in no reaction
+  // (a third body only, N2 here), its EPI row and column are zero and the
+  // stored factors drop it
+  p.na = ns;
+  if (opt.precision == 1 && P.get_int("implicit_method") == 1 && P.get_int("chemSrcMethod") == 1) {
+    int last = -1;
+    for (int r = 0; r < p.nr; ++r)
+      for (int l = 0; l < ns; ++l)
+        if (p.sf[r * ns + l] != 0 || p.sb[r * ns + l] != 0) last = std::max(last, l);
+    // the kernels store the block without the last species only
+    if (last + 1 == ns - 1) p.na = ns - 1;
   }
 }
 
