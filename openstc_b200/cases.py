@@ -361,3 +361,28 @@ def multiblock_case(case: str | Path, mxs: list[int], my: int = 64, mz: int = 32
     _mixing_setup(case, total_step=total_step, output_screen=output_screen, output_file=output_file or 10 ** 9,
                   initial=1, cfl=cfl, dplur=dplur, chem=1)
     return case
+
+
+def batched_block_sizes(seed: int, n_blocks: int = 12, lo: tuple[int, int, int] = (32, 32, 32),
+                        hi: tuple[int, int, int] = (160, 96, 64)) -> tuple[list[int], int, int]:
+    """Block sizes of the batched multi-block workload: n_blocks blocks tiled
+    along x with 1:1 faces, so every block shares one (my, mz) and only mx
+    varies; each drawn uniformly between lo and hi from `seed`.  Returns
+    (mxs, my, mz).  With the bounds 32x32x32 .. 160x96x64, twelve blocks hold
+    at most 11.8 M cells."""
+    rng = np.random.default_rng(seed)
+    my = int(rng.integers(lo[1], hi[1] + 1))
+    mz = int(rng.integers(lo[2], hi[2] + 1))
+    mxs = [int(v) for v in rng.integers(lo[0], hi[0] + 1, size=n_blocks)]
+    return mxs, my, mz
+
+
+def batched_multiblock_case(case: str | Path, seed: int = 0, n_blocks: int = 12, total_step: int = 100,
+                            output_screen: int = 10, output_file: int | None = None, dplur: int = 4,
+                            lo: tuple[int, int, int] = (32, 32, 32),
+                            hi: tuple[int, int, int] = (160, 96, 64)) -> Path:
+    """The mixing-layer physics on n_blocks seeded blocks (batched_block_sizes)
+    tiled along x with 1:1 inner faces: the batched multi-block workload."""
+    mxs, my, mz = batched_block_sizes(seed, n_blocks, lo, hi)
+    return multiblock_case(case, mxs, my=my, mz=mz, total_step=total_step, output_screen=output_screen,
+                           output_file=output_file, dplur=dplur)

@@ -155,3 +155,26 @@ def test_restart_reads_fields_by_name(case_factory):
     for l, n in enumerate(["H2", "H", "O2", "O", "OH", "HO2", "H2O2", "H2O", "N2", "tke", "omega"]):
         assert np.array_equal(sv[l, g:-g, g:-g, g:-g], zones[0][n])
     assert d.info().step == 0
+
+
+def test_batched_block_sizes_are_seeded_and_bounded():
+    a = cases.batched_block_sizes(7)
+    assert a == cases.batched_block_sizes(7) and a != cases.batched_block_sizes(8)
+    mxs, my, mz = a
+    assert len(mxs) == 12 and all(32 <= m <= 160 for m in mxs) and 32 <= my <= 96 and 32 <= mz <= 64
+    assert sum(mxs) * my * mz <= 12 * 160 * 96 * 64
+
+
+def test_batched_multiblock_case_reads_as_twelve_tiled_blocks(tmp_path):
+    lo, hi = (5, 5, 4), (9, 7, 5)
+    case = cases.batched_multiblock_case(tmp_path / "b12", seed=3, total_step=1, output_screen=1, lo=lo, hi=hi)
+    mxs, my, mz = cases.batched_block_sizes(3, 12, lo, hi)
+    d = ostc.Driver(case)
+    info = d.info()
+    assert info.n_block == 12
+    assert [d.dims(b) for b in range(12)] == [(m, my, mz) for m in mxs]
+    # two inner faces per shared plane, each naming its neighbour
+    faces = d.inner_faces()
+    assert len(faces) == 22
+    assert sorted((f.block, f.target_block) for f in faces) == sorted(
+        [(b, b + 1) for b in range(11)] + [(b + 1, b) for b in range(11)])
