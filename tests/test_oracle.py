@@ -80,3 +80,47 @@ def test_oracle_matches_reference_program(case_factory, name, steps):
     tol = 1e-10
     bad = {k: v for k, v in worst.items() if not v <= tol}
     assert not bad, f"beyond {tol}: {bad}"
+
+
+def wall_friction_heatflux_2d(bv, mul, cond, metric, dyn_pressure, g):
+    """Restatement of wall_friction_heatFlux_2d (src/PostProcess.cu:50-73) on
+    ghosted arrays (component, k, j, i): skin friction and wall heat flux at
+    the j = 0 points of the k = 0 plane."""
+    k0, j0, j1 = g, g, g + 1
+    sl = slice(g, -g)
+    xi_x, xi_y = metric[0, k0, j0, sl], metric[1, k0, j0, sl]
+    eta_x, eta_y = metric[3, k0, j0, sl], metric[4, k0, j0, sl]
+    u_parallel = (xi_x * bv[1, k0, j1, sl] + xi_y * bv[2, k0, j1, sl]) / np.sqrt(xi_x * xi_x + xi_y * xi_y)
+    grad_eta = np.sqrt(eta_x * eta_x + eta_y * eta_y)
+    cf = mul[k0, j0, sl] * (u_parallel * grad_eta) / dyn_pressure
+    qw = cond[k0, j0, sl] * (bv[5, k0, j1, sl] - bv[5, k0, j0, sl]) * grad_eta
+    return cf, qw
+
+
+def test_wall_postprocess_restatement_matches_reference_program(case_factory):
+    """The 2-D wall post-processing formula applied to the oracle's fields
+    after 10 steps of the 48x24 ramp reproduces the reference program's own
+    output/wall/friction_heatflux.dat (tests/golden/ramp_wall_s10.dat) to the
+    six significant digits it writes."""
+    fix = GOLDEN / "ramp_wall_s10.dat"
+    if not fix.exists():
+        pytest.skip(f"no reference fixture {fix.name}")
+    lines = fix.read_text().splitlines()
+    assert lines[0] == 'variables = "x", "cf", "qw"'
+    gold = np.array([[float(v) for v in ln.split("\t")] for ln in lines[1:]])
+    case = case_factory("ramp", cases.ramp_case, mx=48, my=24, total_step=10, output_screen=1, output_file=10)
+    s, _ = run(case, 10, threads=4)
+    g = s.info.ngg
+    mx, my, mz = s.dims[0]
+    shp = (mz + 2 * g, my + 2 * g, mx + 2 * g)
+    # freestream of the ramp: air at Mach 3, 220 K, 2.5 kPa
+    r_air = 8314.462618 / 28.9647
+    rho_inf, v_inf = 2500.0 / (r_air * 220.0), 3.0 * np.sqrt(1.4 * r_air * 220.0)
+    cf, qw = wall_friction_heatflux_2d(s.get(0, "bv", (6,) + shp), s.get(0, "mul", shp),
+                                       s.get(0, "conductivity", shp), s.get(0, "metric", (9,) + shp),
+                                       0.5 * rho_inf * v_inf * v_inf, g)
+    x = s.get(0, "x", shp)[g, g, g:-g]
+    ours = np.stack([x, cf, qw], axis=1)
+    assert ours.shape == gold.shape == (48, 3)
+    scale = np.abs(gold).max(axis=0)
+    assert np.all(np.abs(ours - gold) <= 1e-5 * np.abs(gold) + 1e-12 * scale)
