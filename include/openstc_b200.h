@@ -266,17 +266,21 @@ int ostc_driver_set_surrogate(ostc_driver *d, ostc_surrogate *s);
 int ostc_driver_chemistry_stats(ostc_driver *d, long long *accepted, long long *fallback, long long *evaluated);
 
 /* No counterpart in the reference.  Recomputes, from the device state, the
-   normalised residuals of rho, |V|, p, T of the last step that stored its
-   previous state (every output_screen-th step; the same values
-   ostc_driver_residual returns right after such a step), without allocating
-   any device memory: the reduction runs in a static 2 MiB device scratch.
-   For callers that must not allocate, such as a convergence monitor polling
-   a solver whose flow state fills the device.  Limit: grids of at most
-   65536 tiles of 32x4x1 cells (8,388,608 interior cells); larger grids get
-   OSTC_ERR_INPUT.  The first call on a device performs set-up (the scratch's
-   address is looked up once) and should come before any stream capture on
-   that device.  One scratch per device: overlapping calls on the same device
-   race; serialise them.  Requires at least one step (OSTC_ERR_STATE). */
+   normalised residuals of rho, |V|, p, T of the last step, without allocating
+   any device memory: the reduction runs in a static 8 MiB device scratch.
+   Valid only right after a step that computed a residual (step 1 and every
+   output_screen-th step, which store the previous state on the device; the
+   same values ostc_driver_residual returns then); after any other step it
+   returns OSTC_ERR_STATE.  For callers that must not allocate, such as a
+   convergence monitor polling a solver whose flow state fills the device.
+   Limit: grids of at most 262144 tiles of 32x4x1 cells (33,554,432 interior
+   cells); larger grids get OSTC_ERR_INPUT.  The first successful call on a
+   device performs set-up (the scratch's address is looked up and cached; a
+   failed look-up is retried by the next call) and should come before any
+   stream capture on that device.  The driver's device is made current for
+   the call and the caller's device restored.  One scratch per device:
+   overlapping calls on the same device race; serialise them.  Requires at
+   least one step (OSTC_ERR_STATE). */
 int ostc_driver_residual_noalloc(ostc_driver *d, double res[4]);
 
 #ifdef __cplusplus

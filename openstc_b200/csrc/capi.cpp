@@ -267,6 +267,10 @@ int ostc_driver_residual_noalloc(ostc_driver *d, double res[4]) {
   if (!d || !res) return fail(OSTC_ERR_INPUT, "null argument");
   if (!d->drv.initialized()) return fail(OSTC_ERR_STATE, "initialize first");
   if (d->drv.step < 1) return fail(OSTC_ERR_STATE, "no step taken yet: the residual scale is set at step 1");
+  if (!d->drv.last_step_residual)
+    return fail(OSTC_ERR_STATE, "step " + std::to_string(d->drv.step) +
+                                    " computed no residual (only step 1 and every output_screen-th step do): the "
+                                    "device no longer holds the state before it");
   return guarded([&]() -> int {
     ostc::Engine &E = d->drv.engine();
     double raw[4] = {0, 0, 0, 0};
@@ -275,7 +279,7 @@ int ostc_driver_residual_noalloc(ostc_driver *d, double res[4]) {
     if (st == 1)
       return fail(OSTC_ERR_INPUT, "ostc_driver_residual_noalloc: the grid has " + std::to_string(E.residual_tiles()) +
                                       " residual tiles (32x4x1 cells); the static scratch holds at most " +
-                                      std::to_string(ostc::kNoAllocMaxTiles) + " (8388608 interior cells)");
+                                      std::to_string(ostc::kNoAllocMaxTiles) + " (33554432 interior cells)");
     if (st != 0) return fail(OSTC_ERR_CUDA, std::string("CUDA error in ostc_driver_residual_noalloc: ") + why);
     // the normalisation of Driver::compute_residual, without touching its state
     const double n = static_cast<double>(d->drv.mesh.n_grid_total);

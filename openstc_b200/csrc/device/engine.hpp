@@ -104,14 +104,17 @@ class Engine {
 };
 
 // Largest grid ostc_driver_residual_noalloc accepts, in residual tiles
-// (65536 tiles x 128 cells = 8,388,608 interior cells); its static device
-// scratch holds 4 partial sums per tile plus the 4 totals (2 MiB + 32 B).
-constexpr int kNoAllocMaxTiles = 65536;
+// (262144 tiles x 128 cells = 33,554,432 interior cells; the 512x256x224 grid
+// has 229,376); its static device scratch holds 4 partial sums per tile plus
+// the 4 totals (8 MiB + 32 B).
+constexpr int kNoAllocMaxTiles = 262144;
 
 // The residual of the last stored step through the static device scratch of
-// residual_noalloc.cu, with no device allocation.  raw receives the four
+// residual_noalloc.cu, with no device allocation; `device` is made current
+// for the launches and the caller's device restored.  raw receives the four
 // sums.  Returns 0; 1 when the grid has more than kNoAllocMaxTiles tiles;
-// 2 on a CUDA error (*why: the runtime's static message).
+// 2 on a CUDA error (*why: the error's message, valid until the next call on
+// this host thread).
 int residual_sums_noalloc(Engine &engine, int device, double raw[4], const char **why);
 
 std::unique_ptr<Engine> make_engine(const EngineSetup &setup);

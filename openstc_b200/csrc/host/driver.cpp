@@ -462,8 +462,10 @@ double Driver::advance(int n) {
     const bool store = step % screen == 0;
     const bool due = store || step == 1;
     double raw[4] = {0, 0, 0, 0};
+    last_step_residual = false;
     E.step(store, due, raw);
     if (due) err = compute_residual(step, raw);
+    last_step_residual = due;
   }
   E.synchronize();
   return err;
@@ -484,7 +486,9 @@ void Driver::simulate() {
     const bool store = step % screen == 0;
     const bool due = store || step == 1;
     double raw[4] = {0, 0, 0, 0};
+    last_step_residual = false;
     E.step(store, due, raw);
+    last_step_residual = due;
     if (due) {
       const double err_max = compute_residual(step, raw);
       converged = err_max < criteria;

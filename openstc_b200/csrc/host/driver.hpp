@@ -58,6 +58,10 @@ class Driver {
   std::vector<HostInner> host_inner;
   std::vector<double> wall_points;
   int step = 0;
+  // whether step `step` computed a residual (step 1 and every
+  // output_screen-th step): only then does bv_last hold that step's previous
+  // state, so that the residual can be recomputed from the device
+  bool last_step_residual = false;
   std::array<double, 4> res{1, 1, 1, 1}, res_scale{1, 1, 1, 1};
   bool rans = false;
   int mix = 0;

@@ -52,3 +52,26 @@ def test_noalloc_residual_needs_a_step(case_factory):
     d.initialize()
     with pytest.raises(ostc.OstcError, match="no step taken yet"):
         d.residual_noalloc()
+
+
+def test_noalloc_residual_only_after_a_residual_step(case_factory):
+    """With output_screen = 5 the previous state is stored at steps 5, 10, ...
+    only.  Right after step 5 the recomputed residual equals the driver's;
+    after step 7 the device holds the state of step 4 as the previous one, so
+    the entry point refuses instead of returning a residual over three steps."""
+    case = case_factory("zz_ml_s5", cases.mixing_layer_case, mx=16, my=12, mz=6, total_step=20, output_screen=5,
+                        output_file=20)
+    d = ostc.Driver(case)
+    d.initialize()
+    d.step(1)
+    assert close(d.residual_noalloc(), d.residual())  # step 1 computes a residual too
+    d.step(4)
+    ref = d.residual()
+    assert close(d.residual_noalloc(), ref), (d.residual_noalloc(), ref)
+    d.step(2)
+    with pytest.raises(ostc.OstcError, match="computed no residual"):
+        d.residual_noalloc()
+    d.step(3)  # step 10 stores again
+    ref10 = d.residual()
+    assert close(d.residual_noalloc(), ref10), (d.residual_noalloc(), ref10)
+    assert not np.array_equal(ref10, ref)
