@@ -225,57 +225,203 @@ def _mixing_setup(case, *, total_step, output_screen, output_file, initial, cfl,
         chem_src_method=chem, initial=initial, inflows=[UPPER, LOWER]))
 
 
-def _blend_initial_field(case: Path, delta: float = 5e-4) -> None:
+RU = 8314.462618  # J/(kmol K), src/Constants.h:18
+
+# Standard atomic weights of the elements a mechanism here names, as the
+# reference tabulates them (src/Element.cpp:13-166).
+_ATOMIC_WEIGHT = {"H": 1.008, "HE": 4.002602, "C": 12.011, "N": 14.007, "O": 15.999, "AR": 39.95}
+
+
+def _mixture_data(case: Path) -> dict:
+    """Molecular weights, NASA-7 coefficients and Lennard-Jones viscosity data
+    of the mechanism's species, read from the case's therm.dat and tran.dat
+    the way the reference's reader does (src/ChemData.cpp:138-293): the first
+    record of a species wins; name in columns 1-18, element counts in four
+    5-column fields from column 25, T_low / T_high / T_mid in 10-column fields
+    from column 46; three lines of 15-column coefficients (high set first)."""
+    chem = Path(case) / "input_files" / "chemistry"
+    species = _species_names(case)
+    idx = {n: i for i, n in enumerate(species)}
+    ns = len(species)
+    mw = [0.0] * ns
+    t_low, t_mid = [300.0] * ns, [1000.0] * ns
+    low, high = [[0.0] * 7 for _ in range(ns)], [[0.0] * 7 for _ in range(ns)]
+    lines = (chem / "therm.dat").read_text().splitlines()
+    seen = set()
+    i = 2  # THERMO, then the global temperature line
+    while i < len(lines):
+        line = lines[i]
+        key = line[:18].split()[0].upper() if line[:18].split() else ""
+        if key.startswith("END") or key.startswith("REAC") or key.startswith("TRAN"):
+            break
+        if key not in idx or key in seen:
+            i += 4
+            continue
+        sp = idx[key]
+        t_low[sp] = float(line[45:55])
+        tm = line[65:75].split()
+        if tm:
+            t_mid[sp] = float(tm[0])
+        comp = {}
+        for e in range(4):
+            f = line[24 + 5 * e: 29 + 5 * e].strip()
+            if not f or f[0] == "0":
+                break
+            el, cnt = f.split()[0].upper(), int(f.split()[1])
+            comp[el] = cnt
+        w = 0.0
+        for el in sorted(comp):  # the reference sums over its std::map of elements
+            w += _ATOMIC_WEIGHT[el] * comp[el]
+        mw[sp] = w
+        c = []
+        for r in range(3):
+            row = lines[i + 1 + r]
+            c += [float(row[15 * q: 15 * q + 15]) for q in range(4 if r == 2 else 5)]
+        high[sp] = c[0:7]
+        low[sp] = c[7:14]
+        seen.add(key)
+        i += 4
+    lj_inv, vis_coeff = [0.0] * ns, [0.0] * ns
+    for line in (chem / "tran.dat").read_text().splitlines():
+        parts = line.split()
+        if not parts or parts[0][0] == "!":
+            continue
+        name = parts[0].upper()
+        if name in idx and vis_coeff[idx[name]] == 0.0:
+            sp = idx[name]
+            eps_k, sigma = float(parts[2]), float(parts[3])
+            lj_inv[sp] = 1.0 / eps_k
+            vis_coeff[sp] = 2.6693e-6 * math.sqrt(mw[sp]) / (sigma * sigma)
+    return {"species": species, "mw": mw, "t_low": t_low, "t_mid": t_mid, "low": low, "high": high,
+            "lj_inv": lj_inv, "vis_coeff": vis_coeff}
+
+
+def inflow_state(case: Path, bc: dict) -> dict:
+    """The primitive state of an inflow boundary condition of a 9-species
+    k-omega SST case as the reference computes it (src/BoundCond.cpp:8-109):
+    mass fractions as given, W = 1/sum(Y/W_k), mixture viscosity by Wilke's
+    rule over Chapman-Enskog species viscosities (src/Transport.cu:11-38),
+    gamma from the NASA-7 cp (cp/cv), velocity = Mach x speed of sound,
+    density from the ideal gas, tke = 1.5 (TI |V|)^2, mu_t = ratio x mu,
+    omega = rho tke / mu_t.  Returns u, v, w, density, pressure, temperature,
+    sv (ns mass fractions, tke, omega) and mut."""
+    m = _mixture_data(case)
+    ns = len(m["species"])
+    mw_k = m["mw"]
+    Y = [0.0] * ns
+    for name, y in bc.get("Y", {}).items():
+        Y[m["species"].index(name.upper())] = float(y)
+    inv = 0.0
+    for k in range(ns):
+        inv += Y[k] / mw_k[k]
+    mw = 1.0 / inv
+    T, p = float(bc["temperature"]), float(bc["pressure"])
+    x = [Y[k] * mw / mw_k[k] for k in range(ns)]
+    mu = []
+    for k in range(ns):
+        tdl = T * m["lj_inv"][k]
+        om = 1.147 * math.pow(tdl, -0.145) + math.pow(tdl + 0.5, -2)
+        mu.append(m["vis_coeff"][k] * math.sqrt(T) / om)
+    visc = 0.0
+    for i in range(ns):
+        den = 0.0
+        for j in range(ns):
+            if i == j:
+                phi = 1.0
+            else:
+                num = 1 + math.sqrt(mu[i] / mu[j]) * math.pow(mw_k[j] / mw_k[i], 0.25)
+                phi = num * num * (1.0 / math.sqrt(8 * (1 + mw_k[i] / mw_k[j])))
+            den += phi * x[j]
+        visc += mu[i] * x[i] / den
+    cp = cv = 0.0
+    t2 = T * T
+    t3 = t2 * T
+    t4 = t3 * T
+    for k in range(ns):
+        if T < m["t_low"][k]:
+            tt = m["t_low"][k]
+            tt2 = tt * tt
+            tt3 = tt2 * tt
+            c = m["low"][k]
+            cpk = c[0] + c[1] * tt + c[2] * tt2 + c[3] * tt3 + c[4] * (tt3 * tt)
+        else:
+            c = m["low"][k] if T < m["t_mid"][k] else m["high"][k]
+            cpk = c[0] + c[1] * T + c[2] * t2 + c[3] * t3 + c[4] * t4
+        cpk *= RU / mw_k[k]
+        cp += Y[k] * cpk
+        cv += Y[k] * (cpk - RU / mw_k[k])
+    gamma = cp / cv
+    vel = float(bc["mach"]) * math.sqrt(gamma * RU / mw * T)
+    rho = p * mw / (RU * T)
+    mut = float(bc.get("mut_ratio", 1.0)) * visc
+    tke = 1.5 * vel * vel * float(bc.get("ti", 0.01)) * float(bc.get("ti", 0.01))
+    sv = Y + [tke, rho * tke / mut]
+    return {"u": float(bc["u"]) * vel, "v": float(bc["v"]) * vel, "w": float(bc["w"]) * vel, "density": rho,
+            "pressure": p, "temperature": T, "sv": sv, "mut": mut, "mw": mw_k}
+
+
+def _read_grid(case: Path) -> list[tuple[np.ndarray, np.ndarray, np.ndarray]]:
+    """The blocks' (x, y, z) of the case's grid file, shape (mz, my, mx) each."""
+    tok = (Path(case) / "input_files" / "grid" / "grid   0.grd").read_text().split()
+    nb = int(tok[0])
+    dims = [tuple(int(v) for v in tok[1 + 3 * b: 4 + 3 * b]) for b in range(nb)]
+    pos = 1 + 3 * nb
+    vals = np.array(tok[pos:], dtype=np.float64)
+    out, o = [], 0
+    for mx, my, mz in dims:
+        n = mx * my * mz
+        xyz = [vals[o + q * n: o + (q + 1) * n].reshape(mz, my, mx) for q in range(3)]
+        o += 3 * n
+        out.append(tuple(xyz))
+    return out
+
+
+def _blend_initial_field(case: Path, delta: float = 5e-4, spikes: list[tuple[int, int, int, float]] | None = None,
+                         ) -> None:
     """Writes output/field/flowfield.plt with a tanh blend (thickness delta)
-    of the two inflow states across y = 0.025 m, plus step.txt and
-    residual_scale.txt, so that a run with initial = 1 starts from it."""
-    from . import Driver
+    of the two inflow states (UPPER and LOWER) across y = 0.025 m, plus
+    step.txt and residual_scale.txt, so that a run with initial = 1 starts
+    from it.  spikes: (i, j, k, factor) cells of block 0 whose density and
+    pressure are multiplied by factor (same temperature), to put unphysical
+    states in front of limit_flow.  Pure NumPy: generating a case loads no
+    native library."""
     from .plt import write_plt
 
-    drv = Driver(case)
-    try:
-        info = drv.info()
-        prm = drv.params()
-        # the two inflow states: the cold stream is the lower one
-        inflow = [b for b in drv.bcs() if b.type == 5]
-        ns, nsc = info.n_spec, info.n_scalar
-        species = _species_names(case)
-        by_t = sorted(inflow, key=lambda b: b.temperature)
-        lo, up = by_t[0], by_t[-1]
-        names = ["x", "y", "z", "density", "u", "v", "w", "pressure", "temperature", "mach"] + species + [
-            "tke", "omega", "mut"]
-        zones = []
-        for blk in range(info.n_block):
-            x = drv.host_field(blk, "x")[0]
-            y = drv.host_field(blk, "y")[0]
-            z = drv.host_field(blk, "z")[0]
-            g = info.ngg
-            x, y, z = x[g:-g, g:-g, g:-g], y[g:-g, g:-g, g:-g], z[g:-g, g:-g, g:-g]
-            phi = 0.5 * (1.0 + np.tanh((y - 0.025) / delta))
-            mix = lambda a, b: phi * b + (1.0 - phi) * a  # noqa: E731
-            zone = {"x": x, "y": y, "z": z}
-            zone["u"] = mix(lo.u, up.u)
-            zone["v"] = np.zeros_like(x)
-            zone["w"] = np.zeros_like(x)
-            zone["pressure"] = np.full_like(x, up.pressure)
-            zone["temperature"] = mix(lo.temperature, up.temperature)
-            Y = [mix(lo.sv[l], up.sv[l]) for l in range(ns)]
-            mw = 1.0 / sum(Y[l] / prm.mw[l] for l in range(ns))
-            zone["density"] = zone["pressure"] * mw / (8314.462618 * zone["temperature"])
-            zone["mach"] = np.zeros_like(x)
-            for l, n in enumerate(species):
-                zone[n] = Y[l]
-            zone["tke"] = mix(lo.sv[ns], up.sv[ns])
-            zone["omega"] = mix(lo.sv[ns + 1], up.sv[ns + 1])
-            zone["mut"] = mix(lo.mut, up.mut)
-            zones.append(zone)
-        write_plt(case / "output" / "field" / "flowfield.plt", names, zones)
-        msg = case / "output" / "message"
-        msg.mkdir(parents=True, exist_ok=True)
-        (msg / "step.txt").write_text("0")
-        (msg / "residual_scale.txt").write_text("1\n1\n1\n1\n")
-    finally:
-        drv.close()
+    up, lo = inflow_state(case, UPPER), inflow_state(case, LOWER)
+    species = _species_names(case)
+    ns = len(species)
+    mw_k = up["mw"]
+    names = ["x", "y", "z", "density", "u", "v", "w", "pressure", "temperature", "mach"] + species + [
+        "tke", "omega", "mut"]
+    zones = []
+    for x, y, z in _read_grid(case):
+        phi = 0.5 * (1.0 + np.tanh((y - 0.025) / delta))
+        mix = lambda a, b: phi * b + (1.0 - phi) * a  # noqa: E731
+        zone = {"x": x, "y": y, "z": z}
+        zone["u"] = mix(lo["u"], up["u"])
+        zone["v"] = np.zeros_like(x)
+        zone["w"] = np.zeros_like(x)
+        zone["pressure"] = np.full_like(x, up["pressure"])
+        zone["temperature"] = mix(lo["temperature"], up["temperature"])
+        Y = [mix(lo["sv"][l], up["sv"][l]) for l in range(ns)]
+        mw = 1.0 / sum(Y[l] / mw_k[l] for l in range(ns))
+        zone["density"] = zone["pressure"] * mw / (RU * zone["temperature"])
+        zone["mach"] = np.zeros_like(x)
+        for l, n in enumerate(species):
+            zone[n] = Y[l]
+        zone["tke"] = mix(lo["sv"][ns], up["sv"][ns])
+        zone["omega"] = mix(lo["sv"][ns + 1], up["sv"][ns + 1])
+        zone["mut"] = mix(lo["mut"], up["mut"])
+        if spikes and not zones:
+            for i, j, k, f in spikes:
+                zone["density"][k, j, i] *= f
+                zone["pressure"][k, j, i] *= f
+        zones.append(zone)
+    write_plt(case / "output" / "field" / "flowfield.plt", names, zones)
+    msg = case / "output" / "message"
+    msg.mkdir(parents=True, exist_ok=True)
+    (msg / "step.txt").write_text("0")
+    (msg / "residual_scale.txt").write_text("1\n1\n1\n1\n")
 
 
 def _species_names(case: Path) -> list[str]:
@@ -290,12 +436,15 @@ def _species_names(case: Path) -> list[str]:
 
 def mixing_layer_case(case: str | Path, mx: int = 384, my: int = 192, mz: int = 64, total_step: int = 2000,
                       output_screen: int = 100, output_file: int | None = None, cfl: float = 0.5,
-                      dplur: int = 4, chem: int = 1, implicit: int = 1) -> Path:
+                      dplur: int = 4, chem: int = 1, implicit: int = 1,
+                      spikes: list[tuple[int, int, int, float]] | None = None) -> Path:
     """3-D supersonic H2 / vitiated-air mixing layer (0.3 x 0.05 x 0.02 m,
     y clustered at the splitter y = 0.025 m).  Upper stream Mach 2.4, 1250 K,
     Y_O2 0.245, Y_H2O 0.175, N2; lower stream H2 / N2 (0.4 / 0.6) at
     Mach 1.2, 300 K; 1 atm; 9 species / 19 reactions, k-omega SST with 1 %
-    inflow turbulence, DPLUR with `dplur` sweeps, EPI chemistry."""
+    inflow turbulence, DPLUR with `dplur` sweeps, chemistry treatment `chem`
+    (1 point-implicit EPI, 2 diagonal).  spikes: cells whose initial density
+    and pressure are scaled (see _blend_initial_field)."""
     case = Path(case)
     x, y, z = _mixing_layer_grid(mx, my, mz)
     write_grid(case, [(x, y, z)])
@@ -312,7 +461,7 @@ def mixing_layer_case(case: str | Path, mx: int = 384, my: int = 192, mz: int = 
     copy_chemistry(case)
     _mixing_setup(case, total_step=total_step, output_screen=output_screen, output_file=output_file or 10 ** 9,
                   initial=0, cfl=cfl, dplur=dplur, chem=chem, implicit=implicit)
-    _blend_initial_field(case)
+    _blend_initial_field(case, spikes=spikes)
     _mixing_setup(case, total_step=total_step, output_screen=output_screen, output_file=output_file or 10 ** 9,
                   initial=1, cfl=cfl, dplur=dplur, chem=chem, implicit=implicit)
     return case

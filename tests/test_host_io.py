@@ -178,3 +178,38 @@ def test_batched_multiblock_case_reads_as_twelve_tiled_blocks(tmp_path):
     assert len(faces) == 22
     assert sorted((f.block, f.target_block) for f in faces) == sorted(
         [(b, b + 1) for b in range(11)] + [(b + 1, b) for b in range(11)])
+
+
+def test_numpy_inflow_state_equals_the_library_reader(tmp_path):
+    """The case generator restates the inflow state in NumPy (so that writing
+    a case loads no native library); it must equal what the library's own
+    boundary-condition reader computes from the same files, bit for bit."""
+    case = cases.mixing_layer_case(tmp_path / "ml", mx=8, my=6, mz=4, total_step=1)
+    drv = ostc.Driver(case)
+    prm = drv.params()
+    by_t = sorted([b for b in drv.bcs() if b.type == 5], key=lambda b: b.temperature)
+    ns = drv.info().n_spec
+    for lib, spec in ((by_t[0], cases.LOWER), (by_t[-1], cases.UPPER)):
+        st = cases.inflow_state(case, spec)
+        for k in ("density", "u", "v", "w", "pressure", "temperature", "mut"):
+            assert st[k] == getattr(lib, k), (k, st[k], getattr(lib, k))
+        assert st["sv"] == [lib.sv[l] for l in range(ns + 2)]
+        assert st["mw"] == [prm.mw[l] for l in range(ns)]
+    drv.close()
+
+
+def test_blended_initial_field_reads_back(tmp_path):
+    """The tanh-blended restart file: the two streams far from the splitter,
+    and the grid of the case's own grid file."""
+    case = cases.mixing_layer_case(tmp_path / "ml", mx=8, my=24, mz=4, total_step=1)
+    from openstc_b200.plt import read_plt
+
+    names, zones = read_plt(case / "output" / "field" / "flowfield.plt")
+    z = zones[0]
+    up, lo = cases.inflow_state(case, cases.UPPER), cases.inflow_state(case, cases.LOWER)
+    assert np.allclose(z["temperature"][:, -1, :], up["temperature"], rtol=1e-12)
+    assert np.allclose(z["temperature"][:, 0, :], lo["temperature"], rtol=1e-12)
+    assert np.allclose(z["u"][:, -1, :], up["u"], rtol=1e-12)
+    assert np.allclose(z["H2"][:, 0, :], 0.4, rtol=1e-12)
+    grid = cases._read_grid(case)[0]
+    assert np.array_equal(z["y"], grid[1])
