@@ -87,3 +87,43 @@ def has_gpu() -> bool:
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+def err_max_history(rms_by_step: dict) -> dict:
+    """{step: err_max} from the RMS one-step changes of (rho, |V|, p, T) of
+    each residual step, the way Driver::compute_residual forms it
+    (src/Driver.cu:345-380): normalised by the step-1 values (floored at
+    1e-20), then the first one unless a later one is larger in magnitude."""
+    out, scale = {}, None
+    for step in sorted(rms_by_step):
+        res = np.asarray(rms_by_step[step], dtype=np.float64)
+        if step == 1:
+            scale = np.maximum(res, 1e-20)
+        res = res / scale
+        e = res[0]
+        for l in range(1, 4):
+            if abs(res[l]) > e:
+                e = res[l]
+        out[step] = float(e)
+    return out
+
+
+def history_mismatch(ours: dict, gold_rows, rel: float = 1e-9) -> list:
+    """Steps whose err_max differs from the reference's history.dat line.  The
+    reference prints %11.4e (five significant digits), so a value matches
+    when it lies within half a unit of that last digit of the printed value
+    (plus `rel` of it, for rounding at a digit boundary)."""
+    bad = []
+    gold = {int(r[0]): float(r[1]) for r in gold_rows}
+    if set(gold) != set(ours):
+        return [("steps", sorted(set(gold) ^ set(ours)))]
+    for step, g in gold.items():
+        v = ours[step]
+        if g == 0.0:
+            ok = abs(v) < 5e-5 * 1e-300
+        else:
+            unit = 10.0 ** (np.floor(np.log10(abs(g))) - 4)
+            ok = abs(v - g) <= 0.5 * unit + rel * abs(g)
+        if not ok:
+            bad.append((step, v, g))
+    return bad

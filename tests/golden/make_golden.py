@@ -8,7 +8,10 @@ The reference has no CPU path, so this runs on a GPU machine:
 
 Each fixture ``<case>_s<steps>.npz`` holds every variable of the reference's
 output/field/flowfield.plt after <steps> steps (x, y, z dropped) plus the
-history.dat residuals and residual_scale.txt of that run.  ``ramp_wall_s<steps>.dat``
+history.dat residuals and residual_scale.txt of that run; the one-step
+fixtures also keep the raw bytes of that flowfield.plt (``plt_raw``), which
+the library must reproduce byte for byte.  The cases are listed in
+tests/fixture_cases.py.  ``ramp_wall_s<steps>.dat``
 is the reference's output/wall/friction_heatflux.dat (post-processing 0: skin
 friction and heat flux along the ramp wall) of the ramp case run with
 post_process = {0}, verbatim.
@@ -29,14 +32,8 @@ sys.path.insert(0, str(ROOT))
 from openstc_b200 import cases  # noqa: E402
 from openstc_b200.plt import read_plt  # noqa: E402
 
-# name -> (builder, kwargs, steps recorded)
-CASES = {
-    "ramp": (cases.ramp_case, dict(mx=48, my=24), (1, 10, 100)),
-    "ml": (cases.mixing_layer_case, dict(mx=16, my=12, mz=6), (1, 10, 100)),
-    "ml_explicit": (cases.mixing_layer_case, dict(mx=16, my=12, mz=6, implicit=0), (1, 10)),
-    "mb": (cases.multiblock_case, dict(mxs=[10, 8], my=12, mz=6), (1, 10)),
-}
-
+sys.path.insert(0, str(ROOT / "tests"))
+from fixture_cases import FIXTURES as CASES  # noqa: E402
 
 def build_case(name: str, where: Path, steps: int) -> Path:
     fn, kw, _ = CASES[name]
@@ -53,7 +50,7 @@ def run_reference(ref: Path, case: Path) -> None:
         raise RuntimeError(f"reference run failed in {case}:\n{res.stdout[-2000:]}\n{res.stderr[-2000:]}")
 
 
-def collect(case: Path) -> dict[str, np.ndarray]:
+def collect(case: Path, keep_raw: bool = False) -> dict[str, np.ndarray]:
     names, zones = read_plt(case / "output" / "field" / "flowfield.plt")
     out: dict[str, np.ndarray] = {}
     for z, zone in enumerate(zones):
@@ -69,6 +66,8 @@ def collect(case: Path) -> dict[str, np.ndarray]:
     out["history"] = np.array(rows) if rows else np.zeros((0, 2))
     out["residual_scale"] = np.array([float(v) for v in (case / "output" / "message" / "residual_scale.txt")
                                       .read_text().split()])
+    if keep_raw:
+        out["plt_raw"] = np.frombuffer((case / "output" / "field" / "flowfield.plt").read_bytes(), dtype=np.uint8)
     return out
 
 
@@ -102,7 +101,7 @@ def main() -> None:
         for steps in steps_list:
             case = build_case(name, work, steps)
             run_reference(Path(a.ref), case)
-            np.savez_compressed(out / f"{name}_s{steps}.npz", **collect(case))
+            np.savez_compressed(out / f"{name}_s{steps}.npz", **collect(case, keep_raw=steps == 1))
             print(f"{name} {steps} steps: ok", flush=True)
     if not a.only or "ramp_wall" in a.only:
         for steps in WALL_STEPS:

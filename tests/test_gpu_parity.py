@@ -14,17 +14,15 @@ import pytest
 
 import openstc_b200 as ostc
 from openstc_b200 import cases
-from conftest import GOLDEN, rel_err, scaled_err
+from conftest import GOLDEN, history_mismatch, rel_err, scaled_err
 from oracle_bridge import OracleSolver, interior
 
 pytestmark = pytest.mark.gpu
 
-CASES = {
-    "ramp": (cases.ramp_case, dict(mx=48, my=24)),
-    "ml": (cases.mixing_layer_case, dict(mx=16, my=12, mz=6)),
-    "ml_explicit": (cases.mixing_layer_case, dict(mx=16, my=12, mz=6, implicit=0)),
-    "mb": (cases.multiblock_case, dict(mxs=[10, 8], my=12, mz=6)),
-}
+from fixture_cases import FIXTURES
+
+CASES = {n: (fn, kw) for n, (fn, kw, _) in FIXTURES.items()}
+FIXTURE_RUNS = [(n, k) for n, (_, _, steps) in FIXTURES.items() for k in steps]
 
 STATE = ["bv", "sv", "cv", "vel", "acoustic", "mach", "mul", "conductivity", "mut", "turb_cond", "rho_d", "gamma",
          "cp", "wall_dist"]
@@ -94,28 +92,31 @@ def test_each_phase_matches_oracle(case_factory, name):
 
 @pytest.mark.parametrize("name", list(CASES))
 def test_ten_steps_match_oracle(case_factory, name):
-    case = make_case(case_factory, name)
+    """After 10 steps (2 for the limit_flow case, whose planted blast makes
+    the flow chaotic a few steps later) every field within 1e-9."""
+    steps = max(FIXTURES[name][2]) if name == "ml_limit" else 10
+    case = make_case(case_factory, name, steps)
     gpu, orc = pair(case)
-    err_gpu = gpu.step(10)
-    res_orc = None
-    for s in range(1, 11):
-        r = orc.step(s)
-        if r is not None:
-            res_orc = r
+    err_gpu = gpu.step(steps)
+    for s in range(1, steps + 1):
+        orc.step(s)
     compare(gpu, orc, STATE, 1e-9)
     assert np.isfinite(err_gpu)
 
 
-@pytest.mark.parametrize("name,steps", [(n, s) for n in CASES for s in (1, 10, 100)])
+@pytest.mark.parametrize("name,steps", FIXTURE_RUNS)
 def test_matches_reference_program(case_factory, name, steps):
-    """Fields of the reference's own flowfield.plt after `steps` steps."""
+    """Fields of the reference's own flowfield.plt after `steps` steps, and
+    its history.dat: err_max of every step (output_screen = 1)."""
     fix = GOLDEN / f"{name}_s{steps}.npz"
     if not fix.exists():
         pytest.skip(f"no reference fixture {fix.name}")
     gold = np.load(fix)
     gpu = ostc.Driver(make_case(case_factory, name, steps))
     gpu.initialize()
-    gpu.step(steps)
+    hist = {s: gpu.step(1) for s in range(1, steps + 1)}
+    bad_hist = history_mismatch(hist, gold["history"])
+    assert not bad_hist, f"history.dat lines that differ (step, ours, reference): {bad_hist[:10]}"
     names = [k.split("/", 1)[1] for k in gold.files if k.startswith("b0/")]
     info = gpu.info()
     worst = {}
@@ -135,6 +136,29 @@ def test_matches_reference_program(case_factory, name, steps):
         worst.update({f"b{b}/{n}": v for n, v in errs.items()})
     bad = {k: v for k, v in worst.items() if not v <= 1e-10}
     assert not bad, f"fields beyond 1e-10 vs the reference program: {bad}"
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_plt_output_is_byte_identical_to_reference(case_factory, name, tmp_path):
+    """simulate() over one step (output_file = 1) writes the same
+    output/field/flowfield.plt, byte for byte, as the reference program
+    (src/MPIIO.hpp:59-546): Tecplot V112 header, zone records, variable
+    order, min/max pairs and the interior values."""
+    fix = GOLDEN / f"{name}_s1.npz"
+    if not fix.exists() or "plt_raw" not in np.load(fix).files:
+        pytest.skip(f"no raw reference .plt in {fix.name}")
+    import shutil
+
+    case = tmp_path / name
+    shutil.copytree(make_case(case_factory, name, 1), case)
+    gpu = ostc.Driver(case)
+    gpu.initialize()
+    gpu.simulate()
+    ours = (case / "output" / "field" / "flowfield.plt").read_bytes()
+    ref = np.load(fix)["plt_raw"].tobytes()
+    assert len(ours) == len(ref), (len(ours), len(ref))
+    diff = np.flatnonzero(np.frombuffer(ours, np.uint8) != np.frombuffer(ref, np.uint8))
+    assert diff.size == 0, f"{diff.size} bytes differ, first at offset {diff[0]}"
 
 
 @pytest.mark.parametrize("name", list(CASES))

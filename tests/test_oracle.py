@@ -5,18 +5,17 @@ import pytest
 
 import openstc_b200 as ostc
 from openstc_b200 import cases
-from conftest import GOLDEN, scaled_err
+from conftest import GOLDEN, err_max_history, history_mismatch, scaled_err
 from oracle_bridge import OracleSolver, interior
 
-FIXTURE_CASES = {
-    "ramp": (cases.ramp_case, dict(mx=48, my=24)),
-    "ml": (cases.mixing_layer_case, dict(mx=16, my=12, mz=6)),
-    "ml_explicit": (cases.mixing_layer_case, dict(mx=16, my=12, mz=6, implicit=0)),
-    "mb": (cases.multiblock_case, dict(mxs=[10, 8], my=12, mz=6)),
-}
+from fixture_cases import FIXTURES
+
+FIXTURE_RUNS = [(n, k) for n, (_, _, steps) in FIXTURES.items() for k in steps]
 
 
-def run(case, steps, threads=1):
+def run(case, steps, threads=1, raws=None):
+    """The oracle over `steps` steps; raws (dict) collects the RMS one-step
+    changes of (rho, |V|, p, T) of every residual step."""
     s = OracleSolver(ostc.Driver(case), threads=threads)
     s.initialize()
     res = None
@@ -24,6 +23,8 @@ def run(case, steps, threads=1):
         r = s.step(k)
         if r is not None:
             res = r
+            if raws is not None:
+                raws[k] = r.copy()
     return s, res
 
 
@@ -46,16 +47,18 @@ def test_mass_fractions_stay_normalised(case_factory):
     assert np.max(np.abs(ysum - 1.0)) < 1e-8
 
 
-@pytest.mark.parametrize("name,steps", [("ramp", 1), ("ramp", 10), ("ml", 1), ("ml", 10), ("ml_explicit", 1),
-                                        ("ml_explicit", 10), ("mb", 1), ("mb", 10)])
+@pytest.mark.parametrize("name,steps", FIXTURE_RUNS)
 def test_oracle_matches_reference_program(case_factory, name, steps):
+    """Every variable of the reference's flowfield.plt within 1e-10 of its
+    scale, and every line of its history.dat (err_max per step)."""
     fix = GOLDEN / f"{name}_s{steps}.npz"
     if not fix.exists():
         pytest.skip(f"no reference fixture {fix.name}")
     gold = np.load(fix)
-    fn, kw = FIXTURE_CASES[name]
+    fn, kw, _ = FIXTURES[name]
     case = case_factory(name, fn, **dict(kw, total_step=steps, output_screen=1, output_file=steps))
-    s, res = run(case, steps, threads=4)
+    raws = {}
+    s, res = run(case, steps, threads=4, raws=raws)
     info = s.info
     worst = {}
     for b in range(info.n_block):
@@ -80,6 +83,8 @@ def test_oracle_matches_reference_program(case_factory, name, steps):
     tol = 1e-10
     bad = {k: v for k, v in worst.items() if not v <= tol}
     assert not bad, f"beyond {tol}: {bad}"
+    hist = history_mismatch(err_max_history(raws), gold["history"])
+    assert not hist, f"history.dat lines that differ (step, ours, reference): {hist[:10]}"
 
 
 def wall_friction_heatflux_2d(bv, mul, cond, metric, dyn_pressure, g):
