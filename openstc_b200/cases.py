@@ -376,15 +376,15 @@ def _read_grid(case: Path) -> list[tuple[np.ndarray, np.ndarray, np.ndarray]]:
     return out
 
 
-def _blend_initial_field(case: Path, delta: float = 5e-4, spikes: list[tuple[int, int, int, float]] | None = None,
-                         ) -> None:
+def _blend_initial_field(case: Path, delta: float = 5e-4,
+                         spikes: list[tuple[int, int, int, float, float]] | None = None) -> None:
     """Writes output/field/flowfield.plt with a tanh blend (thickness delta)
     of the two inflow states (UPPER and LOWER) across y = 0.025 m, plus
     step.txt and residual_scale.txt, so that a run with initial = 1 starts
-    from it.  spikes: (i, j, k, factor) cells of block 0 whose density and
-    pressure are multiplied by factor (same temperature), to put unphysical
-    states in front of limit_flow.  Pure NumPy: generating a case loads no
-    native library."""
+    from it.  spikes: (i, j, k, f_rho, f_p) cells of block 0 whose density
+    and pressure are multiplied by f_rho and f_p (the temperature by
+    f_p / f_rho, the ideal-gas state), to put unphysical states in front of
+    limit_flow.  Pure NumPy: generating a case loads no native library."""
     from .plt import write_plt
 
     up, lo = inflow_state(case, UPPER), inflow_state(case, LOWER)
@@ -413,9 +413,11 @@ def _blend_initial_field(case: Path, delta: float = 5e-4, spikes: list[tuple[int
         zone["omega"] = mix(lo["sv"][ns + 1], up["sv"][ns + 1])
         zone["mut"] = mix(lo["mut"], up["mut"])
         if spikes and not zones:
-            for i, j, k, f in spikes:
-                zone["density"][k, j, i] *= f
-                zone["pressure"][k, j, i] *= f
+            for i, j, k, f_rho, f_p in spikes:
+                zone["density"][k, j, i] *= f_rho
+                zone["pressure"][k, j, i] *= f_p
+                # the temperature the reference derives from them
+                zone["temperature"][k, j, i] *= f_p / f_rho
         zones.append(zone)
     write_plt(case / "output" / "field" / "flowfield.plt", names, zones)
     msg = case / "output" / "message"
@@ -437,7 +439,7 @@ def _species_names(case: Path) -> list[str]:
 def mixing_layer_case(case: str | Path, mx: int = 384, my: int = 192, mz: int = 64, total_step: int = 2000,
                       output_screen: int = 100, output_file: int | None = None, cfl: float = 0.5,
                       dplur: int = 4, chem: int = 1, implicit: int = 1,
-                      spikes: list[tuple[int, int, int, float]] | None = None) -> Path:
+                      spikes: list[tuple[int, int, int, float, float]] | None = None) -> Path:
     """3-D supersonic H2 / vitiated-air mixing layer (0.3 x 0.05 x 0.02 m,
     y clustered at the splitter y = 0.025 m).  Upper stream Mach 2.4, 1250 K,
     Y_O2 0.245, Y_H2O 0.175, N2; lower stream H2 / N2 (0.4 / 0.6) at

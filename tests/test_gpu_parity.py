@@ -190,3 +190,56 @@ def test_first_step_bit_identical_to_reference(case_factory, name):
                 differ.append(f"b{b}/{n}: {int((~same).sum())} of {same.size}")
     assert not differ, differ
 
+
+
+def test_engine_takes_its_own_parameters_after_another_engine(case_factory):
+    """The physics tables of a configuration live in __constant__ memory that
+    every engine of that configuration shares.  An engine created after
+    another one of the same configuration was destroyed (possibly at the same
+    address) must upload its own: the EPI mixing layer after the DA one still
+    matches the reference program bit for bit after one step."""
+    fix = GOLDEN / "ml_s1.npz"
+    if not fix.exists():
+        pytest.skip(f"no reference fixture {fix.name}")
+    gold = np.load(fix)
+    for _ in range(3):
+        da = ostc.Driver(make_case(case_factory, "ml_da", 1))
+        da.initialize()
+        da.step(1)
+        da.close()
+        gpu = ostc.Driver(make_case(case_factory, "ml", 1))
+        gpu.initialize()
+        gpu.step(1)
+        g = gpu.info().ngg
+        assert np.array_equal(interior(gpu.get(0, "bv"), g)[0], gold["b0/density"])
+        assert np.array_equal(interior(gpu.get(0, "sv"), g)[4], gold["b0/OH"])
+        gpu.close()
+
+
+def test_limit_flow_averages_the_neighbours_of_an_isolated_bad_cell(case_factory):
+    """limit_flow's averaging branch (src/TimeAdvanceFunc.cu:60-160): after
+    the residual and implicit phases the increments of one cell (i = 2 < mz,
+    so its neighbours are read) are set so that the update multiplies its
+    conservative state by 2000, past 1000 rho_inf and 1000 p_inf; the update
+    phase must replace it by the average of its 26 good neighbours, the GPU
+    as the oracle does, within 1e-12."""
+    case = make_case(case_factory, "ml", 1)
+    gpu, orc = pair(case)
+    for ph in ("residual", "implicit"):
+        gpu.run_phase(ph)
+        orc.phase(ph, 0)
+    g = gpu.info().ngg
+    i, j, k = 2, 5, 3
+    dq = gpu.get(0, "dq")  # one ghost layer under DPLUR
+    cv, dt, jac = gpu.get(0, "cv"), gpu.get(0, "dt_local"), gpu.get(0, "jac")
+    scale = jac[0, k + g, j + g, i + g] / dt[0, k, j, i]
+    dq[:, k + 1, j + 1, i + 1] = 1999.0 * cv[:, k + g, j + g, i + g] * scale
+    gpu.set(0, "dq", dq)
+    orc.set(0, "dq", dq)
+    gpu.run_phase("update")
+    orc.phase("update", 0)
+    compare(gpu, orc, ["bv", "sv", "cv"], 1e-12)
+    bv = gpu.get(0, "bv")
+    nb = bv[0, k + g - 1:k + g + 2, j + g - 1:j + g + 2, i + g - 1:i + g + 2].copy()
+    nb[1, 1, 1] = np.nan
+    assert abs(bv[0, k + g, j + g, i + g] - np.nanmean(nb)) <= 1e-12 * np.nanmean(nb)
