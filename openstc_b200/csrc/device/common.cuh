@@ -86,6 +86,10 @@ struct DevBlock {
   // components each): [0] dq0, [1] and [2] the ping-pong of the sweeps; the
   // last sweep writes the FP64 dq.  Null on the FP64 path.
   float *dqf[3];
+  // FP32-bulk path: an FP32 copy (layout G) of every operand of the
+  // direction-pass flux kernels, component by component (fp32::F32); null on
+  // the FP64 path
+  float *f32;
 };
 
 // Work table of a launch: CTA-tiles of every block, in block order.

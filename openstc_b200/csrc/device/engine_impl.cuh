@@ -72,6 +72,7 @@ class EngineT final : public Engine {
     tiles1_ = make_tiles(1);
     tilesg_ = make_tiles(ngg);
     col_tiles_ = make_col_tiles();
+    for (int d = 0; d < 3; ++d) dir_tiles_[d] = make_dir_tiles(d);
     cuda_check(cudaMalloc(&d_partial_, sizeof(double) * 4 * tiles0_.begin[tiles0_.nblk]), "cudaMalloc partial");
     cuda_check(cudaMalloc(&d_res_, sizeof(double) * 4), "cudaMalloc res");
     cuda_check(cudaMalloc(&d_bad_, sizeof(unsigned int)), "cudaMalloc bad");
@@ -118,6 +119,9 @@ class EngineT final : public Engine {
   }
 
   ~EngineT() override {
+    // a later engine of this configuration may be allocated at this address:
+    // it must not take the parameter block on the device for its own
+    if (static_owner() == this) static_owner() = nullptr;
     for (auto &g : graphs_)
       if (g) cudaGraphExecDestroy(g);
     for (void *q : sur_arrays_) cudaFree(q);
@@ -147,7 +151,20 @@ class EngineT final : public Engine {
     check_count(b, field, count);
     upload_params();
     cuda_check(cudaMemcpyAsync(p, host, sizeof(double) * count, cudaMemcpyHostToDevice, stream_), "set_field");
+    if (field == F_METRIC || field == F_JAC || field == F_WALL_DIST) pack_static(b);
     cuda_check(cudaStreamSynchronize(stream_), "set_field sync");
+  }
+
+  // the FP32 copy of block b's geometry (FP32-bulk path)
+  void pack_static(int b) {
+    if constexpr (C::mixed) {
+      k_pack32_static<C><<<pack_grid(b), 256, 0, stream_>>>(d_blocks_, b);
+      cuda_check(cudaGetLastError(), "pack32 static launch");
+    }
+  }
+
+  unsigned pack_grid(int b) const {
+    return static_cast<unsigned>(std::min<int64_t>((blocks_[b].G.size + 255) / 256, 16 * num_sms_));
   }
 
   void get_field(int b, int field, double *host, int64_t count) override {
@@ -212,6 +229,7 @@ class EngineT final : public Engine {
     if constexpr (C::turb) k_init_mut<C><<<grid(tiles1_), block3(), 0, stream_>>>(d_blocks_, tiles1_);
     launch_inner();
     launch_props();
+    for (int b = 0; b < static_cast<int>(blocks_.size()); ++b) pack_static(b);  // after the wall distance
     cuda_check(cudaGetLastError(), "initialize launch");
     cuda_check(cudaStreamSynchronize(stream_), "initialize");
   }
@@ -313,6 +331,7 @@ class EngineT final : public Engine {
   int launches_per_step(bool store_last, bool residual) const override {
     const auto &p = setup_.params;
     int n = 2;  // source, flux
+    if constexpr (C::mixed) n += (p.dim == 3 ? 2 : 1) + static_cast<int>(blocks_.size());  // pack + one pass per direction
     if (p.implicit_method == 1) {
       n += 1 + p.dplur_inner_step;
     } else if ((C::mix == 2 && p.chem_src_method != 0) || (C::turb && p.turb_implicit == 1)) {
@@ -447,6 +466,15 @@ class EngineT final : public Engine {
         f = static_cast<float *>(q);
       }
     }
+    B.f32 = nullptr;
+    if constexpr (C::mixed) {
+      void *q = nullptr;
+      const size_t bytes = sizeof(float) * static_cast<size_t>(B.G.size) * fp32::F32<C>::count;
+      cuda_check(cudaMalloc(&q, bytes), "cudaMalloc f32");
+      cuda_check(cudaMemset(q, 0, bytes), "memset f32");
+      allocations_.push_back(q);
+      B.f32 = static_cast<float *>(q);
+    }
     B.lu_piv = nullptr;
     if (C::mix == 2 && p.chem_src_method == 1) {
       void *q = nullptr;
@@ -469,6 +497,24 @@ class EngineT final : public Engine {
     if (count != field_count(b, f))
       throw std::runtime_error("field " + std::to_string(f) + " holds " + std::to_string(field_count(b, f)) +
                                " values, caller passed " + std::to_string(count));
+  }
+
+  // the tiles of direction pass d of the FP32-bulk flux (dir_tile_counts)
+  Tiles make_dir_tiles(int d) const {
+    Tiles t{};
+    t.nblk = static_cast<int>(blocks_.size());
+    int acc = 0;
+    for (int b = 0; b < t.nblk; ++b) {
+      const DevBlock &B = blocks_[b];
+      int n0 = 0, n1 = 0, n2 = 0;
+      dir_tile_counts(d, B.mx, B.my, B.mz, n0, n1, n2);
+      t.begin[b] = acc;
+      t.ntx[b] = n0;
+      t.nty[b] = n1;
+      acc += n0 * n1 * n2;
+    }
+    t.begin[t.nblk] = acc;
+    return t;
   }
 
   // columns of kTX x kTY cells over kFluxKC planes (the k-marching flux kernel)
@@ -531,9 +577,19 @@ class EngineT final : public Engine {
   }
 
   void launch_flux() {
-    if constexpr (C::mixed)
-      k_flux_mx_col<C><<<grid(col_tiles_), kFluxThreads, 0, stream_>>>(d_blocks_, col_tiles_);
-    else
+    if constexpr (C::mixed) {
+      for (int b = 0; b < static_cast<int>(blocks_.size()); ++b)
+        k_pack32<C><<<pack_grid(b), 256, 0, stream_>>>(d_blocks_, b);
+      mark("pack32");
+      k_flux_x<C><<<grid(dir_tiles_[0]), kCta, 0, stream_>>>(d_blocks_, dir_tiles_[0]);
+      mark("flux_x");
+      k_flux_march<C, 1><<<grid(dir_tiles_[1]), kCta, 0, stream_>>>(d_blocks_, dir_tiles_[1]);
+      mark("flux_y");
+      if (setup_.params.dim == 3) {
+        k_flux_march<C, 2><<<grid(dir_tiles_[2]), kCta, 0, stream_>>>(d_blocks_, dir_tiles_[2]);
+        mark("flux_z");
+      }
+    } else
       k_flux_col<C><<<grid(col_tiles_), kFluxThreads, col_smem_, stream_>>>(d_blocks_, col_tiles_);
   }
 
@@ -571,7 +627,7 @@ class EngineT final : public Engine {
     launch_source();
     mark("source");
     launch_flux();
-    mark("flux");
+    if constexpr (!C::mixed) mark("flux");
   }
 
   // returns the dq buffer holding the final increment (0 dq, 1 dq0, 2 dqk)
@@ -793,7 +849,7 @@ class EngineT final : public Engine {
   double *d_partial_ = nullptr, *d_res_ = nullptr, *h_res_ = nullptr, *d_wall_ = nullptr;
   unsigned int *d_bad_ = nullptr;
   std::vector<void *> allocations_;
-  Tiles tiles0_, tiles1_, tilesg_, col_tiles_;
+  Tiles tiles0_, tiles1_, tilesg_, col_tiles_, dir_tiles_[3];
   size_t source_smem_ = 0, flux_smem_ = 0, col_smem_ = 0, dq0_smem_ = 0;
   int final_dq_ = 0;
   cudaGraphExec_t graphs_[4] = {nullptr, nullptr, nullptr, nullptr};

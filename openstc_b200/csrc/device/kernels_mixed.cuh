@@ -91,6 +91,71 @@ __device__ __forceinline__ void thermo(float t, float *h, float *cp) {
   }
 }
 
+// Where the FP32 kernels read their operands (index n of layout G):
+// Src64 converts the FP64 state arrays on load; Src32 reads their FP32 copy
+// (DevBlock::f32, written once per step by k_pack32 and, for the geometry,
+// once per run by k_pack32_static), half the bytes and no conversion.
+// prim(v, n): primitive v, 0..5 the basic variables (rho, u, v, w, p, T),
+// 6.. the scalars (Y_k, k, omega).
+struct Src64 {
+  const DevBlock &B;
+  __device__ __forceinline__ float prim(int v, int64_t n) const {
+    return ldf((v < 6 ? B.bv + v * B.G.size : B.sv + (v - 6) * B.G.size) + n);
+  }
+  __device__ __forceinline__ float metric(int q, int64_t n) const { return ldf(B.metric + q * B.G.size + n); }
+  __device__ __forceinline__ float jac(int64_t n) const { return ldf(B.jac + n); }
+  __device__ __forceinline__ float mul(int64_t n) const { return ldf(B.mul + n); }
+  __device__ __forceinline__ float mut(int64_t n) const { return ldf(B.mut + n); }
+  __device__ __forceinline__ float cond(int64_t n) const { return ldf(B.cond + n); }
+  __device__ __forceinline__ float tcond(int64_t n) const { return ldf(B.turb_cond + n); }
+  __device__ __forceinline__ float rho_d(int l, int64_t n) const { return ldf(B.rho_d + l * B.G.size + n); }
+  __device__ __forceinline__ float wall(int64_t n) const { return ldf(B.wall_dist + n); }
+  __device__ __forceinline__ float acoustic(int64_t n) const { return ldf(B.acoustic + n); }
+  __device__ __forceinline__ float gamma(int64_t n) const { return ldf(B.gamma + n); }
+};
+
+// Component offsets of the FP32 copy (each component B.G.size floats).
+template <class C>
+struct F32 {
+  static constexpr int prim = 0, mul = 6 + C::nsc, mut = mul + 1, cond = mul + 2, tcond = mul + 3, rho_d = mul + 4,
+                       acoustic = rho_d + C::ns, gamma = acoustic + 1,
+                       n_dynamic = gamma + 1,  // written every step
+                       wall = n_dynamic, jac = wall + 1, metric = jac + 1, count = metric + 9;
+};
+
+template <class C>
+struct Src32 {
+  const float *f;
+  int64_t sz;
+  __device__ __forceinline__ float at(int c, int64_t n) const { return __ldg(f + c * sz + n); }
+  __device__ __forceinline__ float prim(int v, int64_t n) const { return at(F32<C>::prim + v, n); }
+  __device__ __forceinline__ float metric(int q, int64_t n) const { return at(F32<C>::metric + q, n); }
+  __device__ __forceinline__ float jac(int64_t n) const { return at(F32<C>::jac, n); }
+  __device__ __forceinline__ float mul(int64_t n) const { return at(F32<C>::mul, n); }
+  __device__ __forceinline__ float mut(int64_t n) const { return at(F32<C>::mut, n); }
+  __device__ __forceinline__ float cond(int64_t n) const { return at(F32<C>::cond, n); }
+  __device__ __forceinline__ float tcond(int64_t n) const { return at(F32<C>::tcond, n); }
+  __device__ __forceinline__ float rho_d(int l, int64_t n) const { return at(F32<C>::rho_d + l, n); }
+  __device__ __forceinline__ float wall(int64_t n) const { return at(F32<C>::wall, n); }
+  __device__ __forceinline__ float acoustic(int64_t n) const { return at(F32<C>::acoustic, n); }
+  __device__ __forceinline__ float gamma(int64_t n) const { return at(F32<C>::gamma, n); }
+};
+
+// h_k and cp_k of species i at t (thermo<> for one species)
+__device__ __forceinline__ void thermo_one(int i, float t, float &h, float &cp) {
+  const bool below = t < cF.t_low[i];
+  const float tt = below ? cF.t_low[i] : t;
+  const bool lo = below || tt < cF.t_mid[i];
+  const float c0 = nasa(i, 0, lo), c1 = nasa(i, 1, lo), c2 = nasa(i, 2, lo), c3 = nasa(i, 3, lo),
+              c4 = nasa(i, 4, lo);
+  const float c = c0 + tt * (c1 + tt * (c2 + tt * (c3 + tt * c4)));
+  float hh = tt * (c0 + tt * (0.5f * c1 + tt * (c2 * (1.f / 3.f) + tt * (0.25f * c3 + tt * (0.2f * c4))))) +
+             nasa(i, 5, lo);
+  if (below) hh += c * (t - tt);
+  h = hh * cF.ru_mw[i];
+  cp = c * cF.ru_mw[i];
+}
+
 // ------------------------------------------------------------ inviscid face
 // The face functions read the primitive stencil through a reader, so that one
 // copy of the physics serves the kernels that load it from the FP64 arrays
@@ -100,11 +165,10 @@ __device__ __forceinline__ void thermo(float t, float *h, float *cp) {
 
 // get(l, q): flux variable l at cell c + q (q = -1..2) of the face between
 // cell c (linear index n) and c + 1 (n + s).
-template <class C, class Get>
-__device__ __forceinline__ void inviscid_face_r(const DevBlock &B, int64_t n, int d, int64_t s, Get &&get,
+template <class C, class Src, class Get>
+__device__ __forceinline__ void inviscid_face_r(const Src &S, int64_t n, int d, int64_t s, Get &&get,
                                                 float *fc) {
   constexpr int NV = C::nv, NS = C::ns;
-  const int64_t sz = B.G.size;
   float pl[NV + 2], pr[NV + 2];
   const int rec = cP.reconstruction;
   OSTC_UNROLL for (int l = 0; l < NV; ++l) {
@@ -136,17 +200,17 @@ __device__ __forceinline__ void inviscid_face_r(const DevBlock &B, int64_t n, in
     }
     const float tl = pl[4] / (pl[0] * kRu * mwl);
     const float tr = pr[4] / (pr[0] * kRu * mwr);
-    float hl[NS], hr[NS], cpl_i[NS], cpr_i[NS];
-    thermo<NS, true, true>(tl, hl, cpl_i);
-    thermo<NS, true, true>(tr, hr, cpr_i);
     float cpl = 0, cpr = 0, cvl = 0, cvr = 0;
     OSTC_UNROLL for (int l = 0; l < NS; ++l) {
-      cpl += cpl_i[l] * pl[l + 5];
-      cpr += cpr_i[l] * pr[l + 5];
-      cvl += pl[l + 5] * (cpl_i[l] - cF.ru_mw[l]);
-      cvr += pr[l + 5] * (cpr_i[l] - cF.ru_mw[l]);
-      el += hl[l] * pl[l + 5];
-      er += hr[l] * pr[l + 5];
+      float hl, hr, cpl_l, cpr_l;
+      thermo_one(l, tl, hl, cpl_l);
+      thermo_one(l, tr, hr, cpr_l);
+      cpl += cpl_l * pl[l + 5];
+      cpr += cpr_l * pr[l + 5];
+      cvl += pl[l + 5] * (cpl_l - cF.ru_mw[l]);
+      cvr += pr[l + 5] * (cpr_l - cF.ru_mw[l]);
+      el += hl * pl[l + 5];
+      er += hr * pr[l + 5];
     }
     pl[NV] = pl[0] * el - pl[4];
     pr[NV] = pr[0] * er - pr[4];
@@ -159,11 +223,11 @@ __device__ __forceinline__ void inviscid_face_r(const DevBlock &B, int64_t n, in
     pl[NV + 1] = 1.4f;
     pr[NV + 1] = 1.4f;
   }
-  const double *m = B.metric + 3 * d * sz;
-  const float jl = ldf(B.jac + n), jr = ldf(B.jac + n + s);
-  const float k1 = 0.5f * (jl * ldf(m + n) + jr * ldf(m + n + s));
-  const float k2 = 0.5f * (jl * ldf(m + sz + n) + jr * ldf(m + sz + n + s));
-  const float k3 = 0.5f * (jl * ldf(m + 2 * sz + n) + jr * ldf(m + 2 * sz + n + s));
+  const int q0 = 3 * d;
+  const float jl = S.jac(n), jr = S.jac(n + s);
+  const float k1 = 0.5f * (jl * S.metric(q0, n) + jr * S.metric(q0, n + s));
+  const float k2 = 0.5f * (jl * S.metric(q0 + 1, n) + jr * S.metric(q0 + 1, n + s));
+  const float k3 = 0.5f * (jl * S.metric(q0 + 2, n) + jr * S.metric(q0 + 2, n + s));
   const float gk = sqrtf(k1 * k1 + k2 * k2 + k3 * k3);
   const float inv_gk = 1.f / gk;
   const float ul = (k1 * pl[1] + k2 * pl[2] + k3 * pl[3]) * inv_gk;
@@ -209,37 +273,36 @@ __device__ __forceinline__ void inviscid_face_r(const DevBlock &B, int64_t n, in
   OSTC_UNROLL for (int l = 5; l < NV; ++l) fc[l] = coeff * q(l);
 }
 
+template <class C, class Src>
+__device__ __forceinline__ void inviscid_face_s(const Src &S, int64_t n, int d, int64_t s, float *fc) {
+  inviscid_face_r<C>(S, n, d, s, [&](int l, int q) { return S.prim(l < 5 ? l : l + 1, n + q * s); }, fc);
+}
+
 template <class C>
 __device__ __forceinline__ void inviscid_face(const DevBlock &B, int64_t n, int d, int64_t s, float *fc) {
-  const int64_t sz = B.G.size;
-  inviscid_face_r<C>(
-      B, n, d, s,
-      [&](int l, int q) { return ldf((l < 5 ? B.bv + l * sz : B.sv + (l - 5) * sz) + n + q * s); }, fc);
+  inviscid_face_s<C>(Src64{B}, n, d, s, fc);
 }
 
 // ------------------------------------------------------------- viscous face
-__device__ __forceinline__ void face_grad(const double *a, int64_t n, int64_t n1, int d, int64_t sx, int64_t sxy,
-                                          float &dxi, float &deta, float &dzeta) {
-  dxi = d == 0 ? ldf(a + n1) - ldf(a + n)
-               : 0.25f * (ldf(a + n + 1) - ldf(a + n - 1) + ldf(a + n1 + 1) - ldf(a + n1 - 1));
-  deta = d == 1 ? ldf(a + n1) - ldf(a + n)
-                : 0.25f * (ldf(a + n + sx) - ldf(a + n - sx) + ldf(a + n1 + sx) - ldf(a + n1 - sx));
-  dzeta = d == 2 ? ldf(a + n1) - ldf(a + n)
-                 : 0.25f * (ldf(a + n + sxy) - ldf(a + n - sxy) + ldf(a + n1 + sxy) - ldf(a + n1 - sxy));
+// a(q): the variable at linear index q
+template <class A>
+__device__ __forceinline__ void face_grad(A &&a, int64_t n, int64_t n1, int d, int64_t sx, int64_t sxy, float &dxi,
+                                          float &deta, float &dzeta) {
+  dxi = d == 0 ? a(n1) - a(n) : 0.25f * (a(n + 1) - a(n - 1) + a(n1 + 1) - a(n1 - 1));
+  deta = d == 1 ? a(n1) - a(n) : 0.25f * (a(n + sx) - a(n - sx) + a(n1 + sx) - a(n1 - sx));
+  dzeta = d == 2 ? a(n1) - a(n) : 0.25f * (a(n + sxy) - a(n - sxy) + a(n1 + sxy) - a(n1 - sxy));
 }
 
 // val(v, side): primitive v at cell c (side 0) or c + 1 (side 1) of the face;
 // grad(v, g_xi, g_eta, g_zeta): its computational-space gradient at the face
 // (the face_grad stencil).
-template <class C, class Val, class Grad>
-__device__ __forceinline__ void viscous_face_r(const DevBlock &B, int64_t n, int d, int64_t s, Val &&val,
+template <class C, class Src, class Val, class Grad>
+__device__ __forceinline__ void viscous_face_r(const Src &S, int64_t n, int d, int64_t s, Val &&val,
                                                Grad &&grad, float *fv) {
   constexpr int NS = C::ns;
-  const int64_t sz = B.G.size;
   const int64_t n1 = n + s;
-  const double *m = B.metric;
   float mm[9];
-  OSTC_UNROLL for (int q = 0; q < 9; ++q) mm[q] = 0.5f * (ldf(m + q * sz + n) + ldf(m + q * sz + n1));
+  OSTC_UNROLL for (int q = 0; q < 9; ++q) mm[q] = 0.5f * (S.metric(q, n) + S.metric(q, n1));
   const float xi_x = mm[0], xi_y = mm[1], xi_z = mm[2], eta_x = mm[3], eta_y = mm[4], eta_z = mm[5];
   const float zeta_x = mm[6], zeta_y = mm[7], zeta_z = mm[8];
   auto cart = [&](float a_xi, float a_eta, float a_zeta, float &ax, float &ay, float &az) {
@@ -257,9 +320,9 @@ __device__ __forceinline__ void viscous_face_r(const DevBlock &B, int64_t n, int
   cart(g0, g1, g2, w_x, w_y, w_z);
   grad(5, g0, g1, g2);
   cart(g0, g1, g2, t_x, t_y, t_z);
-  const float mul = 0.5f * (ldf(B.mul + n) + ldf(B.mul + n1));
+  const float mul = 0.5f * (S.mul(n) + S.mul(n1));
   float mut = 0;
-  if constexpr (C::turb) mut = 0.5f * (ldf(B.mut + n) + ldf(B.mut + n1));
+  if constexpr (C::turb) mut = 0.5f * (S.mut(n) + S.mut(n1));
   const float viscosity = mul + mut;
   constexpr float third = 1.f / 3.f;
   float tau_xx = viscosity * (4 * u_x - 2 * v_y - 2 * w_z) * third;
@@ -274,11 +337,11 @@ __device__ __forceinline__ void viscous_face_r(const DevBlock &B, int64_t n, int
     tau_yy += tt;
     tau_zz += tt;
   }
-  const double *mr = m + 3 * d * sz;
-  const float ja = ldf(B.jac + n), jb = ldf(B.jac + n1);
-  const float kx = 0.5f * (ldf(mr + n) * ja + ldf(mr + n1) * jb);
-  const float ky = 0.5f * (ldf(mr + sz + n) * ja + ldf(mr + sz + n1) * jb);
-  const float kz = 0.5f * (ldf(mr + 2 * sz + n) * ja + ldf(mr + 2 * sz + n1) * jb);
+  const int q0 = 3 * d;
+  const float ja = S.jac(n), jb = S.jac(n1);
+  const float kx = 0.5f * (S.metric(q0, n) * ja + S.metric(q0, n1) * jb);
+  const float ky = 0.5f * (S.metric(q0 + 1, n) * ja + S.metric(q0 + 1, n1) * jb);
+  const float kz = 0.5f * (S.metric(q0 + 2, n) * ja + S.metric(q0 + 2, n1) * jb);
   fv[0] = 0;
   fv[1] = kx * tau_xx + ky * tau_xy + kz * tau_xz;
   fv[2] = kx * tau_xy + ky * tau_yy + kz * tau_yz;
@@ -286,31 +349,30 @@ __device__ __forceinline__ void viscous_face_r(const DevBlock &B, int64_t n, int
   const float um = 0.5f * (val(1, 0) + val(1, 1));
   const float vm = 0.5f * (val(2, 0) + val(2, 1));
   const float wm = 0.5f * (val(3, 0) + val(3, 1));
-  float conductivity = 0.5f * (ldf(B.cond + n) + ldf(B.cond + n1));
-  if constexpr (C::turb) conductivity += 0.5f * (ldf(B.turb_cond + n) + ldf(B.turb_cond + n1));
+  float conductivity = 0.5f * (S.cond(n) + S.cond(n1));
+  if constexpr (C::turb) conductivity += 0.5f * (S.tcond(n) + S.tcond(n1));
   fv[4] = um * fv[1] + vm * fv[2] + wm * fv[3] + conductivity * (kx * t_x + ky * t_y + kz * t_z);
   if constexpr (C::mix != 0) {
     float turb_d = 0;
     if constexpr (C::turb) turb_d = mut / cF.Sct;
-    float h[NS], dif[NS], yx[NS], yy[NS], yz[NS];
     const float tm = 0.5f * (val(5, 0) + val(5, 1));
-    thermo<NS, true, false>(tm, h, nullptr);
     float rho_uc = 0, rho_vc = 0, rho_wc = 0, hflux = 0;
     OSTC_UNROLL for (int l = 0; l < NS; ++l) {
-      dif[l] = 0.5f * (ldf(B.rho_d + l * sz + n) + ldf(B.rho_d + l * sz + n1)) + turb_d;
+      const float dif = 0.5f * (S.rho_d(l, n) + S.rho_d(l, n1)) + turb_d;
+      float yx, yy, yz, h, cp_unused;
       grad(6 + l, g0, g1, g2);
-      cart(g0, g1, g2, yx[l], yy[l], yz[l]);
-      hflux += dif[l] * h[l] * (kx * yx[l] + ky * yy[l] + kz * yz[l]);
-      rho_uc += dif[l] * yx[l];
-      rho_vc += dif[l] * yy[l];
-      rho_wc += dif[l] * yz[l];
+      cart(g0, g1, g2, yx, yy, yz);
+      thermo_one(l, tm, h, cp_unused);
+      // the diffusive flux of species l through the face, before the correction
+      fv[5 + l] = dif * (kx * yx + ky * yy + kz * yz);
+      hflux += h * fv[5 + l];
+      rho_uc += dif * yx;
+      rho_vc += dif * yy;
+      rho_wc += dif * yz;
     }
     fv[4] += hflux;
     const float corr = kx * rho_uc + ky * rho_vc + kz * rho_wc;
-    OSTC_UNROLL for (int l = 0; l < NS; ++l) {
-      fv[5 + l] = dif[l] * (kx * yx[l] + ky * yy[l] + kz * yz[l]) -
-                  0.5f * (val(6 + l, 0) + val(6 + l, 1)) * corr;
-    }
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) fv[5 + l] -= 0.5f * (val(6 + l, 0) + val(6 + l, 1)) * corr;
   }
   if constexpr (C::turb) {
     float k_x, k_y, k_z, o_x, o_y, o_z;
@@ -318,7 +380,7 @@ __device__ __forceinline__ void viscous_face_r(const DevBlock &B, int64_t n, int
     cart(g0, g1, g2, k_x, k_y, k_z);
     grad(7 + NS, g0, g1, g2);
     cart(g0, g1, g2, o_x, o_y, o_z);
-    const float wall_dist = 0.5f * (ldf(B.wall_dist + n) + ldf(B.wall_dist + n1));
+    const float wall_dist = 0.5f * (S.wall(n) + S.wall(n1));
     float f1 = 1;
     if (wall_dist > 1e-25f) {
       const float km = 0.5f * (val(6 + NS, 0) + val(6 + NS, 1));
@@ -341,13 +403,21 @@ __device__ __forceinline__ void viscous_face_r(const DevBlock &B, int64_t n, int
   }
 }
 
+template <class C, class Src>
+__device__ __forceinline__ void viscous_face_s(const Src &S, int64_t sx, int64_t sxy, int64_t n, int d, int64_t s,
+                                               float *fv) {
+  const int64_t n1 = n + s;
+  viscous_face_r<C>(
+      S, n, d, s, [&](int v, int side) { return S.prim(v, side ? n1 : n); },
+      [&](int v, float &g0, float &g1, float &g2) {
+        face_grad([&](int64_t q) { return S.prim(v, q); }, n, n1, d, sx, sxy, g0, g1, g2);
+      },
+      fv);
+}
+
 template <class C>
 __device__ __forceinline__ void viscous_face(const DevBlock &B, int64_t n, int d, int64_t s, float *fv) {
-  const int64_t sz = B.G.size, sx = B.G.sx, sxy = B.G.sxy, n1 = n + s;
-  auto ptr = [&](int v) { return v < 6 ? B.bv + v * sz : B.sv + (v - 6) * sz; };
-  viscous_face_r<C>(
-      B, n, d, s, [&](int v, int side) { return ldf(ptr(v) + (side ? n1 : n)); },
-      [&](int v, float &g0, float &g1, float &g2) { face_grad(ptr(v), n, n1, d, sx, sxy, g0, g1, g2); }, fv);
+  viscous_face_s<C>(Src64{B}, B.G.sx, B.G.sxy, n, d, s, fv);
 }
 
 // ------------------------------------------------------------- SST source
@@ -560,21 +630,19 @@ __global__ void __launch_bounds__(kCta, 4) k_chem_list(const DevBlock *__restric
 // Local time step of cell (i, j, k) in FP32 (local_time_step,
 // src/TimeAdvanceFunc.cuh:21-71); also stores the spectral radii the DPLUR
 // sweeps use.
-template <class C>
-__device__ __forceinline__ void local_time_step_mx(const DevBlock &B, int i, int j, int k, int64_t n, int64_t nd) {
+template <class C, class Src>
+__device__ __forceinline__ void local_time_step_s(const DevBlock &B, const Src &S, int i, int j, int k, int64_t n,
+                                                  int64_t nd) {
   const int64_t szd = B.D.size;
   const bool three_d = B.mz > 1;
-  const int64_t sz = B.G.size;
-  const double *m = B.metric;
-  using fp32::ldf;
-  const float m11 = ldf(m + n), m12 = ldf(m + sz + n), m13 = ldf(m + 2 * sz + n);
-  const float m21 = ldf(m + 3 * sz + n), m22 = ldf(m + 4 * sz + n), m23 = ldf(m + 5 * sz + n);
-  const float m31 = ldf(m + 6 * sz + n), m32 = ldf(m + 7 * sz + n), m33 = ldf(m + 8 * sz + n);
+  const float m11 = S.metric(0, n), m12 = S.metric(1, n), m13 = S.metric(2, n);
+  const float m21 = S.metric(3, n), m22 = S.metric(4, n), m23 = S.metric(5, n);
+  const float m31 = S.metric(6, n), m32 = S.metric(7, n), m33 = S.metric(8, n);
   const float grad_xi = sqrtf(m11 * m11 + m12 * m12 + m13 * m13);
   const float grad_eta = sqrtf(m21 * m21 + m22 * m22 + m23 * m23);
   const float grad_zeta = sqrtf(m31 * m31 + m32 * m32 + m33 * m33);
-  const float u = ldf(B.bv + sz + n), v = ldf(B.bv + 2 * sz + n), w = ldf(B.bv + 3 * sz + n);
-  const float a = ldf(B.acoustic + n);
+  const float u = S.prim(1, n), v = S.prim(2, n), w = S.prim(3, n);
+  const float a = S.acoustic(n);
   const float s0 = fabsf(u * m11 + v * m12 + w * m13) + a * grad_xi;
   const float s1 = fabsf(u * m21 + v * m22 + w * m23) + a * grad_eta;
   const float s2 = three_d ? fabsf(u * m31 + v * m32 + w * m33) + a * grad_zeta : 0.f;
@@ -582,15 +650,20 @@ __device__ __forceinline__ void local_time_step_mx(const DevBlock &B, int i, int
   B.inv_spec[szd + nd] = s1;
   B.inv_spec[2 * szd + nd] = s2;
   float gamma = 1.4f;
-  if constexpr (C::mix != 0) gamma = ldf(B.gamma + n);
-  const float coeff_1 = fmaxf(gamma, 4.f / 3.f) / ldf(B.bv + n);
-  float coeff_2 = ldf(B.mul + n) / cF.Pr;
-  if constexpr (C::turb) coeff_2 += ldf(B.mut + n) / cF.Prt;
+  if constexpr (C::mix != 0) gamma = S.gamma(n);
+  const float coeff_1 = fmaxf(gamma, 4.f / 3.f) / S.prim(0, n);
+  float coeff_2 = S.mul(n) / cF.Pr;
+  if constexpr (C::turb) coeff_2 += S.mut(n) / cF.Prt;
   float srv = grad_xi * grad_xi + grad_eta * grad_eta;
   if (three_d) srv += grad_zeta * grad_zeta;
   srv *= coeff_1 * coeff_2;
   B.visc_spec[nd] = srv;
   B.dt_local[B.Z.at(i, j, k)] = cF.cfl / (s0 + s1 + s2 + srv);
+}
+
+template <class C>
+__device__ __forceinline__ void local_time_step_mx(const DevBlock &B, int i, int j, int k, int64_t n, int64_t nd) {
+  local_time_step_s<C>(B, fp32::Src64{B}, i, j, k, n, nd);
 }
 
 // Inviscid + viscous flux differences in FP32 (accumulated in FP32 and added
@@ -742,6 +815,166 @@ __global__ void __launch_bounds__(kFluxThreads, 4) k_flux_mx_col(const DevBlock 
     const int64_t n = B.G.at(i, j, k), nd = B.D.at(i, j, k);
     OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq[l * szd + nd] += static_cast<double>(acc[l]);
     local_time_step_mx<C>(B, i, j, k, n, nd);
+  }
+}
+
+// ----------------------------------------------------- direction passes
+// The flux differences as three passes, one per direction d: every face
+// along d is evaluated once, inviscid and viscous together, as
+// G = F_viscous - F_inviscid, and each cell adds G(c + 1/2) - G(c - 1/2) to
+// its FP64 dq.  A pass keeps one face's fluxes in registers and needs no
+// shared memory or barrier, so its warps run independently and the SM keeps
+// as many loads in flight as its register file allows; the price is dq read
+// and written once per direction instead of once.  The x pass also stores
+// the local time step.
+//   x: a warp holds 32 consecutive faces of one row (i - 1/2 + lane) and
+//      gives 31 cells their difference, the left face coming from the lane
+//      below by a shuffle; a CTA covers 4 rows (j).
+//   y, z: each thread marches kMarch cells along d, carrying the lower face
+//      from one cell to the next; lanes run along i, the CTA's 4 warps over
+//      the remaining index (k for y, j for z).
+constexpr int kMarch = 8;
+constexpr int kXSeg = 31;  // cells per warp of the x pass
+
+// Tiles of pass d over every block: (x) i-segments x row groups x k,
+// (y) i-groups x k-groups x j-segments, (z) i-groups x j-groups x k-segments.
+inline void dir_tile_counts(int d, int mx, int my, int mz, int &n0, int &n1, int &n2) {
+  if (d == 0) {
+    n0 = (mx + kXSeg - 1) / kXSeg;
+    n1 = (my + kTY - 1) / kTY;
+    n2 = mz;
+  } else if (d == 1) {
+    n0 = (mx + kTX - 1) / kTX;
+    n1 = (mz + kTY - 1) / kTY;
+    n2 = (my + kMarch - 1) / kMarch;
+  } else {
+    n0 = (mx + kTX - 1) / kTX;
+    n1 = (my + kTY - 1) / kTY;
+    n2 = (mz + kMarch - 1) / kMarch;
+  }
+}
+
+__device__ __forceinline__ void dir_tile(const Tiles &T, int &b, int &t0, int &t1, int &t2) {
+  int t = blockIdx.x;
+  b = 0;
+  while (b + 1 < T.nblk && t >= T.begin[b + 1]) ++b;
+  t -= T.begin[b];
+  t0 = t % T.ntx[b];
+  t /= T.ntx[b];
+  t1 = t % T.nty[b];
+  t2 = t / T.nty[b];
+}
+
+// G = F_viscous - F_inviscid at the face between linear index nl and nl + s,
+// from the FP32 copy of the operands
+template <class C>
+__device__ __forceinline__ void face_g(const DevBlock &B, int64_t nl, int d, int64_t s, float *g) {
+  constexpr int NV = C::nv;
+  const fp32::Src32<C> S{B.f32, B.G.size};
+  fp32::inviscid_face_s<C>(S, nl, d, s, g);
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) g[l] = -g[l];
+  if (cP.viscous_order != 0) {
+    float t[NV];
+    fp32::viscous_face_s<C>(S, B.G.sx, B.G.sxy, nl, d, s, t);
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) g[l] += t[l];
+  }
+}
+
+// The FP32 copy of the operands of the direction passes, over every point of
+// layout G: the fields that change every step (after the source stage, which
+// writes mu_t and lambda_t) ...
+template <class C>
+__global__ void __launch_bounds__(256) k_pack32(const DevBlock *__restrict__ blks, int b) {
+  using L = fp32::F32<C>;
+  const DevBlock &B = blks[b];
+  const int64_t sz = B.G.size;
+  float *f = B.f32;
+  for (int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; n < sz;
+       n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    OSTC_UNROLL for (int v = 0; v < 6; ++v) f[(L::prim + v) * sz + n] = static_cast<float>(B.bv[v * sz + n]);
+    OSTC_UNROLL for (int v = 0; v < C::nsc; ++v) f[(L::prim + 6 + v) * sz + n] = static_cast<float>(B.sv[v * sz + n]);
+    f[L::mul * sz + n] = static_cast<float>(B.mul[n]);
+    f[L::cond * sz + n] = static_cast<float>(B.cond[n]);
+    if constexpr (C::turb) {
+      f[L::mut * sz + n] = static_cast<float>(B.mut[n]);
+      f[L::tcond * sz + n] = static_cast<float>(B.turb_cond[n]);
+    }
+    OSTC_UNROLL for (int l = 0; l < C::ns; ++l) f[(L::rho_d + l) * sz + n] = static_cast<float>(B.rho_d[l * sz + n]);
+    f[L::acoustic * sz + n] = static_cast<float>(B.acoustic[n]);
+    if constexpr (C::mix != 0) f[L::gamma * sz + n] = static_cast<float>(B.gamma[n]);
+  }
+}
+
+// ... and the geometry, which changes only when the grid is set.
+template <class C>
+__global__ void __launch_bounds__(256) k_pack32_static(const DevBlock *__restrict__ blks, int b) {
+  using L = fp32::F32<C>;
+  const DevBlock &B = blks[b];
+  const int64_t sz = B.G.size;
+  float *f = B.f32;
+  for (int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; n < sz;
+       n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    f[L::wall * sz + n] = B.wall_dist ? static_cast<float>(B.wall_dist[n]) : 0.f;
+    f[L::jac * sz + n] = static_cast<float>(B.jac[n]);
+    OSTC_UNROLL for (int q = 0; q < 9; ++q) f[(L::metric + q) * sz + n] = static_cast<float>(B.metric[q * sz + n]);
+  }
+}
+
+template <class C>
+__global__ void __launch_bounds__(kCta, 4) k_flux_x(const DevBlock *__restrict__ blks, Tiles T) {
+  constexpr int NV = C::nv;
+  int b, t0, t1, t2;
+  dir_tile(T, b, t0, t1, t2);
+  const DevBlock &B = blks[b];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j = t1 * kTY + warp, k = t2;
+  if (j >= B.my) return;  // the whole warp
+  const int f = t0 * kXSeg - 1 + lane;  // the face between cells f and f + 1
+  const bool face = f < B.mx;
+  float g[NV];
+  if (face) {
+    face_g<C>(B, B.G.at(f, j, k), 0, 1, g);
+  } else {
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) g[l] = 0;
+  }
+  const bool cell = face && lane > 0;
+  const int64_t szd = B.D.size;
+  const int64_t nd = cell ? B.D.at(f, j, k) : 0;
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) {
+    const float gm = __shfl_up_sync(0xffffffffu, g[l], 1);
+    if (cell) B.dq[l * szd + nd] += static_cast<double>(g[l] - gm);
+  }
+  if (cell) local_time_step_s<C>(B, fp32::Src32<C>{B.f32, B.G.size}, f, j, k, B.G.at(f, j, k), nd);
+}
+
+template <class C, int D>
+__global__ void __launch_bounds__(kCta, 4) k_flux_march(const DevBlock *__restrict__ blks, Tiles T) {
+  constexpr int NV = C::nv;
+  static_assert(D == 1 || D == 2, "march passes run along y or z");
+  int b, t0, t1, t2;
+  dir_tile(T, b, t0, t1, t2);
+  const DevBlock &B = blks[b];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = t0 * kTX + lane, o = t1 * kTY + warp;  // o: k for the y pass, j for the z pass
+  if (i >= B.mx || o >= (D == 1 ? B.mz : B.my)) return;
+  const int m = D == 1 ? B.my : B.mz;
+  const int c0 = t2 * kMarch, c1 = min(c0 + kMarch, m);
+  const int64_t s = D == 1 ? B.G.sx : B.G.sxy;
+  const int64_t n0 = D == 1 ? B.G.at(i, c0, o) : B.G.at(i, o, c0);
+  const int64_t sd = D == 1 ? B.D.sx : B.D.sxy;
+  const int64_t nd0 = D == 1 ? B.D.at(i, c0, o) : B.D.at(i, o, c0);
+  const int64_t szd = B.D.size;
+  float gm[NV];
+  face_g<C>(B, n0 - s, D, s, gm);  // face c0 - 1/2
+#pragma unroll 1
+  for (int c = c0; c < c1; ++c) {
+    float g[NV];
+    face_g<C>(B, n0 + (c - c0) * s, D, s, g);  // face c + 1/2
+    const int64_t nd = nd0 + (c - c0) * sd;
+    OSTC_UNROLL for (int l = 0; l < NV; ++l) {
+      B.dq[l * szd + nd] += static_cast<double>(g[l] - gm[l]);
+      gm[l] = g[l];
+    }
   }
 }
 
