@@ -69,6 +69,18 @@ typedef struct ostc_options {
                     flux Jacobians and transport, FP64 state, update, temperature
                     inversion, chemistry, point-implicit solve and residual (finite-rate
                     SST cases only) */
+  int exact_inner; /* 0: inner faces as the reference treats them
+                      (src/DataCommunication.cuh:58-98: the shared plane averaged,
+                      bv / sv ghosts copied from the neighbour, the DPLUR sweeps
+                      treating the face as a boundary).  1 (FP64 path, 3-D, faces
+                      that cover whole block faces): a multi-block grid computes what
+                      the same grid as one block computes, bit for bit: every array a
+                      stencil reads across the face (the ghost rows next to the face,
+                      mu_t, lambda_t, |V|, the spectral radii, the species enthalpies,
+                      the DPLUR increments of each sweep) is copied from the
+                      neighbour, the sweeps take the neighbours across the face, and
+                      the shared plane, computed identically on both sides, is not
+                      re-averaged.  No counterpart in the reference. */
 } ostc_options;
 
 typedef struct ostc_info {
@@ -264,6 +276,26 @@ int ostc_driver_set_surrogate(ostc_driver *d, ostc_surrogate *s);
    evaluations of the network (a rejected cell is evaluated again within a few
    steps, in between it keeps EPI; evaluated may be NULL). */
 int ostc_driver_chemistry_stats(ostc_driver *d, long long *accepted, long long *fallback, long long *evaluated);
+
+/* The launch tuning of the step (no counterpart in the reference, which
+   launches each block separately with fixed 2-D thread blocks,
+   src/Driver.cu:205-216).  schedule: the order in which the blocks of a
+   multi-block grid share each launch (0 block order, 1 largest block first);
+   flux_variant: the variant of the FP32-bulk flux passes (resident CTAs per SM
+   and cells each thread marches over; 0 on the FP64 path).  No choice changes
+   a result. */
+typedef struct ostc_tuning {
+  int schedule, flux_variant;
+  int candidates;     /* pairs timed */
+  double ms;          /* device time of one pass of source, flux and implicit stages, chosen pair */
+  double ms_default;  /* the same for (0, 0) */
+} ostc_tuning;
+/* Times every pair on the driver's own case (reps passes each, the flow state
+   is not advanced), applies the fastest and records it in
+   output/message/autotune.txt, which ostc_driver_initialize applies again
+   when the configuration and block sizes match.  out may be NULL. */
+int ostc_driver_autotune(ostc_driver *d, int reps, ostc_tuning *out);
+int ostc_driver_set_tuning(ostc_driver *d, int schedule, int flux_variant);
 
 /* No counterpart in the reference.  Recomputes, from the device state, the
    normalised residuals of rho, |V|, p, T of the last step, without allocating

@@ -35,7 +35,7 @@ class OstcError(RuntimeError):
 
 
 class Options(C.Structure):
-    _fields_ = [("device", C.c_int), ("quiet", C.c_int), ("precision", C.c_int)]
+    _fields_ = [("device", C.c_int), ("quiet", C.c_int), ("precision", C.c_int), ("exact_inner", C.c_int)]
 
 
 class SurrogateEval(C.Structure):
@@ -80,6 +80,11 @@ class Params(C.Structure):
         ("troe_alpha", C.c_double * MAX_REAC), ("troe_t3", C.c_double * MAX_REAC),
         ("troe_t1", C.c_double * MAX_REAC), ("troe_t2", C.c_double * MAX_REAC),
     ]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("schedule", C.c_int), ("flux_variant", C.c_int), ("candidates", C.c_int), ("ms", C.c_double),
+                ("ms_default", C.c_double)]
 
 
 class Bc(C.Structure):
@@ -128,6 +133,8 @@ def library() -> C.CDLL:
         "ostc_driver_step": ([P, C.c_int, D], C.c_int),
         "ostc_driver_residual": ([P, D], C.c_int),
         "ostc_driver_residual_noalloc": ([P, D], C.c_int),
+        "ostc_driver_autotune": ([P, C.c_int, C.POINTER(Tuning)], C.c_int),
+        "ostc_driver_set_tuning": ([P, C.c_int, C.c_int], C.c_int),
         "ostc_tc_gemm_bf16": ([P, C.c_int, P, C.c_int, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, P], C.c_int),
         "ostc_surrogate_create": ([P, C.c_ulonglong, C.POINTER(P)], C.c_int),
         "ostc_surrogate_destroy": ([P], None),
@@ -183,15 +190,18 @@ class Driver:
     ``step(n)`` n loop iterations without file output.
     """
 
-    def __init__(self, case_dir: str | Path, device: int = 0, quiet: bool = True, precision: str = "fp64"):
+    def __init__(self, case_dir: str | Path, device: int = 0, quiet: bool = True, precision: str = "fp64",
+                 exact_inner: bool = False):
         """precision: "fp64" (the reference's arithmetic) or "mixed" (FP32 fluxes,
         limiter, SST, flux Jacobians and transport; FP64 state, update,
-        temperature inversion, chemistry, point-implicit solve, residual)."""
+        temperature inversion, chemistry, point-implicit solve, residual).
+        exact_inner: a multi-block grid computes what the same grid as one
+        block computes (ostc_options.exact_inner; FP64 path)."""
         lib = library()
         self._h = C.c_void_p()
         if precision not in PRECISIONS:
             raise OstcError(f"precision must be one of {sorted(PRECISIONS)}")
-        opt = Options(device, 1 if quiet else 0, PRECISIONS[precision])
+        opt = Options(device, 1 if quiet else 0, PRECISIONS[precision], 1 if exact_inner else 0)
         _check(lib.ostc_driver_create(str(case_dir).encode(), C.byref(opt), C.byref(self._h)))
         self.case_dir = Path(case_dir)
 
@@ -296,6 +306,17 @@ class Driver:
         a, f, e = C.c_longlong(), C.c_longlong(), C.c_longlong()
         _check(library().ostc_driver_chemistry_stats(self._h, C.byref(a), C.byref(f), C.byref(e)))
         return e.value
+
+    def autotune(self, reps: int = 3) -> dict:
+        """Time every launch tuning (block schedule x FP32 flux variant) on
+        this case, apply the fastest and record it for later runs
+        (ostc_driver_autotune)."""
+        t = Tuning()
+        _check(library().ostc_driver_autotune(self._h, reps, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in Tuning._fields_}
+
+    def set_tuning(self, schedule: int, flux_variant: int = 0) -> None:
+        _check(library().ostc_driver_set_tuning(self._h, schedule, flux_variant))
 
     def residual_noalloc(self) -> np.ndarray:
         """The residual of the last stored step recomputed on the device in

@@ -74,6 +74,7 @@ int ostc_driver_create(const char *case_dir, const ostc_options *opt, ostc_drive
       o.device = opt->device;
       o.quiet = opt->quiet != 0;
       o.precision = opt->precision;
+      o.exact_inner = opt->exact_inner != 0;
     }
     *out = new ostc_driver(case_dir, o);
     return OSTC_OK;
@@ -261,6 +262,31 @@ int ostc_driver_residual(const ostc_driver *d, double res[4]) {
   if (!d || !res) return fail(OSTC_ERR_INPUT, "null argument");
   for (int l = 0; l < 4; ++l) res[l] = d->drv.res[l];
   return OSTC_OK;
+}
+
+int ostc_driver_autotune(ostc_driver *d, int reps, ostc_tuning *out) {
+  if (!d || reps < 1) return fail(OSTC_ERR_INPUT, "bad argument");
+  if (!d->drv.initialized()) return fail(OSTC_ERR_STATE, "initialize first");
+  return guarded([&] {
+    const ostc::Driver::Tuning t = d->drv.autotune(reps);
+    if (out) {
+      out->schedule = t.schedule;
+      out->flux_variant = t.flux_variant;
+      out->candidates = t.candidates;
+      out->ms = t.ms;
+      out->ms_default = t.ms_default;
+    }
+    return OSTC_OK;
+  });
+}
+
+int ostc_driver_set_tuning(ostc_driver *d, int schedule, int flux_variant) {
+  if (!d) return fail(OSTC_ERR_INPUT, "null argument");
+  if (!d->drv.initialized()) return fail(OSTC_ERR_STATE, "initialize first");
+  return guarded([&] {
+    d->drv.engine().set_tuning(schedule, flux_variant);
+    return OSTC_OK;
+  });
 }
 
 int ostc_driver_residual_noalloc(ostc_driver *d, double res[4]) {

@@ -90,14 +90,31 @@ struct DevBlock {
   // direction-pass flux kernels, component by component (fp32::F32); null on
   // the FP64 path
   float *f32;
+  // with exact inner faces: bit 2 d + (1 for the high side) is set when that
+  // block face is an inner face whose neighbours the DPLUR sweeps take
+  int inner_mask;
 };
 
-// Work table of a launch: CTA-tiles of every block, in block order.
+// Work table of a launch: CTA-tiles of every block.  The blocks are laid out
+// in schedule order (slot s holds block block[s], whose tiles are CTAs
+// begin[s] .. begin[s + 1] - 1); ntx / nty and cbegin (the block's first
+// tile in block order, which fixes the residual's reduction order whatever
+// the schedule) are indexed by block.
 struct Tiles {
   int nblk = 0;
   int begin[kMaxBlocks + 1] = {};
+  int block[kMaxBlocks] = {};
+  int cbegin[kMaxBlocks] = {};
   int ntx[kMaxBlocks] = {}, nty[kMaxBlocks] = {};
   int halo = 0;  // cells [-halo, m+halo) in every direction
 };
+
+// The block of this CTA and the CTA's tile index within the block.
+OSTC_HD inline int tile_of(const Tiles &T, int cta, int &b) {
+  int s = 0;
+  while (s + 1 < T.nblk && cta >= T.begin[s + 1]) ++s;
+  b = T.block[s];
+  return cta - T.begin[s];
+}
 
 }  // namespace ostc

@@ -44,6 +44,7 @@ struct EngineSetup {
   std::vector<double> wall_points;  // x,y,z triples for the wall distance
   int device = 0;
   int precision = 0;  // 0 FP64 (the reference's arithmetic), 1 FP32-bulk / FP64-critical
+  bool exact_inner = false;  // inner faces computed as the interior of one block (FP64)
 };
 
 class Engine {
@@ -101,6 +102,17 @@ class Engine {
   // each) and their device-to-host copies into cf / qw; the values are there
   // once the next output event (or a synchronize) has passed.
   virtual void wall_friction_heatflux_2d(int b, double dyn_pressure, double *cf, double *qw) = 0;
+
+  // Tuning.  schedule: the order of the blocks in every launch (0 block
+  // order, 1 largest block first); flux_variant: the variant of the FP32-bulk
+  // flux passes (fp32 kFluxVariant; 0 on the FP64 path).  Neither changes a
+  // result.  Drops the captured step graphs.
+  virtual void set_tuning(int schedule, int flux_variant) = 0;
+  virtual int flux_variants() const = 0;
+  // Device time (ms) of one pass of the stages that leave the flow state
+  // alone (source, flux, implicit increments), eagerly launched `reps`
+  // times after one untimed pass; the state is not advanced.
+  virtual double time_stages(int reps) = 0;
 };
 
 // Largest grid ostc_driver_residual_noalloc accepts, in residual tiles

@@ -40,6 +40,7 @@ class EngineT final : public Engine {
       blocks_.push_back(B);
     }
     for (int b = 0; b < static_cast<int>(blocks_.size()); ++b) allocate(blocks_[b]);
+    if (s.exact_inner) mark_exact_inner_faces();
     cuda_check(cudaMalloc(&d_blocks_, sizeof(DevBlock) * blocks_.size()), "cudaMalloc blocks");
     // uploads go through the engine's own (non-blocking) stream: a copy on the
     // legacy default stream from pageable memory may still be in flight when
@@ -68,11 +69,7 @@ class EngineT final : public Engine {
                                  stream_),
                  "copy inner");
     }
-    tiles0_ = make_tiles(0);
-    tiles1_ = make_tiles(1);
-    tilesg_ = make_tiles(ngg);
-    col_tiles_ = make_col_tiles();
-    for (int d = 0; d < 3; ++d) dir_tiles_[d] = make_dir_tiles(d);
+    make_all_tiles();
     cuda_check(cudaMalloc(&d_partial_, sizeof(double) * 4 * tiles0_.begin[tiles0_.nblk]), "cudaMalloc partial");
     cuda_check(cudaMalloc(&d_res_, sizeof(double) * 4), "cudaMalloc res");
     cuda_check(cudaMalloc(&d_bad_, sizeof(unsigned int)), "cudaMalloc bad");
@@ -345,6 +342,11 @@ class EngineT final : public Engine {
     if (store_last) n += 1;
     if (residual) n += 2;
     if (sur_on_) n += (C::mixed ? 4 : 2) * static_cast<int>(blocks_.size());  // candidates + inference (+ chemistry list)
+    if (setup_.exact_inner) {  // the halo copies of exact inner faces
+      int sets = 2;  // mu_t / lambda_t, |V|
+      if (p.implicit_method == 1) sets += 2 + p.dplur_inner_step;  // spectral radii, enthalpies, each sweep's input
+      n += sets * static_cast<int>(setup_.inner.size());
+    }
     return n;
   }
 
@@ -499,55 +501,67 @@ class EngineT final : public Engine {
                                " values, caller passed " + std::to_string(count));
   }
 
-  // the tiles of direction pass d of the FP32-bulk flux (dir_tile_counts)
-  Tiles make_dir_tiles(int d) const {
+  // A tile table over every block: count(B, ntx, nty) gives block B's tiles
+  // in x and y and returns its total; blocks laid out in order_ (the
+  // schedule), cbegin in block order.
+  template <class Count>
+  Tiles build_tiles(Count &&count, int halo = 0) const {
     Tiles t{};
     t.nblk = static_cast<int>(blocks_.size());
+    t.halo = halo;
+    int n[kMaxBlocks] = {};
     int acc = 0;
     for (int b = 0; b < t.nblk; ++b) {
-      const DevBlock &B = blocks_[b];
-      int n0 = 0, n1 = 0, n2 = 0;
-      dir_tile_counts(d, B.mx, B.my, B.mz, n0, n1, n2);
-      t.begin[b] = acc;
-      t.ntx[b] = n0;
-      t.nty[b] = n1;
-      acc += n0 * n1 * n2;
+      n[b] = count(blocks_[b], t.ntx[b], t.nty[b]);
+      t.cbegin[b] = acc;
+      acc += n[b];
+    }
+    acc = 0;
+    for (int s = 0; s < t.nblk; ++s) {
+      const int b = order_.empty() ? s : order_[s];
+      t.block[s] = b;
+      t.begin[s] = acc;
+      acc += n[b];
     }
     t.begin[t.nblk] = acc;
     return t;
+  }
+
+  // the tiles of direction pass d of the FP32-bulk flux (dir_tile_counts)
+  Tiles make_dir_tiles(int d) const {
+    const int march = kFluxVariant[flux_variant_].march;
+    return build_tiles([d, march](const DevBlock &B, int &ntx, int &nty) {
+      int n2 = 0;
+      dir_tile_counts(d, march, B.mx, B.my, B.mz, ntx, nty, n2);
+      return ntx * nty * n2;
+    });
   }
 
   // columns of kTX x kTY cells over kFluxKC planes (the k-marching flux kernel)
   Tiles make_col_tiles() const {
-    Tiles t{};
-    t.nblk = static_cast<int>(blocks_.size());
-    int acc = 0;
-    for (int b = 0; b < t.nblk; ++b) {
-      const DevBlock &B = blocks_[b];
-      t.begin[b] = acc;
-      t.ntx[b] = (B.mx + kTX - 1) / kTX;
-      t.nty[b] = (B.my + kTY - 1) / kTY;
-      acc += t.ntx[b] * t.nty[b] * ((B.mz + kFluxKC - 1) / kFluxKC);
-    }
-    t.begin[t.nblk] = acc;
-    return t;
+    return build_tiles([](const DevBlock &B, int &ntx, int &nty) {
+      ntx = (B.mx + kTX - 1) / kTX;
+      nty = (B.my + kTY - 1) / kTY;
+      return ntx * nty * ((B.mz + kFluxKC - 1) / kFluxKC);
+    });
   }
 
   Tiles make_tiles(int halo) const {
-    Tiles t{};
-    t.nblk = static_cast<int>(blocks_.size());
-    t.halo = halo;
-    int acc = 0;
-    for (int b = 0; b < t.nblk; ++b) {
-      const DevBlock &B = blocks_[b];
-      t.begin[b] = acc;
-      t.ntx[b] = (B.mx + 2 * halo + kTX - 1) / kTX;
-      t.nty[b] = (B.my + 2 * halo + kTY - 1) / kTY;
-      const int ntz = (B.mz + 2 * halo + kTZ - 1) / kTZ;
-      acc += t.ntx[b] * t.nty[b] * ntz;
-    }
-    t.begin[t.nblk] = acc;
-    return t;
+    return build_tiles(
+        [halo](const DevBlock &B, int &ntx, int &nty) {
+          ntx = (B.mx + 2 * halo + kTX - 1) / kTX;
+          nty = (B.my + 2 * halo + kTY - 1) / kTY;
+          return ntx * nty * ((B.mz + 2 * halo + kTZ - 1) / kTZ);
+        },
+        halo);
+  }
+
+  void make_all_tiles() {
+    tiles0_ = make_tiles(0);
+    tiles1_ = make_tiles(1);
+    tilesg_ = make_tiles(setup_.ngg);
+    col_tiles_ = make_col_tiles();
+    for (int d = 0; d < 3; ++d) dir_tiles_[d] = make_dir_tiles(d);
   }
 
   static dim3 grid(const Tiles &t) { return dim3(static_cast<unsigned>(t.begin[t.nblk])); }
@@ -581,16 +595,26 @@ class EngineT final : public Engine {
       for (int b = 0; b < static_cast<int>(blocks_.size()); ++b)
         k_pack32<C><<<pack_grid(b), 256, 0, stream_>>>(d_blocks_, b);
       mark("pack32");
-      k_flux_x<C><<<grid(dir_tiles_[0]), kCta, 0, stream_>>>(d_blocks_, dir_tiles_[0]);
-      mark("flux_x");
-      k_flux_march<C, 1><<<grid(dir_tiles_[1]), kCta, 0, stream_>>>(d_blocks_, dir_tiles_[1]);
-      mark("flux_y");
-      if (setup_.params.dim == 3) {
-        k_flux_march<C, 2><<<grid(dir_tiles_[2]), kCta, 0, stream_>>>(d_blocks_, dir_tiles_[2]);
-        mark("flux_z");
+      switch (flux_variant_) {
+        case 0: launch_flux_passes<kFluxVariant[0].min_blocks, kFluxVariant[0].march>(); break;
+        case 1: launch_flux_passes<kFluxVariant[1].min_blocks, kFluxVariant[1].march>(); break;
+        case 2: launch_flux_passes<kFluxVariant[2].min_blocks, kFluxVariant[2].march>(); break;
+        default: launch_flux_passes<kFluxVariant[3].min_blocks, kFluxVariant[3].march>(); break;
       }
     } else
       k_flux_col<C><<<grid(col_tiles_), kFluxThreads, col_smem_, stream_>>>(d_blocks_, col_tiles_);
+  }
+
+  template <int MINB, int MARCH>
+  void launch_flux_passes() {
+    k_flux_x<C, MINB><<<grid(dir_tiles_[0]), kCta, 0, stream_>>>(d_blocks_, dir_tiles_[0]);
+    mark("flux_x");
+    k_flux_march<C, 1, MINB, MARCH><<<grid(dir_tiles_[1]), kCta, 0, stream_>>>(d_blocks_, dir_tiles_[1]);
+    mark("flux_y");
+    if (setup_.params.dim == 3) {
+      k_flux_march<C, 2, MINB, MARCH><<<grid(dir_tiles_[2]), kCta, 0, stream_>>>(d_blocks_, dir_tiles_[2]);
+      mark("flux_z");
+    }
   }
 
   void launch_props() {
@@ -626,8 +650,10 @@ class EngineT final : public Engine {
     if (sur_on_) launch_classify();
     launch_source();
     mark("source");
+    launch_halo(kHaloTurb);
     launch_flux();
     if constexpr (!C::mixed) mark("flux");
+    launch_halo(kHaloSpec);
   }
 
   // returns the dq buffer holding the final increment (0 dq, 1 dq0, 2 dqk)
@@ -649,8 +675,10 @@ class EngineT final : public Engine {
         final_dq_ = p.dplur_inner_step > 0 ? 0 : 1;
       } else {
         int in = 1;
+        launch_halo(kHaloHspec);
         for (int s = 0; s < p.dplur_inner_step; ++s) {
           const int out = (s % 2 == 0) ? 2 : 0;
+          launch_halo(kHaloDq, in);
           k_sweep<C><<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_, in, out);
           mark("dplur_sweep");
           in = out;
@@ -781,10 +809,46 @@ class EngineT final : public Engine {
   void launch_inner() {
     for (int q = 0; q < static_cast<int>(setup_.inner.size()); ++q) {
       const HostInner &f = setup_.inner[q];
+      if (f.n_point[0] * f.n_point[1] * f.n_point[2] <= 0) continue;
+      const int tg = setup_.exact_inner ? setup_.ngg : 0;
+      int np = 1;
+      for (int d = 0; d < 3; ++d) np *= f.n_point[d] + (d != f.face && f.n_point[d] > 1 ? 2 * tg : 0);
+      k_inner<C><<<(np + 127) / 128, 128, 0, stream_>>>(d_blocks_, d_inner_, q, setup_.exact_inner, tg);
+      mark("inner_face");
+    }
+    launch_halo(kHaloVel);
+  }
+
+  // exact inner faces: the first ghost layer of one array set copied from the
+  // neighbours (k_halo); nothing otherwise
+  void launch_halo(int set, int dq_sel = 0) {
+    if (!setup_.exact_inner) return;
+    // the spectral radii, increments and enthalpies have their ghost layer under DPLUR only
+    if (set != kHaloTurb && set != kHaloVel && setup_.params.implicit_method != 1) return;
+    for (int q = 0; q < static_cast<int>(setup_.inner.size()); ++q) {
+      const HostInner &f = setup_.inner[q];
       const int np = f.n_point[0] * f.n_point[1] * f.n_point[2];
       if (np <= 0) continue;
-      k_inner<C><<<(np + 127) / 128, 128, 0, stream_>>>(d_blocks_, d_inner_, q);
-      mark("inner_face");
+      k_halo<C><<<(np + 127) / 128, 128, 0, stream_>>>(d_blocks_, d_inner_, q, set, dq_sel);
+      mark("halo");
+    }
+  }
+
+  // exact inner faces: the block faces the DPLUR sweeps cross (each inner
+  // face must cover its whole block face; FP64 path, 3-D grids)
+  void mark_exact_inner_faces() {
+    if (C::mixed) throw std::runtime_error("exact inner faces are implemented on the FP64 path only");
+    if (setup_.params.dim != 3) throw std::runtime_error("exact inner faces are implemented for 3-D grids");
+    for (const HostInner &f : setup_.inner) {
+      DevBlock &B = blocks_.at(f.block);
+      const int ext[3] = {B.mx, B.my, B.mz};
+      for (int q = 0; q < 3; ++q) {
+        if (q == f.face) continue;
+        if (f.n_point[q] != ext[q])
+          throw std::runtime_error("exact inner faces must cover whole block faces (block " + std::to_string(f.block) +
+                                   ")");
+      }
+      B.inner_mask |= 1 << (2 * f.face + (f.direction > 0 ? 1 : 0));
     }
   }
 
@@ -824,6 +888,47 @@ class EngineT final : public Engine {
 
   int residual_tiles() const override { return tiles0_.begin[tiles0_.nblk]; }
 
+  void set_tuning(int schedule, int flux_variant) override {
+    if (schedule < 0 || schedule > 1) throw std::runtime_error("schedule must be 0 or 1");
+    if (flux_variant < 0 || flux_variant >= flux_variants()) throw std::runtime_error("no such flux variant");
+    synchronize();
+    order_.clear();
+    if (schedule == 1) {
+      for (int b = 0; b < static_cast<int>(blocks_.size()); ++b) order_.push_back(b);
+      auto cells = [this](int b) { return static_cast<int64_t>(blocks_[b].mx) * blocks_[b].my * blocks_[b].mz; };
+      std::stable_sort(order_.begin(), order_.end(), [&](int a, int b) { return cells(a) > cells(b); });
+    }
+    flux_variant_ = flux_variant;
+    make_all_tiles();
+    for (auto &g : graphs_)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+  }
+
+  int flux_variants() const override { return C::mixed ? kFluxVariants : 1; }
+
+  double time_stages(int reps) override {
+    upload_params();
+    auto pass = [this] {
+      launch_source();
+      launch_halo(kHaloTurb);
+      launch_flux();
+      launch_halo(kHaloSpec);
+      launch_implicit();
+    };
+    pass();
+    cuda_check(cudaEventRecord(ev0_, stream_), "event");
+    for (int r = 0; r < reps; ++r) pass();
+    cuda_check(cudaEventRecord(ev1_, stream_), "event");
+    cuda_check(cudaGetLastError(), "tuning launch");
+    cuda_check(cudaEventSynchronize(ev1_), "tuning sync");
+    float ms = 0;
+    cuda_check(cudaEventElapsedTime(&ms, ev0_, ev1_), "event time");
+    return ms / std::max(1, reps);
+  }
+
   void residual_sums_to(double *partial, double *out) override {
     const int n_part = tiles0_.begin[tiles0_.nblk];
     k_res_partial<<<grid(tiles0_), block3(), 0, stream_>>>(d_blocks_, tiles0_, partial);
@@ -850,6 +955,8 @@ class EngineT final : public Engine {
   unsigned int *d_bad_ = nullptr;
   std::vector<void *> allocations_;
   Tiles tiles0_, tiles1_, tilesg_, col_tiles_, dir_tiles_[3];
+  std::vector<int> order_;  // the blocks' schedule in every tile table (empty: block order)
+  int flux_variant_ = 0;    // kFluxVariant entry of the FP32-bulk flux passes
   size_t source_smem_ = 0, flux_smem_ = 0, col_smem_ = 0, dq0_smem_ = 0;
   int final_dq_ = 0;
   cudaGraphExec_t graphs_[4] = {nullptr, nullptr, nullptr, nullptr};

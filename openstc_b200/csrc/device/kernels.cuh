@@ -22,10 +22,7 @@ constexpr double delta_beta = beta_1 - beta_2, delta_gamma = gamma1 - gamma2;
 // ---------------------------------------------------------------- tiling
 template <int TX, int TY, int TZ>
 __device__ __forceinline__ bool tile_cell(const Tiles &T, int &b, int &i, int &j, int &k, const DevBlock *blks) {
-  int t = blockIdx.x;
-  b = 0;
-  while (b + 1 < T.nblk && t >= T.begin[b + 1]) ++b;
-  t -= T.begin[b];
+  int t = tile_of(T, blockIdx.x, b);
   const int tx = t % T.ntx[b];
   t /= T.ntx[b];
   const int ty = t % T.nty[b];

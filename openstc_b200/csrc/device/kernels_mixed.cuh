@@ -833,12 +833,23 @@ __global__ void __launch_bounds__(kFluxThreads, 4) k_flux_mx_col(const DevBlock 
 //   y, z: each thread marches kMarch cells along d, carrying the lower face
 //      from one cell to the next; lanes run along i, the CTA's 4 warps over
 //      the remaining index (k for y, j for z).
-constexpr int kMarch = 8;
 constexpr int kXSeg = 31;  // cells per warp of the x pass
+// The variants of the passes an autotuner chooses from: resident CTAs per
+// SM the register allocator is asked to allow (8 caps a thread at 64
+// registers, ~400 B of spills) and the cells a thread of the y / z pass
+// marches over.  Measured at 384x192x64 with a march of 8, the three passes
+// take 5.7 ms at 4 CTAs per SM, 5.0 at 6, 4.8 at 7, 4.4 at 8.  Every variant
+// computes the same values.
+struct FluxVariant {
+  int min_blocks, march;
+};
+constexpr int kFluxVariants = 4;
+constexpr FluxVariant kFluxVariant[kFluxVariants] = {{8, 8}, {8, 16}, {6, 8}, {4, 8}};
 
 // Tiles of pass d over every block: (x) i-segments x row groups x k,
-// (y) i-groups x k-groups x j-segments, (z) i-groups x j-groups x k-segments.
-inline void dir_tile_counts(int d, int mx, int my, int mz, int &n0, int &n1, int &n2) {
+// (y) i-groups x k-groups x j-segments, (z) i-groups x j-groups x k-segments
+// of kMarch cells.
+inline void dir_tile_counts(int d, int kMarch, int mx, int my, int mz, int &n0, int &n1, int &n2) {
   if (d == 0) {
     n0 = (mx + kXSeg - 1) / kXSeg;
     n1 = (my + kTY - 1) / kTY;
@@ -855,10 +866,7 @@ inline void dir_tile_counts(int d, int mx, int my, int mz, int &n0, int &n1, int
 }
 
 __device__ __forceinline__ void dir_tile(const Tiles &T, int &b, int &t0, int &t1, int &t2) {
-  int t = blockIdx.x;
-  b = 0;
-  while (b + 1 < T.nblk && t >= T.begin[b + 1]) ++b;
-  t -= T.begin[b];
+  int t = tile_of(T, blockIdx.x, b);
   t0 = t % T.ntx[b];
   t /= T.ntx[b];
   t1 = t % T.nty[b];
@@ -920,8 +928,8 @@ __global__ void __launch_bounds__(256) k_pack32_static(const DevBlock *__restric
   }
 }
 
-template <class C>
-__global__ void __launch_bounds__(kCta, 4) k_flux_x(const DevBlock *__restrict__ blks, Tiles T) {
+template <class C, int MINB>
+__global__ void __launch_bounds__(kCta, MINB) k_flux_x(const DevBlock *__restrict__ blks, Tiles T) {
   constexpr int NV = C::nv;
   int b, t0, t1, t2;
   dir_tile(T, b, t0, t1, t2);
@@ -947,8 +955,8 @@ __global__ void __launch_bounds__(kCta, 4) k_flux_x(const DevBlock *__restrict__
   if (cell) local_time_step_s<C>(B, fp32::Src32<C>{B.f32, B.G.size}, f, j, k, B.G.at(f, j, k), nd);
 }
 
-template <class C, int D>
-__global__ void __launch_bounds__(kCta, 4) k_flux_march(const DevBlock *__restrict__ blks, Tiles T) {
+template <class C, int D, int MINB, int kMarch>
+__global__ void __launch_bounds__(kCta, MINB) k_flux_march(const DevBlock *__restrict__ blks, Tiles T) {
   constexpr int NV = C::nv;
   static_assert(D == 1 || D == 2, "march passes run along y or z");
   int b, t0, t1, t2;

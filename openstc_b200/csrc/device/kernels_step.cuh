@@ -203,10 +203,7 @@ constexpr int kFluxKC = 8;                  // k planes per column
 constexpr int kFluxThreads = kCta + 32;     // 4 compute warps + the minus-face warp
 
 __device__ __forceinline__ void col_tile(const Tiles &T, int &b, int &i0, int &j0, int &k0) {
-  int t = blockIdx.x;
-  b = 0;
-  while (b + 1 < T.nblk && t >= T.begin[b + 1]) ++b;
-  t -= T.begin[b];
+  int t = tile_of(T, blockIdx.x, b);
   const int tx = t % T.ntx[b];
   t /= T.ntx[b];
   const int ty = t % T.nty[b];
@@ -625,7 +622,7 @@ __global__ void __launch_bounds__(kCta, OSTC_SWEEP_MIN_BLOCKS) k_sweep(const Dev
     const bool plus = q >= 3;
     const int id = d == 0 ? i : (d == 1 ? j : k);
     const int ext = d == 0 ? B.mx : (d == 1 ? B.my : B.mz);
-    if (plus ? id == ext - 1 : id == 0) continue;
+    if ((plus ? id == ext - 1 : id == 0) && !(B.inner_mask >> (2 * d + (plus ? 1 : 0)) & 1)) continue;
     const int64_t gs = d == 0 ? 1 : (d == 1 ? sx : sxy), ds = d == 0 ? 1 : (d == 1 ? dsx : dsxy);
     const int64_t on = plus ? n + gs : n - gs, od = plus ? nd + ds : nd - ds;
     const double sr = isr[d * szd + od];
@@ -1129,13 +1126,21 @@ struct DevInner {
   int start[3], end[3], loop_dir[3], tstart[3], tloop_dir[3], src_tar[3], n_point[3];
 };
 
+// exact: the shared plane is computed identically by both blocks and is not
+// re-averaged, and the ghost copy also covers the face's tangential ghost
+// rows (tg = ngg), which the viscous stencils read next to the face
 template <class C>
-__global__ void k_inner(const DevBlock *__restrict__ blks, const DevInner *__restrict__ faces, int fi) {
+__global__ void k_inner(const DevBlock *__restrict__ blks, const DevInner *__restrict__ faces, int fi, bool exact,
+                        int tg) {
   const DevInner &f = faces[fi];
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int np = f.n_point[0] * f.n_point[1] * f.n_point[2];
+  int ext[3];
+  for (int q = 0; q < 3; ++q) ext[q] = f.n_point[q] + (q != f.face && f.n_point[q] > 1 ? 2 * tg : 0);
+  const int np = ext[0] * ext[1] * ext[2];
   if (t >= np) return;
-  const int nn[3] = {t % f.n_point[0], (t / f.n_point[0]) % f.n_point[1], t / (f.n_point[0] * f.n_point[1])};
+  int nn[3] = {t % ext[0], (t / ext[0]) % ext[1], t / (ext[0] * ext[1])};
+  for (int q = 0; q < 3; ++q)
+    if (ext[q] != f.n_point[q]) nn[q] -= tg;
   int idx[3], it[3], d[3];
   for (int q = 0; q < 3; ++q) {
     d[q] = f.loop_dir[q] * nn[q];
@@ -1148,6 +1153,7 @@ __global__ void k_inner(const DevBlock *__restrict__ blks, const DevInner *__res
   const int64_t sz = B.G.size, tsz = Tb.G.size;
   const int face_dir = f.direction > 0 ? f.start[f.face] : f.end[f.face];
   if (idx[f.face] == face_dir) {
+    if (exact) return;
     OSTC_UNROLL for (int l = 0; l < C::nv; ++l) {
       const double ave = 0.5 * (Tb.cv[l * tsz + tn] + B.cv[l * sz + n]);
       B.cv[l * sz + n] = ave;
@@ -1157,6 +1163,55 @@ __global__ void k_inner(const DevBlock *__restrict__ blks, const DevInner *__res
   } else {
     for (int l = 0; l < 6; ++l) B.bv[l * sz + n] = Tb.bv[l * tsz + tn];
     OSTC_UNROLL for (int l = 0; l < C::nsc; ++l) B.sv[l * sz + n] = Tb.sv[l * tsz + tn];
+  }
+}
+
+// Exact inner faces: the first ghost layer of an array that the stencils
+// read across the face, copied from the neighbour's interior (the point map
+// of k_inner).  set: 0 mu_t and lambda_t, 1 |V|, 2 the inviscid spectral
+// radii, 3 the DPLUR increments of buffer dq_sel (0 dq, 1 dq0, 2 dqk), 4 the
+// species enthalpies of the sweeps.
+enum HaloSet { kHaloTurb = 0, kHaloVel = 1, kHaloSpec = 2, kHaloDq = 3, kHaloHspec = 4 };
+
+template <class C>
+__global__ void k_halo(const DevBlock *__restrict__ blks, const DevInner *__restrict__ faces, int fi, int set,
+                       int dq_sel) {
+  const DevInner &f = faces[fi];
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int np = f.n_point[0] * f.n_point[1] * f.n_point[2];
+  if (t >= np) return;
+  const int nn[3] = {t % f.n_point[0], (t / f.n_point[0]) % f.n_point[1], t / (f.n_point[0] * f.n_point[1])};
+  int idx[3], it[3], d[3];
+  for (int q = 0; q < 3; ++q) {
+    d[q] = f.loop_dir[q] * nn[q];
+    idx[q] = f.start[q] + d[q];
+  }
+  for (int q = 0; q < 3; ++q) it[q] = f.tstart[q] + f.tloop_dir[q] * d[f.src_tar[q]];
+  const int face_dir = f.direction > 0 ? f.start[f.face] : f.end[f.face];
+  if (abs(idx[f.face] - face_dir) != 1) return;
+  const DevBlock &B = blks[f.block];
+  const DevBlock &Tb = blks[f.target_block];
+  if (set == kHaloTurb || set == kHaloVel) {
+    const int64_t n = B.G.at(idx[0], idx[1], idx[2]), tn = Tb.G.at(it[0], it[1], it[2]);
+    if (set == kHaloVel) {
+      B.vel[n] = Tb.vel[tn];
+    } else if constexpr (C::turb) {
+      B.mut[n] = Tb.mut[tn];
+      B.turb_cond[n] = Tb.turb_cond[tn];
+    }
+    return;
+  }
+  const int64_t n = B.D.at(idx[0], idx[1], idx[2]), tn = Tb.D.at(it[0], it[1], it[2]);
+  const int64_t sz = B.D.size, tsz = Tb.D.size;
+  if (set == kHaloSpec) {
+    for (int l = 0; l < 3; ++l) B.inv_spec[l * sz + n] = Tb.inv_spec[l * tsz + tn];
+  } else if (set == kHaloDq) {
+    double *dst = dq_sel == 0 ? B.dq : (dq_sel == 1 ? B.dq0 : B.dqk);
+    const double *src = dq_sel == 0 ? Tb.dq : (dq_sel == 1 ? Tb.dq0 : Tb.dqk);
+    OSTC_UNROLL for (int l = 0; l < C::nv; ++l) dst[l * sz + n] = src[l * tsz + tn];
+  } else if (set == kHaloHspec) {
+    if constexpr (C::ns > 0)
+      OSTC_UNROLL for (int l = 0; l < C::ns; ++l) B.h_spec[l * sz + n] = Tb.h_spec[l * tsz + tn];
   }
 }
 
@@ -1222,7 +1277,11 @@ static __global__ void __launch_bounds__(kCta) k_res_partial(const DevBlock *__r
   if (tid < 4) {
     double v = 0;
     for (int w = 0; w < kCta / 32; ++w) v += red[tid][w];
-    partial[static_cast<int64_t>(blockIdx.x) * 4 + tid] = v;
+    // stored in block order, so that the reduction's order and result do
+    // not depend on the schedule of the blocks
+    int bb = 0;
+    const int slot = tile_of(T, blockIdx.x, bb) + T.cbegin[bb];
+    partial[static_cast<int64_t>(slot) * 4 + tid] = v;
   }
 }
 

@@ -193,7 +193,7 @@ class PltPipeline {
 Driver::~Driver() = default;
 
 Driver::Driver(const std::string &dir, const DriverOptions &o) : case_dir(dir), opt(o), parameter(dir) {
-  mesh = Mesh(parameter);
+  mesh = Mesh(parameter, opt.exact_inner);
   spec = Species(parameter);
   reac = Reaction(parameter, spec);
   const bool species = parameter.get_bool("species");
@@ -412,6 +412,7 @@ void Driver::initialize_computation() {
   s.wall_points = wall_points;
   s.device = opt.device;
   s.precision = opt.precision;
+  s.exact_inner = opt.exact_inner;
   plt_out_.reset();  // bound to the engine it copies from
   engine_ = make_engine(s);
   for (int b = 0; b < mesh.n_block; ++b) {
@@ -429,7 +430,46 @@ void Driver::initialize_computation() {
       engine_->set_field(b, F_SV, field[b].sv.data(), static_cast<int64_t>(field[b].sv.size()));
   }
   engine_->initialize();
+  // a choice the autotuner recorded for this configuration and these blocks
+  std::ifstream tuned(std::filesystem::path(case_dir) / "output" / "message" / "autotune.txt");
+  std::string key;
+  int schedule = 0, variant = 0;
+  if (tuned && std::getline(tuned, key) && key == tuning_key() && (tuned >> schedule >> variant) &&
+      variant < engine_->flux_variants())
+    engine_->set_tuning(schedule, variant);
   if (!opt.quiet) std::printf("The flowfield is completely initialized on GPU.\n");
+}
+
+std::string Driver::tuning_key() const {
+  std::string k = "mix " + std::to_string(mix) + " rans " + std::to_string(rans ? 1 : 0) + " precision " +
+                  std::to_string(opt.precision) + " exact " + std::to_string(opt.exact_inner ? 1 : 0) + " blocks";
+  for (const auto &b : mesh.block) k += " " + std::to_string(b.mx) + "x" + std::to_string(b.my) + "x" + std::to_string(b.mz);
+  return k;
+}
+
+Driver::Tuning Driver::autotune(int reps) {
+  Engine &E = engine();
+  Tuning t;
+  t.ms = -1;
+  for (int schedule = 0; schedule < 2; ++schedule) {
+    for (int v = 0; v < E.flux_variants(); ++v) {
+      E.set_tuning(schedule, v);
+      const double ms = E.time_stages(reps);
+      ++t.candidates;
+      if (schedule == 0 && v == 0) t.ms_default = ms;
+      if (t.ms < 0 || ms < t.ms) {
+        t.ms = ms;
+        t.schedule = schedule;
+        t.flux_variant = v;
+      }
+    }
+  }
+  E.set_tuning(t.schedule, t.flux_variant);
+  const std::filesystem::path dir = std::filesystem::path(case_dir) / "output" / "message";
+  std::filesystem::create_directories(dir);
+  std::ofstream out(dir / "autotune.txt");
+  out << tuning_key() << '\n' << t.schedule << ' ' << t.flux_variant << '\n' << t.ms << ' ' << t.ms_default << '\n';
+  return t;
 }
 
 double Driver::compute_residual(int step_no, const double raw[4]) {

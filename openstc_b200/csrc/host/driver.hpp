@@ -22,6 +22,7 @@ struct DriverOptions {
   int device = 0;
   bool quiet = false;
   int precision = 0;  // 0 FP64, 1 FP32-bulk / FP64-critical
+  bool exact_inner = false;  // multi-block grids computed as one block (ostc_options::exact_inner)
 };
 
 class Driver {
@@ -42,6 +43,19 @@ class Driver {
   double advance(int n);
 
   void write_field(const std::string &path);
+
+  // The autotuner: times every (schedule, flux variant) pair of the engine
+  // (Engine::time_stages, `reps` passes each) on this case, applies the
+  // fastest and records it in output/message/autotune.txt under a key of the
+  // configuration and block sizes; initialize_computation applies a recorded
+  // choice whose key matches.  Returns the chosen pair, its time per pass and
+  // the time of the default (0, 0).
+  struct Tuning {
+    int schedule = 0, flux_variant = 0, candidates = 0;
+    double ms = 0, ms_default = 0;
+  };
+  Tuning autotune(int reps);
+  std::string tuning_key() const;
   bool initialized() const { return engine_ != nullptr; }
   Engine &engine();
 

@@ -209,7 +209,8 @@ void Block::trim_ghost_layers() {
 }
 
 // ---------------------------------------------------------------- mesh
-Mesh::Mesh(Parameter &parameter) : dimension(parameter.get_int("dimension")), ngg(parameter.get_int("ngg")) {
+Mesh::Mesh(Parameter &parameter, bool exact_inner)
+    : dimension(parameter.get_int("dimension")), ngg(parameter.get_int("ngg")) {
   const std::string &dir = parameter.case_dir();
   read_grid(dir);
   parameter.set("n_block", n_block);
@@ -218,6 +219,8 @@ Mesh::Mesh(Parameter &parameter) : dimension(parameter.get_int("dimension")), ng
   const double s = parameter.get_real("gridScale");
   if (std::abs(s - 1.0) > 1e-15) scale(s);
   init_ghost_grid();
+  // after the edge and corner completion: the neighbours' own ghost rows
+  if (exact_inner) init_inner_ghost_grid(ngg + 1);
   for (auto &b : block) b.compute_jac_metric(dir);
   for (auto &b : block) b.trim_ghost_layers();
 }
@@ -421,8 +424,10 @@ void Mesh::init_ghost_grid() {
   }
 }
 
-void Mesh::init_inner_ghost_grid() {
-  // src/Mesh.cpp:945-993
+void Mesh::init_inner_ghost_grid(int tangential_ghosts) {
+  // src/Mesh.cpp:945-993.  tangential_ghosts > 0 extends the copy by that many
+  // rows past the face's tangential ends (exact inner faces; faces that cover
+  // the whole block face in the same orientation as the neighbour's).
   for (auto &B : block) {
     for (const auto &fc : B.inner_face) {
       const Block &N = block[fc.target_block];
@@ -433,6 +438,16 @@ void Mesh::init_inner_ghost_grid() {
       lo[fc.face] += shift;
       hi[fc.face] += shift;
       tlo[fc.target_face] += fc.target_direction > 0 ? -1 : 1;
+      for (int q = 0; q < 3 && tangential_ghosts > 0; ++q) {
+        if (q == fc.face || lo[q] == hi[q]) continue;
+        int t = 0;  // the target direction that runs along this one (src_tar: target -> source)
+        while (t < 2 && fc.src_tar[t] != q) ++t;
+        if (fc.loop_dir[q] < 0 || fc.target_loop_dir[t] < 0)
+          throw ParameterError("exact inner faces need faces oriented as their neighbours'");
+        lo[q] -= tangential_ghosts;
+        hi[q] += tangential_ghosts;
+        tlo[t] -= tangential_ghosts;
+      }
       int d[3];
       for (int i1 = lo[0]; fc.loop_dir[0] * (i1 - hi[0]) != 1; i1 += fc.loop_dir[0]) {
         d[0] = i1 - lo[0];

@@ -87,7 +87,10 @@ class Mesh {
   std::vector<Block> block;
 
   Mesh() = default;
-  explicit Mesh(Parameter &parameter);
+  // exact_inner: the ghost grid of every inner face, its tangential ghost
+  // rows included, is the neighbour's grid, so that the metrics next to the
+  // face are those of the same grid as one block (see DriverOptions)
+  explicit Mesh(Parameter &parameter, bool exact_inner = false);
   Block &operator[](size_t i) { return block[i]; }
   const Block &operator[](size_t i) const { return block[i]; }
 
@@ -97,7 +100,7 @@ class Mesh {
   void read_inner_interface(const std::string &case_dir);
   void scale(double s);
   void init_ghost_grid();
-  void init_inner_ghost_grid();
+  void init_inner_ghost_grid(int tangential_ghosts = 0);
 };
 
 std::string process_file_name(const std::string &stem, int id, const std::string &ext);

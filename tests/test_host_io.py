@@ -213,3 +213,34 @@ def test_blended_initial_field_reads_back(tmp_path):
     assert np.allclose(z["H2"][:, 0, :], 0.4, rtol=1e-12)
     grid = cases._read_grid(case)[0]
     assert np.array_equal(z["y"], grid[1])
+
+
+def test_exact_inner_faces_give_the_one_block_geometry(tmp_path):
+    """With exact inner faces the ghost grid of each inner face, its
+    tangential ghost rows included, is the neighbour's grid, so every block's
+    coordinates, Jacobian and metrics over its whole ghosted extent equal
+    those of the same grid as one block; the reference's completion of the
+    ghost corners (src/Mesh.cpp:864-943) differs from them in the last bits."""
+    mxs, my, mz = [9, 7, 11], 12, 6
+    total = sum(mxs) - (len(mxs) - 1)
+    one = ostc.Driver(cases.mixing_layer_case(tmp_path / "one", mx=total, my=my, mz=mz, total_step=1))
+    many = cases.multiblock_case(tmp_path / "many", mxs=mxs, my=my, mz=mz, total_step=1)
+    g = one.info().ngg
+    for exact in (True, False):
+        drv = ostc.Driver(many, exact_inner=exact)
+        worst = 0.0
+        for f in ("x", "y", "z", "jac", "metric"):
+            whole = one.host_field(0, f)
+            i0 = 0
+            for b, m in enumerate(mxs):
+                part = drv.host_field(b, f)
+                lo, hi = max(i0 - g, -g), min(i0 + m + g, total + g)
+                seg = part[..., lo - (i0 - g):lo - (i0 - g) + hi - lo]
+                worst = max(worst, float(np.max(np.abs(seg - whole[..., lo + g:hi + g]))))
+                i0 += m - 1
+        if exact:
+            assert worst == 0.0
+        else:
+            assert worst > 0.0
+        drv.close()
+    one.close()
