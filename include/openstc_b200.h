@@ -258,6 +258,11 @@ int ostc_surrogate_normalisation(const ostc_surrogate *s, float *in_mu, float *i
    Takes effect for drivers at their next ostc_driver_set_surrogate. */
 typedef struct ostc_surrogate_gate {
   float t_min, t_max, lp_min, lp_max, ldt_min, ldt_max, defect_tol, rel_max, out_max, y_floor;
+  /* the judge: every accepted increment must agree with the diagonal
+     point-implicit increment (dt omega_k / rho) / (1 + dt omega_d,k / (rho Y_k))
+     of the cell's own chemistry (the DA treatment) within judge_rel of it
+     plus judge_abs (Y_k + y_floor); judge_rel < 0 turns it off */
+  float judge_rel, judge_abs;
 } ostc_surrogate_gate;
 int ostc_surrogate_get_gate(const ostc_surrogate *s, ostc_surrogate_gate *g);
 int ostc_surrogate_set_gate(ostc_surrogate *s, const ostc_surrogate_gate *g);

@@ -47,7 +47,7 @@ class SurrogateEval(C.Structure):
 
 class SurrogateGate(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("t_min", "t_max", "lp_min", "lp_max", "ldt_min", "ldt_max", "defect_tol",
-                                         "rel_max", "out_max", "y_floor")]
+                                         "rel_max", "out_max", "y_floor", "judge_rel", "judge_abs")]
 
 
 class Info(C.Structure):

@@ -341,7 +341,7 @@ class EngineT final : public Engine {
     n += 1;  // properties
     if (store_last) n += 1;
     if (residual) n += 2;
-    if (sur_on_) n += (C::mixed ? 4 : 2) * static_cast<int>(blocks_.size());  // candidates + inference (+ chemistry list)
+    if (sur_on_) n += (C::mixed ? 5 : 3) * static_cast<int>(blocks_.size());  // candidates, inference, judge (+ chemistry list)
     if (setup_.exact_inner) {  // the halo copies of exact inner faces
       int sets = 2;  // mu_t / lambda_t, |V|
       if (p.implicit_method == 1) sets += 2 + p.dplur_inner_step;  // spectral radii, enthalpies, each sweep's input
@@ -363,6 +363,12 @@ class EngineT final : public Engine {
     if (owner != this) {
       cuda_check(cudaMemcpyToSymbolAsync(cP, &setup_.params, sizeof(DevParams), 0, cudaMemcpyHostToDevice, stream_),
                  "upload params");
+      if constexpr (C::mix == 2) {
+        const sur::JudgeTables jt = sur::make_judge_tables(setup_.params);
+        cuda_check(cudaMemcpyToSymbolAsync(sur::cJ, &jt, sizeof(jt), 0, cudaMemcpyHostToDevice, stream_),
+                   "upload judge tables");
+        cuda_check(cudaStreamSynchronize(stream_), "upload judge tables");
+      }
       if constexpr (C::mixed) {
         const MixParams f = make_mix_params(setup_.params);
         cuda_check(cudaMemcpyToSymbolAsync(cF, &f, sizeof(MixParams), 0, cudaMemcpyHostToDevice, stream_),
@@ -642,6 +648,10 @@ class EngineT final : public Engine {
             d_blocks_, b, sur_, d_fb_count_, d_fb_list_, d_sur_stats_, d_sur_err_, d_fb_list_, d_fb_count_,
             last ? d_sur_phase_ : nullptr);
         mark("surrogate");
+        sur::k_sur_judge<C><<<static_cast<unsigned>(8 * num_sms_), 256, 0, stream_>>>(d_blocks_, b, sur_.gate,
+                                                                                     d_fb_list_, d_fb_count_,
+                                                                                     d_sur_stats_);
+        mark("surrogate_judge");
       }
     }
   }

@@ -14,6 +14,50 @@
 namespace ostc {
 namespace sur {
 
+// FP32 copies of the mechanism tables the judge reads (one per translation
+// unit, uploaded with the FP64 tables): sign(A) and ln|A| of both Arrhenius
+// sets, b, Ea, Troe parameters, third-body efficiencies, W_k and NASA-7.
+struct JudgeTables {
+  float sA[kMaxReac], lnA[kMaxReac], b[kMaxReac], Ea[kMaxReac];
+  float sA2[kMaxReac], lnA2[kMaxReac], b2[kMaxReac], Ea2[kMaxReac];
+  float troe_a[kMaxReac], troe_t3[kMaxReac], troe_t1[kMaxReac], troe_t2[kMaxReac];
+  float tb[kMaxReac * kMaxSpec];
+  float mw[kMaxSpec], t_low[kMaxSpec], t_mid[kMaxSpec], low[kMaxSpec * 7], high[kMaxSpec * 7];
+};
+
+static __constant__ JudgeTables cJ;
+
+inline JudgeTables make_judge_tables(const DevParams &p) {
+  JudgeTables j{};
+  auto sgn = [](double a) { return a > 0 ? 1.f : (a < 0 ? -1.f : 0.f); };
+  for (int r = 0; r < kMaxReac; ++r) {
+    j.sA[r] = sgn(p.A[r]);
+    j.lnA[r] = static_cast<float>(p.lnA[r]);
+    j.b[r] = static_cast<float>(p.b[r]);
+    j.Ea[r] = static_cast<float>(p.Ea[r]);
+    j.sA2[r] = sgn(p.A2[r]);
+    j.lnA2[r] = static_cast<float>(p.lnA2[r]);
+    j.b2[r] = static_cast<float>(p.b2[r]);
+    j.Ea2[r] = static_cast<float>(p.Ea2[r]);
+    j.troe_a[r] = static_cast<float>(p.troe_a[r]);
+    j.troe_t3[r] = static_cast<float>(p.troe_t3[r]);
+    j.troe_t1[r] = static_cast<float>(p.troe_t1[r]);
+    j.troe_t2[r] = static_cast<float>(p.troe_t2[r]);
+  }
+  for (int q = 0; q < kMaxReac * kMaxSpec; ++q) j.tb[q] = static_cast<float>(p.tb[q]);
+  for (int k = 0; k < kMaxSpec; ++k) {
+    j.mw[k] = static_cast<float>(p.mw[k]);
+    j.t_low[k] = static_cast<float>(p.t_low[k]);
+    j.t_mid[k] = static_cast<float>(p.t_mid[k]);
+  }
+  for (int q = 0; q < kMaxSpec * 7; ++q) {
+    j.low[q] = static_cast<float>(p.low[q]);
+    j.high[q] = static_cast<float>(p.high[q]);
+  }
+  return j;
+}
+
+
 // One FP64 EPI step at fixed density: rho dY = (I - dt J)^-1 dt omega, with
 // omega and J as the solver computes them (finite_rate_chemistry and
 // compute_chem_src_jacobian, src/FiniteRateChem.cu:7-194; EPI, :211-234).
@@ -49,6 +93,118 @@ __device__ inline void epi_increment(double T, double rho, const double *Y, doub
   for (int k = 0; k < NS; ++k) dy[k] = dt * x[k] / rho;
 }
 
+// The judge's increment of one cell in FP32: the point-implicit step with the
+// diagonal of the chemistry Jacobian (the reference's DA treatment,
+// src/FiniteRateChem.cu:196-209, 400-412), dY_k = (dt omega_k / rho) /
+// (1 + dt omega_d,k / (rho Y_k)), from the production and destruction rates of
+// finite_rate_chemistry (src/FiniteRateChem.cu:7-171; every rate and
+// equilibrium constant as one exponential, exponents clamped to the FP32
+// range).  The full EPI step (I - dt J)^-1 dt omega / rho couples the species;
+// the diagonal keeps each species' own stiffness, which is what bounds the
+// increments of trace radicals, so it follows the EPI step closely where the
+// explicit increment would not.  A cell whose network increment disagrees
+// with it is reacting in a way the network did not capture.  p in Pa, dt in s.
+template <int NS>
+__device__ __forceinline__ void judge_increment(float T, float p, float dt, const double *Y, float *e) {
+  float inv_mw = 0;
+#pragma unroll
+  for (int k = 0; k < NS; ++k) inv_mw += static_cast<float>(Y[k]) / cJ.mw[k];
+  const float rho = p / (8314.462618f * T * inv_mw);
+  float c[NS], g[NS];
+  const float ln_t = logf(T), t_inv = 1.f / T;
+#pragma unroll
+  for (int k = 0; k < NS; ++k) {
+    c[k] = rho * static_cast<float>(Y[k]) / cJ.mw[k] * 1e-3f;
+    // g_k / RT from the NASA-7 polynomials (frozen below T_low)
+    const float tt = T < cJ.t_low[k] ? cJ.t_low[k] : T;
+    const bool lo = tt < cJ.t_mid[k];
+    const float *a = lo ? &cJ.low[k * 7] : &cJ.high[k * 7];
+    const float lt = tt == T ? ln_t : logf(tt);
+    g[k] = a[0] * (1.f - lt) - 0.5f * a[1] * tt - a[2] * tt * tt * (1.f / 6.f) - a[3] * tt * tt * tt * (1.f / 12.f) -
+           a[4] * tt * tt * tt * tt * 0.05f + a[5] / tt - a[6];
+  }
+  float omega[NS], destruction[NS];
+#pragma unroll
+  for (int k = 0; k < NS; ++k) omega[k] = destruction[k] = 0;
+  auto rate = [&](float sA, float lnA, float b, float Ea) {
+    return sA * expf(fminf(lnA + b * ln_t - Ea * t_inv, 80.f));
+  };
+  const float ln_temp_t = logf(101325.0f / 8314.462618f * 1e-3f) - ln_t;
+  const int nr = cP.nr;
+  for (int r = 0; r < nr; ++r) {
+    const int type = cP.label[r];
+    float kf = rate(cJ.sA[r], cJ.lnA[r], cJ.b[r], cJ.Ea[r]);
+    if (type == 3) kf += rate(cJ.sA2[r], cJ.lnA2[r], cJ.b2[r], cJ.Ea2[r]);
+    if (type > 3) {
+      float cc = 0;
+#pragma unroll
+      for (int k = 0; k < NS; ++k) cc += c[k] * cJ.tb[r * NS + k];
+      if (type == 4) {
+        kf *= cc;
+      } else if (kf > 0.f) {  // a high-pressure rate that underflows FP32 leaves the rate at zero
+        const float pr = fmaxf(rate(cJ.sA2[r], cJ.lnA2[r], cJ.b2[r], cJ.Ea2[r]) * cc / kf, 1e-30f);
+        float F = 1.f;
+        if (type > 5) {
+          const float a = cJ.troe_a[r];
+          float fc = (1 - a) * expf(-T / cJ.troe_t3[r]) + a * expf(-T / cJ.troe_t1[r]);
+          if (type == 7) fc += expf(-cJ.troe_t2[r] / T);
+          const float lfc = log10f(fc), lpr = log10f(pr);
+          const float cq = -0.4f - 0.67f * lfc, nq = 0.75f - 1.27f * lfc;
+          const float tmp = (lpr + cq) / (nq - 0.14f * (lpr + cq));
+          F = exp10f(lfc / (1.f + tmp * tmp));
+        }
+        kf = kf * pr / (1.f + pr) * F;
+      }
+    }
+    float kb;
+    if (type != 2) {
+      float dg = 0;
+#pragma unroll
+      for (int k = 0; k < NS; ++k) dg += g[k] * static_cast<float>(cP.sb[r * NS + k] - cP.sf[r * NS + k]);
+      kb = kf * expf(fminf(dg - static_cast<float>(cP.order[r]) * ln_temp_t, 80.f));
+    } else {
+      kb = rate(cJ.sA2[r], cJ.lnA2[r], cJ.b2[r], cJ.Ea2[r]);
+    }
+    float q1 = kf, q2 = kb;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      for (int m = 0; m < cP.sf[r * NS + k]; ++m) q1 *= c[k];
+      for (int m = 0; m < cP.sb[r * NS + k]; ++m) q2 *= c[k];
+    }
+    const float q = q1 - q2;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      omega[k] += static_cast<float>(cP.sb[r * NS + k] - cP.sf[r * NS + k]) * q;
+      destruction[k] += static_cast<float>(cP.sf[r * NS + k]) * q1 + static_cast<float>(cP.sb[r * NS + k]) * q2;
+    }
+  }
+  const float f = dt / rho;
+#pragma unroll
+  for (int k = 0; k < NS; ++k) {
+    const float w = cJ.mw[k] * 1e3f;
+    const float y = fmaxf(static_cast<float>(Y[k]), 1e-30f);
+    e[k] = f * omega[k] * w / (1.f + f * destruction[k] * w / y);
+  }
+}
+
+// The judge's verdict on an increment dy of a cell (T, p, Y, dt): every
+// species within gate.judge_rel of the diagonal point-implicit increment plus
+// gate.judge_abs (Y_k + gate.y_floor); a non-finite judge increment fails.
+template <int NS>
+__device__ __forceinline__ bool judge_accepts(const SurrogateGate &g, float T, float p, float dt, const double *Y,
+                                              const double *dy) {
+  float e[NS];
+  judge_increment<NS>(T, p, dt, Y, e);
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < NS; ++k) {
+    const float err = fabsf(static_cast<float>(dy[k]) - e[k]);
+    const float tol = g.judge_rel * fabsf(e[k]) + g.judge_abs * static_cast<float>(Y[k] + g.y_floor);
+    if (!(err <= tol)) ok = false;
+  }
+  return ok;
+}
+
 // Network output o (normalised, bias added) -> dY_k = (Y_k + eps) c_k
 // sinh(s_k o_k); the increment is then projected onto element conservation
 // (weighted least squares, weights |dY_k| + 1e-3 Y_k).  The cell is accepted
@@ -58,11 +214,18 @@ __device__ inline void epi_increment(double T, double rho, const double *Y, doub
 // (species below the floor are judged by their absolute change), and no mass
 // fraction is driven below -1e-9: the network is trusted where the chemistry
 // changes the composition little, the EPI step takes the reacting cells.
+// The judge: an accepted increment must also agree, species by species,
+// with the diagonal point-implicit increment (judge_increment) within
+// gate.judge_rel of it plus gate.judge_abs (Y_k + gate.y_floor); an
+// increment the network under-predicts (down to none at all) for a reacting
+// cell fails it.  gate.judge_rel < 0 turns the judge off.
 // NE is a compile-time bound on the element count (elements past p.n_elem
 // have zero rows and drop out), so every array lives in registers.  The
 // network's own error is ~1e-2, so the transcendental functions of the decode
 // run in FP32; the projection and the increments stay in FP64.
-template <int NS, int NE>
+// JUDGE: apply the judge here (the fused inference kernel leaves it to
+// k_sur_judge, which runs it at full occupancy over the accepted cells).
+template <int NS, int NE, bool JUDGE = true>
 __device__ __forceinline__ bool decode_ne(const SurrogateDev &p, const float *o, float T, float lp, float ldt,
                                           const double *Y, double *dy) {
   const SurrogateGate &g = p.gate;
@@ -121,6 +284,7 @@ __device__ __forceinline__ bool decode_ne(const SurrogateDev &p, const float *o,
     dy[k] -= w[k] * corr;
     if (Y[k] + dy[k] < -1e-9) ok = false;
   }
+  if (JUDGE && ok && g.judge_rel >= 0.f) ok = judge_accepts<NS>(g, T, exp10f(lp), exp10f(ldt), Y, dy);
   return ok;
 }
 
@@ -316,7 +480,7 @@ __device__ __forceinline__ void tile_apply(const DevBlock &B, const SurrogateDev
     for (int s = 0; s < NS; ++s) out[s] = o[s] + bias_out[s];
     rho = B.bv[n];
     dt = B.dt_local[nz];
-    acc = dt > 0 && decode_ne<NS, NE>(P, out, static_cast<float>(B.bv[5 * sz + n]),
+    acc = dt > 0 && decode_ne<NS, NE, false>(P, out, static_cast<float>(B.bv[5 * sz + n]),
                                       log10f(static_cast<float>(B.bv[4 * sz + n])), log10f(static_cast<float>(dt)),
                                       Y, dy);
   }
@@ -606,6 +770,41 @@ __global__ void __launch_bounds__(256) k_sur_candidates(const DevBlock *__restri
     }
     at = __shfl_sync(0xffffffffu, at, 0);
     if (pick) list[at + __popc(m & ((1u << lane) - 1u))] = static_cast<int>(c);
+  }
+}
+
+// The judge over the cells the fused inference accepted (the candidate list
+// of this step): a cell whose increment (recovered from its rate rho dY / dt)
+// the judge refuses goes back to the point-implicit chemistry, and the
+// statistics move it from accepted to fallback.
+template <class C>
+__global__ void __launch_bounds__(256) k_sur_judge(const DevBlock *__restrict__ blks, int b, SurrogateGate g,
+                                                   const int *__restrict__ cand, const int *cand_count,
+                                                   unsigned long long *stats) {
+  constexpr int NS = C::ns;
+  if (g.judge_rel < 0.f) return;
+  const DevBlock &B = blks[b];
+  const int count = *cand_count;
+  const int64_t sz = B.G.size, sz0 = B.Z.size;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+    const int64_t c = cand[q];
+    const int i = static_cast<int>(c % B.mx), j = static_cast<int>((c / B.mx) % B.my),
+              k = static_cast<int>(c / (static_cast<int64_t>(B.mx) * B.my));
+    const int64_t n = B.G.at(i, j, k), nz = B.Z.at(i, j, k);
+    if (!B.chem_quiet[nz]) continue;
+    const double rho = B.bv[n], dt = B.dt_local[nz];
+    double Y[NS], dy[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      Y[s] = B.sv[s * sz + n];
+      dy[s] = B.chem_rate[s * sz0 + nz] * dt / rho;
+    }
+    if (!judge_accepts<NS>(g, static_cast<float>(B.bv[5 * sz + n]), static_cast<float>(B.bv[4 * sz + n]),
+                           static_cast<float>(dt), Y, dy)) {
+      B.chem_quiet[nz] = 0;
+      atomicAdd(&stats[0], ~0ull);  // minus one
+      atomicAdd(&stats[1], 1ull);
+    }
   }
 }
 

@@ -405,6 +405,9 @@ Surrogate::~Surrogate() {
 // may still be in flight when a kernel on this non-blocking stream starts.
 void Surrogate::upload_chem() {
   ck(cudaMemcpyToSymbolAsync(cP, &chem_, sizeof(DevParams), 0, cudaMemcpyHostToDevice, stream_), "upload mechanism");
+  const sur::JudgeTables jt = sur::make_judge_tables(chem_);
+  ck(cudaMemcpyToSymbolAsync(sur::cJ, &jt, sizeof(jt), 0, cudaMemcpyHostToDevice, stream_), "upload judge tables");
+  ck(cudaStreamSynchronize(stream_), "upload judge tables");
 }
 
 void Surrogate::pack() {
@@ -865,7 +868,7 @@ const SurrogateDev &Surrogate::device_params() {
 void Surrogate::save(const std::string &path) const {
   std::ofstream f(path, std::ios::binary);
   if (!f) throw std::runtime_error("cannot write " + path);
-  const char magic[8] = {'O', 'S', 'T', 'C', 'M', 'L', 'P', '4'};
+  const char magic[8] = {'O', 'S', 'T', 'C', 'M', 'L', 'P', '5'};
   f.write(magic, 8);
   f.write(reinterpret_cast<const char *>(in_mu.data()), sizeof(in_mu));
   f.write(reinterpret_cast<const char *>(in_sig.data()), sizeof(in_sig));
@@ -880,7 +883,7 @@ void Surrogate::load(const std::string &path) {
   if (!f) throw std::runtime_error("cannot open " + path);
   char magic[8];
   f.read(magic, 8);
-  if (std::memcmp(magic, "OSTCMLP4", 8) != 0) throw std::runtime_error(path + " is not a surrogate file");
+  if (std::memcmp(magic, "OSTCMLP5", 8) != 0) throw std::runtime_error(path + " is not a surrogate file");
   f.read(reinterpret_cast<char *>(in_mu.data()), sizeof(in_mu));
   f.read(reinterpret_cast<char *>(in_sig.data()), sizeof(in_sig));
   f.read(reinterpret_cast<char *>(out_c.data()), sizeof(out_c));

@@ -39,6 +39,11 @@ struct SurrogateGate {
   float rel_max = 0.01f;                   // largest accepted |dY_k| / (Y_k + y_floor)
   float out_max = 6.f;                     // largest accepted |network output|
   float y_floor = 1e-10f;                  // mass fraction below which changes count as absolute
+  // the judge: |dY_k - dY_DA,k| <= judge_rel |dY_DA,k| + judge_abs (Y_k +
+  // y_floor) for every species, dY_DA the diagonal point-implicit increment
+  // of the cell's own chemistry; judge_rel < 0 turns it off
+  float judge_rel = 0.25f;
+  float judge_abs = 1e-4f;
 };
 
 // Parameters the fused inference kernel reads (device memory).

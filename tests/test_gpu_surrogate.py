@@ -124,13 +124,16 @@ def trained(drv, tmp_path_factory):
     field.initialize()
     field.step(20)
     sur = ostc.Surrogate(field, seed=17)
-    sur.generate(1 << 18, seed=5, field=field, field_fraction=0.9)
-    sur.train(500, batch=16384, lr=2e-3)
+    sur.generate(1 << 19, seed=5, field=field, field_fraction=0.9)
+    sur.train(3000, batch=16384, lr=2e-3)
     return case, field, sur
 
 
 def test_fused_inference_matches_unfused(trained):
+    """The fused kernel against the unfused prediction on the same cells (the
+    judge off, so that the comparison covers accepted cells too)."""
     case, field, sur = trained
+    sur.set_gate(judge_rel=-1.0)
     st = cell_states(field)
     dy_net, acc_net = sur.predict(st)
     dy_epi = sur.label(st)
@@ -153,4 +156,75 @@ def test_fused_inference_matches_unfused(trained):
     # where the unfused gate accepted, the fused kernel gave the network's increment
     assert np.mean(net_like[acc_net]) > 0.98, np.mean(net_like[acc_net])
     field.set_surrogate(None)
+    sur.set_gate(judge_rel=0.25, judge_abs=1e-4)
     print("fused: accepted", acc, "fallback", fb)
+
+
+def test_judge_rejects_a_silent_network_on_reacting_cells(drv):
+    """A network whose every weight and bias is zero predicts no change at
+    all.  The gate's own checks (training box, element defect, |dY_k| <=
+    rel_max (Y_k + y_floor)) accept that wherever the change is small, even
+    where the cell reacts; the judge compares with the cell's explicit
+    increment (the diagonal point-implicit one) and rejects it on every cell that reacts
+    measurably (an EPI increment above ten times the judge's floor)."""
+    sur = ostc.Surrogate(drv, seed=7)
+    sur.generate(1 << 14, seed=3)  # feature and target scaling
+    sur.set_params(np.zeros_like(sur.params()))
+    st = random_states(1 << 14, 31)
+    dy_epi = sur.label(st)
+    g = sur.gate()
+    Y = st[:, 2:11]
+    reacting = np.any(np.abs(dy_epi) > 10 * g["judge_abs"] * (Y + g["y_floor"]), axis=1)
+    pred, acc = sur.predict(st)
+    assert np.all(pred == 0.0)
+    assert reacting.sum() > 1000
+    assert not np.any(acc & reacting), int(np.sum(acc & reacting))
+    # where nothing happens (cold hydrogen without oxygen) it is still trusted
+    cold = np.zeros((256, 12))
+    cold[:, 0] = np.linspace(300.0, 400.0, 256)
+    cold[:, 1] = 101325.0
+    cold[:, 2], cold[:, 10] = 0.4, 0.6  # H2, N2
+    cold[:, 11] = 1e-7
+    _, acc_cold = sur.predict(cold)
+    assert np.all(acc_cold)
+    sur.set_gate(judge_rel=-1.0)
+    _, acc_unjudged = sur.predict(st)
+    assert np.sum(acc_unjudged & reacting) > 100  # what the judge catches
+
+
+def test_what_the_network_gains(trained, tmp_path):
+    """The surrogate against the method without it on the same flow field and
+    steps: the point-implicit chemistry everywhere (the FP32-bulk path) and
+    the surrogate path both stay within the metric's 1e-3 relative L2 of
+    (T, Y_OH, p) against the plain FP64 path, and the network takes the
+    chemistry of a share of the cell-steps, whose EPI Jacobian,
+    factorisation and DPLUR solves are skipped.  (Step time is measured at
+    the benchmark's size, where it means something: bench.py --mode
+    surrogate against --mode mixed.)"""
+    case, _, sur = trained
+    steps = 30
+    runs = {}
+    for name, kw, use in (("fp64", dict(precision="fp64"), False), ("epi", dict(precision="mixed"), False),
+                          ("surrogate", dict(precision="mixed"), True)):
+        d = ostc.Driver(case, **kw)
+        d.initialize()
+        d.step(20)
+        if use:
+            d.set_surrogate(sur)
+        d.step(steps)
+        g = d.info().ngg
+        bv = d.get(0, "bv")[:, g:-g, g:-g, g:-g]
+        sv = d.get(0, "sv")[:, g:-g, g:-g, g:-g]
+        runs[name] = {"T": bv[5].copy(), "Y_OH": sv[4].copy(), "p": bv[4].copy()}
+        if use:
+            runs["stats"] = d.chemistry_stats()
+            d.set_surrogate(None)
+        d.close()
+    for name in ("epi", "surrogate"):
+        for f in ("T", "Y_OH", "p"):
+            rel = np.linalg.norm(runs[name][f] - runs["fp64"][f]) / np.linalg.norm(runs["fp64"][f])
+            assert rel <= 1e-3, (name, f, rel)
+    accepted, fallback = runs["stats"]
+    assert accepted + fallback == steps * runs["fp64"]["T"].size
+    assert accepted > 0
+    print(f"network took {accepted / (accepted + fallback):.3f} of the cell-steps' chemistry")
