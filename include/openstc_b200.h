@@ -81,6 +81,10 @@ typedef struct ostc_options {
                       neighbour, the sweeps take the neighbours across the face, and
                       the shared plane, computed identically on both sides, is not
                       re-averaged.  No counterpart in the reference. */
+  int wall_distance; /* the wall distance of SST cases: 0 automatic (bucket search
+                        above 2048 wall points), 1 the reference's brute force over
+                        every wall point (src/Driver.cu:461-482), 2 an exact search of
+                        a uniform bucket grid of the wall points (the same values) */
 } ostc_options;
 
 typedef struct ostc_info {

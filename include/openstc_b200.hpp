@@ -51,6 +51,7 @@ struct Parameter {
     options.quiet = 0;
     options.precision = 0;
     options.exact_inner = 0;
+    options.wall_distance = 0;
   }
   std::string case_dir;
   ostc_options options;

@@ -35,7 +35,8 @@ class OstcError(RuntimeError):
 
 
 class Options(C.Structure):
-    _fields_ = [("device", C.c_int), ("quiet", C.c_int), ("precision", C.c_int), ("exact_inner", C.c_int)]
+    _fields_ = [("device", C.c_int), ("quiet", C.c_int), ("precision", C.c_int), ("exact_inner", C.c_int),
+                ("wall_distance", C.c_int)]
 
 
 class SurrogateEval(C.Structure):
@@ -191,17 +192,22 @@ class Driver:
     """
 
     def __init__(self, case_dir: str | Path, device: int = 0, quiet: bool = True, precision: str = "fp64",
-                 exact_inner: bool = False):
+                 exact_inner: bool = False, wall_distance: str = "auto"):
         """precision: "fp64" (the reference's arithmetic) or "mixed" (FP32 fluxes,
         limiter, SST, flux Jacobians and transport; FP64 state, update,
         temperature inversion, chemistry, point-implicit solve, residual).
         exact_inner: a multi-block grid computes what the same grid as one
-        block computes (ostc_options.exact_inner; FP64 path)."""
+        block computes (ostc_options.exact_inner; FP64 path).
+        wall_distance: "auto", "brute" (the reference's search over every wall
+        point) or "grid" (an exact bucket search; the same values)."""
         lib = library()
         self._h = C.c_void_p()
         if precision not in PRECISIONS:
             raise OstcError(f"precision must be one of {sorted(PRECISIONS)}")
-        opt = Options(device, 1 if quiet else 0, PRECISIONS[precision], 1 if exact_inner else 0)
+        walls = {"auto": 0, "brute": 1, "grid": 2}
+        if wall_distance not in walls:
+            raise OstcError(f"wall_distance must be one of {sorted(walls)}")
+        opt = Options(device, 1 if quiet else 0, PRECISIONS[precision], 1 if exact_inner else 0, walls[wall_distance])
         _check(lib.ostc_driver_create(str(case_dir).encode(), C.byref(opt), C.byref(self._h)))
         self.case_dir = Path(case_dir)
 

@@ -218,11 +218,13 @@ def _mixing_layer_grid(mx, my, mz, x0=0.0, lx=0.3):
     return x, y, z
 
 
-def _mixing_setup(case, *, total_step, output_screen, output_file, initial, cfl, dplur, chem, implicit=1):
+def _mixing_setup(case, *, total_step, output_screen, output_file, initial, cfl, dplur, chem, implicit=1,
+                  wall=False):
     write_setup(case, setup_files(
         dimension=3, total_step=total_step, output_file=output_file, output_screen=output_screen, cfl=cfl,
         implicit_method=implicit, dplur_inner_step=dplur, species=True, reaction=True, turbulence=True,
-        chem_src_method=chem, initial=initial, inflows=[UPPER, LOWER]))
+        chem_src_method=chem, initial=initial, inflows=[UPPER, LOWER],
+        walls=[dict(name="wall", label=2, temperature=300.0)] if wall else None))
 
 
 RU = 8314.462618  # J/(kmol K), src/Constants.h:18
@@ -439,14 +441,16 @@ def _species_names(case: Path) -> list[str]:
 def mixing_layer_case(case: str | Path, mx: int = 384, my: int = 192, mz: int = 64, total_step: int = 2000,
                       output_screen: int = 100, output_file: int | None = None, cfl: float = 0.5,
                       dplur: int = 4, chem: int = 1, implicit: int = 1,
-                      spikes: list[tuple[int, int, int, float, float]] | None = None) -> Path:
+                      spikes: list[tuple[int, int, int, float, float]] | None = None, wall_j0: bool = False) -> Path:
     """3-D supersonic H2 / vitiated-air mixing layer (0.3 x 0.05 x 0.02 m,
     y clustered at the splitter y = 0.025 m).  Upper stream Mach 2.4, 1250 K,
     Y_O2 0.245, Y_H2O 0.175, N2; lower stream H2 / N2 (0.4 / 0.6) at
     Mach 1.2, 300 K; 1 atm; 9 species / 19 reactions, k-omega SST with 1 %
     inflow turbulence, DPLUR with `dplur` sweeps, chemistry treatment `chem`
     (1 point-implicit EPI, 2 diagonal).  spikes: cells whose initial density
-    and pressure are scaled (see _blend_initial_field)."""
+    and pressure are scaled (see _blend_initial_field).  wall_j0: the j = 0
+    face is an isothermal 300 K wall instead of a symmetry plane (the SST
+    wall distance then has mx x mz wall points)."""
     case = Path(case)
     x, y, z = _mixing_layer_grid(mx, my, mz)
     write_grid(case, [(x, y, z)])
@@ -455,17 +459,17 @@ def mixing_layer_case(case: str | Path, mx: int = 384, my: int = 192, mz: int = 
         (0, 0, js, my - 1, 0, mz - 1, 5),
         (0, 0, 0, js - 1, 0, mz - 1, 9),
         (mx - 1, mx - 1, 0, my - 1, 0, mz - 1, 6),
-        (0, mx - 1, 0, 0, 0, mz - 1, 3),
+        (0, mx - 1, 0, 0, 0, mz - 1, 2 if wall_j0 else 3),
         (0, mx - 1, my - 1, my - 1, 0, mz - 1, 3),
         (0, mx - 1, 0, my - 1, 0, 0, 3),
         (0, mx - 1, 0, my - 1, mz - 1, mz - 1, 3),
     ]])
     copy_chemistry(case)
     _mixing_setup(case, total_step=total_step, output_screen=output_screen, output_file=output_file or 10 ** 9,
-                  initial=0, cfl=cfl, dplur=dplur, chem=chem, implicit=implicit)
+                  initial=0, cfl=cfl, dplur=dplur, chem=chem, implicit=implicit, wall=wall_j0)
     _blend_initial_field(case, spikes=spikes)
     _mixing_setup(case, total_step=total_step, output_screen=output_screen, output_file=output_file or 10 ** 9,
-                  initial=1, cfl=cfl, dplur=dplur, chem=chem, implicit=implicit)
+                  initial=1, cfl=cfl, dplur=dplur, chem=chem, implicit=implicit, wall=wall_j0)
     return case
 
 

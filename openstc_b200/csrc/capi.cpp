@@ -75,6 +75,8 @@ int ostc_driver_create(const char *case_dir, const ostc_options *opt, ostc_drive
       o.quiet = opt->quiet != 0;
       o.precision = opt->precision;
       o.exact_inner = opt->exact_inner != 0;
+      if (opt->wall_distance < 0 || opt->wall_distance > 2) throw std::invalid_argument("wall_distance must be 0, 1 or 2");
+      o.wall_distance = opt->wall_distance;
     }
     *out = new ostc_driver(case_dir, o);
     return OSTC_OK;

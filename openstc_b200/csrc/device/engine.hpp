@@ -45,6 +45,7 @@ struct EngineSetup {
   int device = 0;
   int precision = 0;  // 0 FP64 (the reference's arithmetic), 1 FP32-bulk / FP64-critical
   bool exact_inner = false;  // inner faces computed as the interior of one block (FP64)
+  int wall_distance = 0;     // 0 automatic, 1 brute force (the reference's), 2 bucket search
 };
 
 class Engine {

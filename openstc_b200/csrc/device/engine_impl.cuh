@@ -76,6 +76,7 @@ class EngineT final : public Engine {
     cuda_check(cudaMemset(d_bad_, 0, sizeof(unsigned int)), "memset bad");
     cuda_check(cudaMallocHost(&h_res_, sizeof(double) * 4), "cudaMallocHost res");
     if (!s.wall_points.empty()) {
+      build_wall_grid(s.wall_points);
       cuda_check(cudaMalloc(&d_wall_, sizeof(double) * s.wall_points.size()), "cudaMalloc wall");
       cuda_check(cudaMemcpyAsync(d_wall_, s.wall_points.data(), sizeof(double) * s.wall_points.size(),
                                  cudaMemcpyHostToDevice, stream_),
@@ -218,8 +219,13 @@ class EngineT final : public Engine {
     upload_params();
     const auto &p = setup_.params;
     if (C::turb && p.rans_model == 2)
-      k_wall_distance<<<grid(tilesg_), block3(), 0, stream_>>>(d_blocks_, tilesg_, d_wall_,
-                                                              static_cast<int>(setup_.wall_points.size() / 3));
+    {
+      if (wall_grid_.start)
+        k_wall_distance_grid<<<grid(tilesg_), block3(), 0, stream_>>>(d_blocks_, tilesg_, wall_grid_);
+      else
+        k_wall_distance<<<grid(tilesg_), block3(), 0, stream_>>>(d_blocks_, tilesg_, d_wall_,
+                                                                static_cast<int>(setup_.wall_points.size() / 3));
+    }
     if (p.dim == 2) launch_kcopy();
     launch_bcs();
     k_cv_from_bv<C><<<grid(tilesg_), block3(), 0, stream_>>>(d_blocks_, tilesg_);
@@ -648,7 +654,7 @@ class EngineT final : public Engine {
             d_blocks_, b, sur_, d_fb_count_, d_fb_list_, d_sur_stats_, d_sur_err_, d_fb_list_, d_fb_count_,
             last ? d_sur_phase_ : nullptr);
         mark("surrogate");
-        sur::k_sur_judge<C><<<static_cast<unsigned>(8 * num_sms_), 256, 0, stream_>>>(d_blocks_, b, sur_.gate,
+        sur::k_sur_judge<C><<<static_cast<unsigned>(8 * num_sms_), sur::kJudgeCta, 0, stream_>>>(d_blocks_, b, sur_.gate,
                                                                                      d_fb_list_, d_fb_count_,
                                                                                      d_sur_stats_);
         mark("surrogate_judge");
@@ -844,6 +850,74 @@ class EngineT final : public Engine {
     }
   }
 
+  // The bucket grid of the wall points for k_wall_distance_grid: method 2, or
+  // method 0 (automatic) with more than 2048 points; buckets of edge h chosen
+  // for about four points per bucket over the points' bounding box.
+  void build_wall_grid(const std::vector<double> &w) {
+    const int64_t nw = static_cast<int64_t>(w.size() / 3);
+    const int method = setup_.wall_distance;
+    if (nw == 0 || method == 1 || (method == 0 && nw <= 2048)) return;
+    double lo[3], hi[3];
+    for (int d = 0; d < 3; ++d) lo[d] = hi[d] = w[d];
+    for (int64_t q = 0; q < nw; ++q)
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = std::min(lo[d], w[3 * q + d]);
+        hi[d] = std::max(hi[d], w[3 * q + d]);
+      }
+    const double ext = std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]});
+    auto count = [&](double h, int *n) {
+      int64_t c = 1;
+      for (int d = 0; d < 3; ++d) {
+        n[d] = std::max(1, static_cast<int>(std::ceil((hi[d] - lo[d]) / h)));
+        c *= n[d];
+      }
+      return c;
+    };
+    const int64_t target = std::max<int64_t>(1, std::min<int64_t>(nw / 4, int64_t(1) << 22));
+    double h = ext > 0 ? ext : 1.0, a = h * 1e-7;  // count(h) <= target <= count(a)
+    int n[3];
+    for (int it = 0; it < 80 && ext > 0; ++it) {
+      const double m = std::sqrt(a * h);
+      if (count(m, n) > target) a = m; else h = m;
+    }
+    count(h, n);
+    const int nb = n[0] * n[1] * n[2];
+    std::vector<int> bucket(static_cast<size_t>(nw)), start(static_cast<size_t>(nb) + 1, 0);
+    for (int64_t q = 0; q < nw; ++q) {
+      int c[3];
+      for (int d = 0; d < 3; ++d)
+        c[d] = std::min(n[d] - 1, std::max(0, static_cast<int>(std::floor((w[3 * q + d] - lo[d]) / h))));
+      bucket[q] = (c[2] * n[1] + c[1]) * n[0] + c[0];
+      ++start[bucket[q] + 1];
+    }
+    for (int b = 0; b < nb; ++b) start[b + 1] += start[b];
+    std::vector<int> fill(start.begin(), start.end() - 1);
+    std::vector<double> pts(w.size());
+    for (int64_t q = 0; q < nw; ++q) {
+      const int at = fill[bucket[q]]++;
+      for (int d = 0; d < 3; ++d) pts[3 * static_cast<size_t>(at) + d] = w[3 * q + d];
+    }
+    int *d_start = nullptr;
+    double *d_pts = nullptr;
+    cuda_check(cudaMalloc(&d_start, sizeof(int) * start.size()), "cudaMalloc wall grid");
+    cuda_check(cudaMalloc(&d_pts, sizeof(double) * pts.size()), "cudaMalloc wall grid");
+    allocations_.push_back(d_start);
+    allocations_.push_back(d_pts);
+    cuda_check(cudaMemcpyAsync(d_start, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice, stream_),
+               "copy wall grid");
+    cuda_check(cudaMemcpyAsync(d_pts, pts.data(), sizeof(double) * pts.size(), cudaMemcpyHostToDevice, stream_),
+               "copy wall grid");
+    cuda_check(cudaStreamSynchronize(stream_), "copy wall grid");  // the host vectors go out of scope
+    for (int d = 0; d < 3; ++d) {
+      wall_grid_.lo[d] = lo[d];
+      wall_grid_.hi[d] = hi[d];
+      wall_grid_.n[d] = n[d];
+    }
+    wall_grid_.h = h;
+    wall_grid_.start = d_start;
+    wall_grid_.pts = d_pts;
+  }
+
   // exact inner faces: the block faces the DPLUR sweeps cross (each inner
   // face must cover its whole block face; FP64 path, 3-D grids)
   void mark_exact_inner_faces() {
@@ -967,6 +1041,7 @@ class EngineT final : public Engine {
   Tiles tiles0_, tiles1_, tilesg_, col_tiles_, dir_tiles_[3];
   std::vector<int> order_;  // the blocks' schedule in every tile table (empty: block order)
   int flux_variant_ = 0;    // kFluxVariant entry of the FP32-bulk flux passes
+  WallGrid wall_grid_{};    // the bucket grid of the wall points (start null: brute force)
   size_t source_smem_ = 0, flux_smem_ = 0, col_smem_ = 0, dq0_smem_ = 0;
   int final_dq_ = 0;
   cudaGraphExec_t graphs_[4] = {nullptr, nullptr, nullptr, nullptr};

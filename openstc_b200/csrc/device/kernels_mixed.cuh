@@ -899,17 +899,28 @@ __global__ void __launch_bounds__(256) k_pack32(const DevBlock *__restrict__ blk
   float *f = B.f32;
   for (int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; n < sz;
        n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    OSTC_UNROLL for (int v = 0; v < 6; ++v) f[(L::prim + v) * sz + n] = static_cast<float>(B.bv[v * sz + n]);
-    OSTC_UNROLL for (int v = 0; v < C::nsc; ++v) f[(L::prim + 6 + v) * sz + n] = static_cast<float>(B.sv[v * sz + n]);
-    f[L::mul * sz + n] = static_cast<float>(B.mul[n]);
-    f[L::cond * sz + n] = static_cast<float>(B.cond[n]);
+    // all loads, then all stores (a store would otherwise hold back the
+    // loads after it: the compiler cannot rule out that they overlap)
+    float v[L::n_dynamic];
+    OSTC_UNROLL for (int q = 0; q < L::n_dynamic; ++q) v[q] = 0.f;
+    OSTC_UNROLL for (int q = 0; q < 6; ++q) v[L::prim + q] = static_cast<float>(__ldg(B.bv + q * sz + n));
+    OSTC_UNROLL for (int q = 0; q < C::nsc; ++q) v[L::prim + 6 + q] = static_cast<float>(__ldg(B.sv + q * sz + n));
+    v[L::mul] = static_cast<float>(__ldg(B.mul + n));
+    v[L::cond] = static_cast<float>(__ldg(B.cond + n));
     if constexpr (C::turb) {
-      f[L::mut * sz + n] = static_cast<float>(B.mut[n]);
-      f[L::tcond * sz + n] = static_cast<float>(B.turb_cond[n]);
+      v[L::mut] = static_cast<float>(__ldg(B.mut + n));
+      v[L::tcond] = static_cast<float>(__ldg(B.turb_cond + n));
     }
-    OSTC_UNROLL for (int l = 0; l < C::ns; ++l) f[(L::rho_d + l) * sz + n] = static_cast<float>(B.rho_d[l * sz + n]);
-    f[L::acoustic * sz + n] = static_cast<float>(B.acoustic[n]);
-    if constexpr (C::mix != 0) f[L::gamma * sz + n] = static_cast<float>(B.gamma[n]);
+    OSTC_UNROLL for (int l = 0; l < C::ns; ++l) v[L::rho_d + l] = static_cast<float>(__ldg(B.rho_d + l * sz + n));
+    v[L::acoustic] = static_cast<float>(__ldg(B.acoustic + n));
+    if constexpr (C::mix != 0) v[L::gamma] = static_cast<float>(__ldg(B.gamma + n));
+    OSTC_UNROLL for (int q = 0; q < L::n_dynamic; ++q) {
+      if (q == L::mut || q == L::tcond) {
+        if constexpr (!C::turb) continue;
+      }
+      if (q == L::gamma && C::mix == 0) continue;
+      f[q * sz + n] = v[q];
+    }
   }
 }
 
@@ -1015,6 +1026,7 @@ __global__ void __launch_bounds__(kCta, 4) k_sweep_mx(const DevBlock *__restrict
   const int64_t sz = B.G.size, szd = B.D.size, sz0 = B.Z.size;
   const int64_t n = B.G.at(i, j, k), nd = B.D.at(i, j, k), nz = B.Z.at(i, j, k);
   const int64_t sx = B.G.sx, sxy = B.G.sxy, dsx = B.D.sx, dsxy = B.D.sxy;
+  const fp32::Src32<C> f{B.f32, sz};
   float tot[NV];
   OSTC_UNROLL for (int l = 0; l < NV; ++l) tot[l] = 0;
   const double *isr = B.inv_spec;
@@ -1028,31 +1040,30 @@ __global__ void __launch_bounds__(kCta, 4) k_sweep_mx(const DevBlock *__restrict
     const int64_t gs = dir == 0 ? 1 : (dir == 1 ? sx : sxy), ds = dir == 0 ? 1 : (dir == 1 ? dsx : dsxy);
     const int64_t on = plus ? n + gs : n - gs, od = plus ? nd + ds : nd - ds;
     const float sr = ldf(isr + dir * szd + od);
-    // compute_jacobian_times_dq (src/DPLURHPP.cuh:78-125) at the neighbour
-    const double *mr = B.metric + 3 * dir * sz;
-    const float xi_x = ldf(mr + on), xi_y = ldf(mr + sz + on), xi_z = ldf(mr + 2 * sz + on);
-    const float u = ldf(B.bv + sz + on), v = ldf(B.bv + 2 * sz + on), w = ldf(B.bv + 3 * sz + on);
+    // compute_jacobian_times_dq (src/DPLURHPP.cuh:78-125) at the neighbour,
+    // its state from the step's FP32 copy (k_pack32; unchanged until the update)
+    const float xi_x = f.metric(3 * dir, on), xi_y = f.metric(3 * dir + 1, on), xi_z = f.metric(3 * dir + 2, on);
+    const float u = f.prim(1, on), v = f.prim(2, on), w = f.prim(3, on);
     const float U = xi_x * u + xi_y * v + xi_z * w;
     const float lmd1 = U + (plus ? -sr : sr);
-    const float vel = ldf(B.vel + on);
-    const float e = 0.5f * vel * vel;
+    const float e = 0.5f * (u * u + v * v + w * w);
     float d[NV];
     OSTC_UNROLL for (int l = 0; l < NV; ++l) d[l] = __ldg(dqin + l * szd + od);
     float gamma = 1.4f, b3 = 0, b4 = 0, h = 0;
     if constexpr (C::mix != 0) {
-      const float t = ldf(B.bv + 5 * sz + on);
-      gamma = ldf(B.gamma + on);
+      const float t = f.prim(5, on);
+      gamma = f.gamma(on);
       OSTC_UNROLL for (int l = 0; l < NS; ++l) {
         const float hk = ldf(B.h_spec + l * szd + od);
         b3 += fp32::kRu * t * cF.mw_inv[l] * d[5 + l];
         b4 += hk * d[5 + l];
-        h += ldf(B.sv + l * sz + on) * hk;
+        h += f.prim(6 + l, on) * hk;
       }
       b3 *= gamma;
       b4 *= gamma - 1;
       h += e;
     } else {
-      h = gamma / (gamma - 1) * ldf(B.bv + 4 * sz + on) / ldf(B.bv + on) + e;
+      h = gamma / (gamma - 1) * f.prim(4, on) / f.prim(0, on) + e;
     }
     const float b1 = xi_x * d[1] + xi_y * d[2] + xi_z * d[3] - U * d[0];
     const float b2 = (gamma - 1) * (e * d[0] - u * d[1] - v * d[2] - w * d[3] + d[4]);
@@ -1063,7 +1074,7 @@ __global__ void __launch_bounds__(kCta, 4) k_sweep_mx(const DevBlock *__restrict
     tot[2] += sg * (v * b1 + xi_y * b2 + lmd1 * d[2] + xi_y * b34);
     tot[3] += sg * (w * b1 + xi_z * b2 + lmd1 * d[3] + xi_z * b34);
     tot[4] += sg * (h * b1 + U * b2 + lmd1 * d[4] + U * b34);
-    OSTC_UNROLL for (int l = 0; l < C::nsc; ++l) tot[5 + l] += sg * (lmd1 * d[5 + l] + ldf(B.sv + l * sz + on) * b1);
+    OSTC_UNROLL for (int l = 0; l < C::nsc; ++l) tot[5 + l] += sg * (lmd1 * d[5 + l] + f.prim(6 + l, on) * b1);
   }
   const double dt = B.dt_local[nz];
   const double diag = 1 + dt * (isr[nd] + isr[szd + nd] + isr[2 * szd + nd]);
@@ -1134,7 +1145,7 @@ __global__ void __launch_bounds__(kCta) k_props_mx(const DevBlock *__restrict__ 
     const float a = sqrtf(gamma * fp32::kRu * t * mw_inv);
     B.acoustic[n] = a;
     const float mw = 1.f / mw_inv;
-    float X[NS], vis[NS];
+    float X[NS], vis[NS], rs[NS], sq[NS];  // sq = sqrt(mu_k), rs = 1 / sq
     const float st = sqrtf(t);
     OSTC_UNROLL for (int l = 0; l < NS; ++l) {
       X[l] = Y[l] * mw * cF.mw_inv[l];
@@ -1142,14 +1153,16 @@ __global__ void __launch_bounds__(kCta) k_props_mx(const DevBlock *__restrict__ 
       const float r = 1.f / (t_dl + 0.5f);
       const float ci = 1.147f * powf(t_dl, -0.145f) + r * r;
       vis[l] = cF.vis_coeff[l] * st / ci;
+      rs[l] = rsqrtf(vis[l]);
+      sq[l] = vis[l] * rs[l];
     }
     float viscosity = 0, conductivity = 0;
     OSTC_UNROLL for (int m = 0; m < NS; ++m) {
       float vt = 0;
       OSTC_UNROLL for (int q = 0; q < NS; ++q) {
         float phi = 1.f;
-        if (m != q) {
-          const float num = 1 + sqrtf(vis[m] / vis[q]) * cF.wq[m * NS + q];
+        if (m != q) {  // Wilke's phi_mq with sqrt(mu_m / mu_q) as sqrt(mu_m) / sqrt(mu_q)
+          const float num = 1 + sq[m] * rs[q] * cF.wq[m * NS + q];
           phi = num * num * cF.w8[m * NS + q];
         }
         vt += phi * X[q];

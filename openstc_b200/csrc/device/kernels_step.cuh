@@ -476,14 +476,14 @@ __global__ void __launch_bounds__(kCta) k_dq0(const DevBlock *__restrict__ blks,
   const int64_t nd = B.D.at(i, j, k), nz = B.Z.at(i, j, k), szd = B.D.size, sz0 = B.Z.size;
   const double dt = B.dt_local[nz];
   const double diag = 1 + dt * (B.inv_spec[nd] + B.inv_spec[szd + nd] + B.inv_spec[2 * szd + nd]);
+  double dq[NV];  // loaded before the first store, which would hold the loads back
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] = B.dq[l * szd + nd];
   if constexpr (C::mix != 0) {
     // T is fixed during the sweeps: evaluate the species enthalpies once
     double hk[NS];
     enthalpy<NS>(B.bv[5 * B.G.size + B.G.at(i, j, k)], hk);
     OSTC_UNROLL for (int l = 0; l < NS; ++l) B.h_spec[l * szd + nd] = hk[l];
   }
-  double dq[NV];
-  OSTC_UNROLL for (int l = 0; l < NV; ++l) dq[l] = B.dq[l * szd + nd];
   if constexpr (C::mix != 2) {
     OSTC_UNROLL for (int l = 0; l < 5 + NS; ++l) dq[l] /= diag;
   } else {
@@ -693,36 +693,59 @@ __device__ __forceinline__ void newton_temperature(const double *Y, double rho, 
 }
 
 // Primitive recovery from Q at one point (update_bv_1_point,
-// src/FieldOperation.cuh:185-215); cv must already hold the new Q.
+// src/FieldOperation.cuh:185-215), from the new Q held in registers: writes
+// bv, sv and the velocity magnitude of point n and leaves rho, u, v, w, p in
+// v5 and k, omega in turb2 (RANS) for the caller's checks.  Every load (the
+// previous temperature, the Newton start) comes before the first store.
 template <class C>
-__device__ __forceinline__ void primitives_from_q(const DevBlock &B, int64_t n) {
+__device__ __forceinline__ void primitives_from_regs(const DevBlock &B, int64_t n, const double *q, double *v5,
+                                                     double *turb2) {
   constexpr int NS = C::ns;
   const int64_t sz = B.G.size;
-  const double rho = B.cv[n];
-  B.bv[n] = rho;
+  const double rho = q[0];
   const double rinv = 1.0 / rho;
-  const double u = B.cv[sz + n] * rinv, v = B.cv[2 * sz + n] * rinv, w = B.cv[3 * sz + n] * rinv;
+  const double u = q[1] * rinv, v = q[2] * rinv, w = q[3] * rinv;
+  const double vel2 = u * u + v * v + w * w;
+  double sv[C::nsc > 0 ? C::nsc : 1];
+  if constexpr (C::mix != 0 || C::turb) {
+    OSTC_UNROLL for (int l = 0; l < C::nsc; ++l) sv[l] = q[5 + l] * rinv;
+  }
+  double p, t;
+  if constexpr (C::mix != 0) {
+    const double e = q[4] / rho - 0.5 * (u * u + v * v + w * w);
+    t = B.bv[5 * sz + n];
+    newton_temperature<NS>(sv, rho, e, t, p);
+  } else {
+    p = (kDGammaAir - 1) * (q[4] - 0.5 * rho * vel2);
+    t = p * kDMwAir * rinv / kDR_u;
+  }
+  B.bv[n] = rho;
   B.bv[sz + n] = u;
   B.bv[2 * sz + n] = v;
   B.bv[3 * sz + n] = w;
-  const double vel2 = u * u + v * v + w * w;
+  B.bv[4 * sz + n] = p;
+  B.bv[5 * sz + n] = t;
   if constexpr (C::mix != 0 || C::turb) {
-    OSTC_UNROLL for (int l = 0; l < C::nsc; ++l) B.sv[l * sz + n] = B.cv[(5 + l) * sz + n] * rinv;
-  }
-  if constexpr (C::mix != 0) {
-    double Y[NS];
-    OSTC_UNROLL for (int l = 0; l < NS; ++l) Y[l] = B.sv[l * sz + n];
-    const double e = B.cv[4 * sz + n] / rho - 0.5 * (u * u + v * v + w * w);
-    double t = B.bv[5 * sz + n], p;
-    newton_temperature<NS>(Y, rho, e, t, p);
-    B.bv[5 * sz + n] = t;
-    B.bv[4 * sz + n] = p;
-  } else {
-    const double p = (kDGammaAir - 1) * (B.cv[4 * sz + n] - 0.5 * rho * vel2);
-    B.bv[4 * sz + n] = p;
-    B.bv[5 * sz + n] = p * kDMwAir * rinv / kDR_u;
+    OSTC_UNROLL for (int l = 0; l < C::nsc; ++l) B.sv[l * sz + n] = sv[l];
   }
   B.vel[n] = sqrt(vel2);
+  v5[0] = rho;
+  v5[1] = u;
+  v5[2] = v;
+  v5[3] = w;
+  v5[4] = p;
+  if constexpr (C::turb) {
+    turb2[0] = sv[NS];
+    turb2[1] = sv[NS + 1];
+  }
+}
+
+// The same from Q in memory (cv of point n must already hold the new Q).
+template <class C>
+__device__ __forceinline__ void primitives_from_q(const DevBlock &B, int64_t n) {
+  double q[C::nv], v5[5], turb2[2];
+  OSTC_UNROLL for (int l = 0; l < C::nv; ++l) q[l] = B.cv[l * B.G.size + n];
+  primitives_from_regs<C>(B, n, q, v5, turb2);
 }
 
 __device__ __forceinline__ bool flow_unphysical(const double *v) {
@@ -734,7 +757,7 @@ __device__ __forceinline__ bool flow_unphysical(const double *v) {
 // update_cv_and_bv, src/FieldOperation.cuh:139-183.  Counts unphysical cells
 // so that the limiter pass can skip the block when there are none.
 template <class C>
-__global__ void __launch_bounds__(kCta) k_update(const DevBlock *__restrict__ blks, Tiles T, int dq_sel,
+__global__ void __launch_bounds__(kCta, 3) k_update(const DevBlock *__restrict__ blks, Tiles T, int dq_sel,
                                                  unsigned int *bad_count) {
   constexpr int NV = C::nv;
   int b, i, j, k;
@@ -743,15 +766,20 @@ __global__ void __launch_bounds__(kCta) k_update(const DevBlock *__restrict__ bl
   const double *dq = dq_sel == 0 ? B.dq : (dq_sel == 1 ? B.dq0 : B.dqk);
   const int64_t n = B.G.at(i, j, k), nd = B.D.at(i, j, k), nz = B.Z.at(i, j, k);
   const int64_t sz = B.G.size, szd = B.D.size;
+  // every load first (the arrays may alias as far as the compiler knows, so a
+  // load after a store would wait for it), then the arithmetic, then the stores
   const double dt_div_jac = B.dt_local[nz] / B.jac[n];
-  OSTC_UNROLL for (int l = 0; l < NV; ++l) B.cv[l * sz + n] += dq[l * szd + nd] * dt_div_jac;
-  if (B.mz == 1) B.cv[3 * sz + n] = 0;
-  primitives_from_q<C>(B, n);
-  double v[5];
-  OSTC_UNROLL for (int l = 0; l < 5; ++l) v[l] = B.bv[l * sz + n];
+  double q[NV], d[NV];
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) q[l] = B.cv[l * sz + n];
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) d[l] = dq[l * szd + nd];
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) q[l] += d[l] * dt_div_jac;
+  if (B.mz == 1) q[3] = 0;
+  double v[5], turb2[2];
+  primitives_from_regs<C>(B, n, q, v, turb2);
+  OSTC_UNROLL for (int l = 0; l < NV; ++l) B.cv[l * sz + n] = q[l];
   bool bad = flow_unphysical(v);
   if constexpr (C::turb) {
-    const double tk = B.sv[C::ns * sz + n], tw = B.sv[(C::ns + 1) * sz + n];
+    const double tk = turb2[0], tw = turb2[1];
     bad |= isnan(tk) || isnan(tw) || tk < 0 || tw < 0;
   }
   if (bad) atomicAdd(bad_count, 1u);
@@ -1340,6 +1368,14 @@ __global__ void __launch_bounds__(kCta) k_init_mut(const DevBlock *__restrict__ 
 }
 
 // compute_wall_distance, src/Driver.cu:461-482 (brute force; halo ngg)
+// Squared distance to wall point w: the one expression both searches use, so
+// that they find the same minimum to the last bit.
+__device__ __forceinline__ double wall_d2(double x, double y, double z, const double *w) {
+  return (x - w[0]) * (x - w[0]) + (y - w[1]) * (y - w[1]) + (z - w[2]) * (z - w[2]);
+}
+
+// compute_wall_distance, src/Driver.cu:461-482: the square root of the least
+// squared distance to every wall point, capped at 1e6 as in the reference.
 static __global__ void __launch_bounds__(kCta) k_wall_distance(const DevBlock *__restrict__ blks, Tiles T,
                                                         const double *__restrict__ wall, int n_wall) {
   int b, i, j, k;
@@ -1349,9 +1385,81 @@ static __global__ void __launch_bounds__(kCta) k_wall_distance(const DevBlock *_
   const double x = B.x[n], y = B.y[n], z = B.z[n];
   double wd = 1e+6;
   for (int l = 0; l < n_wall; ++l) {
-    const double d = (x - wall[3 * l]) * (x - wall[3 * l]) + (y - wall[3 * l + 1]) * (y - wall[3 * l + 1]) +
-                     (z - wall[3 * l + 2]) * (z - wall[3 * l + 2]);
+    const double d = wall_d2(x, y, z, wall + 3 * l);
     if (wd > d) wd = d;
+  }
+  B.wall_dist[n] = sqrt(wd);
+}
+
+// The wall points sorted into a uniform grid of buckets of edge h over their
+// bounding box [lo, hi] (start: first point of each bucket, CSR; pts: x, y, z
+// of the points in bucket order).
+struct WallGrid {
+  double lo[3], hi[3], h;
+  int n[3];
+  const int *start;
+  const double *pts;
+};
+
+// The same distance by an exact search of the bucket grid: the buckets in
+// shells of growing Chebyshev index distance s around the point's own bucket
+// (clamped to the grid), stopping before shell s once the best squared
+// distance cannot exceed the least squared distance of any point in it.  A
+// bucket of shell s is s buckets away along some axis a that still has
+// buckets there, so its points are at least max((s - 1) h, out_a) away along
+// a and at least out_d along every other axis d, out_d being the point's
+// distance outside the points' bounding box along d (for a flat wall this
+// counts the height above it, so a point far from the wall stops after a few
+// shells).  The minimum found is the brute force's minimum: same points where
+// it matters, same expression (wall_d2).
+static __global__ void __launch_bounds__(kCta) k_wall_distance_grid(const DevBlock *__restrict__ blks, Tiles T,
+                                                             WallGrid G) {
+  int b, i, j, k;
+  if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
+  const DevBlock &B = blks[b];
+  const int64_t n = B.G.at(i, j, k);
+  const double p[3] = {B.x[n], B.y[n], B.z[n]};
+  int c[3];
+  double out2[3];
+  for (int d = 0; d < 3; ++d) {
+    const double f = floor((p[d] - G.lo[d]) / G.h);
+    c[d] = f < 0 ? 0 : (f >= G.n[d] ? G.n[d] - 1 : static_cast<int>(f));
+    const double o = p[d] < G.lo[d] ? G.lo[d] - p[d] : (p[d] > G.hi[d] ? p[d] - G.hi[d] : 0.0);
+    out2[d] = o * o;
+  }
+  const int smax = max(G.n[0], max(G.n[1], G.n[2]));
+  double wd = 1e+6;
+  for (int s = 0; s <= smax; ++s) {
+    if (s >= 1) {
+      double bound = -1;  // least squared distance of a point in shell s (none: -1)
+      for (int a = 0; a < 3; ++a) {
+        if (c[a] + s >= G.n[a] && c[a] - s < 0) continue;
+        const double g = (s - 1) * G.h;
+        double lb = fmax(g * g, out2[a]);
+        for (int d = 0; d < 3; ++d)
+          if (d != a) lb += out2[d];
+        bound = bound < 0 ? lb : fmin(bound, lb);
+      }
+      if (bound < 0 || wd <= bound * (1 - 1e-12)) break;
+    }
+    for (int dz = -s; dz <= s; ++dz) {
+      const int z = c[2] + dz;
+      if (z < 0 || z >= G.n[2]) continue;
+      for (int dy = -s; dy <= s; ++dy) {
+        const int y = c[1] + dy;
+        if (y < 0 || y >= G.n[1]) continue;
+        const bool face = abs(dz) == s || abs(dy) == s;
+        for (int dx = -s; dx <= s; dx += (face ? 1 : 2 * max(s, 1))) {
+          const int x = c[0] + dx;
+          if (x < 0 || x >= G.n[0]) continue;
+          const int bk = (z * G.n[1] + y) * G.n[0] + x;
+          for (int q = G.start[bk]; q < G.start[bk + 1]; ++q) {
+            const double d = wall_d2(p[0], p[1], p[2], G.pts + 3 * q);
+            if (wd > d) wd = d;
+          }
+        }
+      }
+    }
   }
   B.wall_dist[n] = sqrt(wd);
 }

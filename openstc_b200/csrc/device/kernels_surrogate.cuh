@@ -22,10 +22,14 @@ struct JudgeTables {
   float sA2[kMaxReac], lnA2[kMaxReac], b2[kMaxReac], Ea2[kMaxReac];
   float troe_a[kMaxReac], troe_t3[kMaxReac], troe_t1[kMaxReac], troe_t2[kMaxReac];
   float tb[kMaxReac * kMaxSpec];
-  float mw[kMaxSpec], t_low[kMaxSpec], t_mid[kMaxSpec], low[kMaxSpec * 7], high[kMaxSpec * 7];
+  float sf[kMaxReac * kMaxSpec], sb[kMaxReac * kMaxSpec], nu[kMaxReac * kMaxSpec];  // stoichiometry, sb - sf
+  float order[kMaxReac];
+  float mw[kMaxSpec], ln_t_low[kMaxSpec], t_mid[kMaxSpec], low[kMaxSpec * 7], high[kMaxSpec * 7];
 };
 
 static __constant__ JudgeTables cJ;
+
+constexpr int kJudgeCta = 256;  // threads of a k_sur_judge block
 
 inline JudgeTables make_judge_tables(const DevParams &p) {
   JudgeTables j{};
@@ -44,10 +48,16 @@ inline JudgeTables make_judge_tables(const DevParams &p) {
     j.troe_t1[r] = static_cast<float>(p.troe_t1[r]);
     j.troe_t2[r] = static_cast<float>(p.troe_t2[r]);
   }
-  for (int q = 0; q < kMaxReac * kMaxSpec; ++q) j.tb[q] = static_cast<float>(p.tb[q]);
+  for (int q = 0; q < kMaxReac * kMaxSpec; ++q) {
+    j.tb[q] = static_cast<float>(p.tb[q]);
+    j.sf[q] = static_cast<float>(p.sf[q]);
+    j.sb[q] = static_cast<float>(p.sb[q]);
+    j.nu[q] = static_cast<float>(p.sb[q] - p.sf[q]);
+  }
+  for (int r = 0; r < kMaxReac; ++r) j.order[r] = static_cast<float>(p.order[r]);
   for (int k = 0; k < kMaxSpec; ++k) {
     j.mw[k] = static_cast<float>(p.mw[k]);
-    j.t_low[k] = static_cast<float>(p.t_low[k]);
+    j.ln_t_low[k] = p.t_low[k] > 0 ? static_cast<float>(std::log(p.t_low[k])) : -80.f;
     j.t_mid[k] = static_cast<float>(p.t_mid[k]);
   }
   for (int q = 0; q < kMaxSpec * 7; ++q) {
@@ -97,31 +107,40 @@ __device__ inline void epi_increment(double T, double rho, const double *Y, doub
 // diagonal of the chemistry Jacobian (the reference's DA treatment,
 // src/FiniteRateChem.cu:196-209, 400-412), dY_k = (dt omega_k / rho) /
 // (1 + dt omega_d,k / (rho Y_k)), from the production and destruction rates of
-// finite_rate_chemistry (src/FiniteRateChem.cu:7-171; every rate and
-// equilibrium constant as one exponential, exponents clamped to the FP32
-// range).  The full EPI step (I - dt J)^-1 dt omega / rho couples the species;
-// the diagonal keeps each species' own stiffness, which is what bounds the
-// increments of trace radicals, so it follows the EPI step closely where the
-// explicit increment would not.  A cell whose network increment disagrees
-// with it is reacting in a way the network did not capture.  p in Pa, dt in s.
+// finite_rate_chemistry (src/FiniteRateChem.cu:7-171).  The full EPI step
+// (I - dt J)^-1 dt omega / rho couples the species; the diagonal keeps each
+// species' own stiffness, which is what bounds the increments of trace
+// radicals, so it follows the EPI step closely where the explicit increment
+// would not.  A cell whose network increment disagrees with it is reacting in
+// a way the network did not capture.  p in Pa, dt in s.
+// Arithmetic: every rate, equilibrium constant and concentration product is
+// one exponential of a sum over the species with the stoichiometric
+// coefficients as FP32 factors (q_f = k_f exp(sum_k nu'_k ln c_k)), exponents
+// clamped to the FP32 range, so the loops over species have compile-time trip
+// counts and read uniform constant-bank operands.  Concentrations below 1e-30
+// count as 1e-30 (their products underflow to zero like the exact ones).
 template <int NS>
-__device__ __forceinline__ void judge_increment(float T, float p, float dt, const double *Y, float *e) {
+__device__ __forceinline__ void judge_increment(float T, float p, float dt, const float *Y, float *e) {
   float inv_mw = 0;
 #pragma unroll
-  for (int k = 0; k < NS; ++k) inv_mw += static_cast<float>(Y[k]) / cJ.mw[k];
+  for (int k = 0; k < NS; ++k) inv_mw += Y[k] / cJ.mw[k];
   const float rho = p / (8314.462618f * T * inv_mw);
-  float c[NS], g[NS];
+  float c[NS], lc[NS], g[NS];
   const float ln_t = logf(T), t_inv = 1.f / T;
 #pragma unroll
   for (int k = 0; k < NS; ++k) {
-    c[k] = rho * static_cast<float>(Y[k]) / cJ.mw[k] * 1e-3f;
-    // g_k / RT from the NASA-7 polynomials (frozen below T_low)
-    const float tt = T < cJ.t_low[k] ? cJ.t_low[k] : T;
+    c[k] = rho * Y[k] / cJ.mw[k] * 1e-3f;
+    lc[k] = logf(fmaxf(c[k], 1e-30f));
+    // g_k / RT from the NASA-7 polynomials (frozen below T_low): tt = max(T,
+    // T_low) and ln tt = max(ln T, ln T_low)
+    const float lt = fmaxf(ln_t, cJ.ln_t_low[k]);
+    const float tt = lt == ln_t ? T : expf(lt);
     const bool lo = tt < cJ.t_mid[k];
-    const float *a = lo ? &cJ.low[k * 7] : &cJ.high[k * 7];
-    const float lt = tt == T ? ln_t : logf(tt);
-    g[k] = a[0] * (1.f - lt) - 0.5f * a[1] * tt - a[2] * tt * tt * (1.f / 6.f) - a[3] * tt * tt * tt * (1.f / 12.f) -
-           a[4] * tt * tt * tt * tt * 0.05f + a[5] / tt - a[6];
+    float a[7];
+#pragma unroll
+    for (int m = 0; m < 7; ++m) a[m] = lo ? cJ.low[k * 7 + m] : cJ.high[k * 7 + m];
+    g[k] = a[0] * (1.f - lt) + a[5] / tt - a[6] -
+           tt * (0.5f * a[1] + tt * (a[2] * (1.f / 6.f) + tt * (a[3] * (1.f / 12.f) + tt * (a[4] * 0.05f))));
   }
   float omega[NS], destruction[NS];
 #pragma unroll
@@ -156,33 +175,28 @@ __device__ __forceinline__ void judge_increment(float T, float p, float dt, cons
         kf = kf * pr / (1.f + pr) * F;
       }
     }
-    float kb;
-    if (type != 2) {
-      float dg = 0;
-#pragma unroll
-      for (int k = 0; k < NS; ++k) dg += g[k] * static_cast<float>(cP.sb[r * NS + k] - cP.sf[r * NS + k]);
-      kb = kf * expf(fminf(dg - static_cast<float>(cP.order[r]) * ln_temp_t, 80.f));
-    } else {
-      kb = rate(cJ.sA2[r], cJ.lnA2[r], cJ.b2[r], cJ.Ea2[r]);
-    }
-    float q1 = kf, q2 = kb;
+    float s1 = 0, s2 = 0, dg = 0;
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
-      for (int m = 0; m < cP.sf[r * NS + k]; ++m) q1 *= c[k];
-      for (int m = 0; m < cP.sb[r * NS + k]; ++m) q2 *= c[k];
+      s1 += cJ.sf[r * NS + k] * lc[k];
+      s2 += cJ.sb[r * NS + k] * lc[k];
+      dg += cJ.nu[r * NS + k] * g[k];
     }
+    const float q1 = kf * expf(fminf(s1, 80.f));
+    const float q2 = type != 2 ? kf * expf(fminf(fminf(dg - cJ.order[r] * ln_temp_t, 80.f) + s2, 80.f))
+                               : rate(cJ.sA2[r], cJ.lnA2[r], cJ.b2[r], cJ.Ea2[r]) * expf(fminf(s2, 80.f));
     const float q = q1 - q2;
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
-      omega[k] += static_cast<float>(cP.sb[r * NS + k] - cP.sf[r * NS + k]) * q;
-      destruction[k] += static_cast<float>(cP.sf[r * NS + k]) * q1 + static_cast<float>(cP.sb[r * NS + k]) * q2;
+      omega[k] += cJ.nu[r * NS + k] * q;
+      destruction[k] += cJ.sf[r * NS + k] * q1 + cJ.sb[r * NS + k] * q2;
     }
   }
   const float f = dt / rho;
 #pragma unroll
   for (int k = 0; k < NS; ++k) {
     const float w = cJ.mw[k] * 1e3f;
-    const float y = fmaxf(static_cast<float>(Y[k]), 1e-30f);
+    const float y = fmaxf(Y[k], 1e-30f);
     e[k] = f * omega[k] * w / (1.f + f * destruction[k] * w / y);
   }
 }
@@ -191,15 +205,15 @@ __device__ __forceinline__ void judge_increment(float T, float p, float dt, cons
 // species within gate.judge_rel of the diagonal point-implicit increment plus
 // gate.judge_abs (Y_k + gate.y_floor); a non-finite judge increment fails.
 template <int NS>
-__device__ __forceinline__ bool judge_accepts(const SurrogateGate &g, float T, float p, float dt, const double *Y,
-                                              const double *dy) {
+__device__ __forceinline__ bool judge_accepts(const SurrogateGate &g, float T, float p, float dt, const float *Y,
+                                              const float *dy) {
   float e[NS];
   judge_increment<NS>(T, p, dt, Y, e);
   bool ok = true;
 #pragma unroll
   for (int k = 0; k < NS; ++k) {
-    const float err = fabsf(static_cast<float>(dy[k]) - e[k]);
-    const float tol = g.judge_rel * fabsf(e[k]) + g.judge_abs * static_cast<float>(Y[k] + g.y_floor);
+    const float err = fabsf(dy[k] - e[k]);
+    const float tol = g.judge_rel * fabsf(e[k]) + g.judge_abs * (Y[k] + g.y_floor);
     if (!(err <= tol)) ok = false;
   }
   return ok;
@@ -284,7 +298,15 @@ __device__ __forceinline__ bool decode_ne(const SurrogateDev &p, const float *o,
     dy[k] -= w[k] * corr;
     if (Y[k] + dy[k] < -1e-9) ok = false;
   }
-  if (JUDGE && ok && g.judge_rel >= 0.f) ok = judge_accepts<NS>(g, T, exp10f(lp), exp10f(ldt), Y, dy);
+  if (JUDGE && ok && g.judge_rel >= 0.f) {
+    float yf[NS], dyf[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      yf[k] = static_cast<float>(Y[k]);
+      dyf[k] = static_cast<float>(dy[k]);
+    }
+    ok = judge_accepts<NS>(g, T, exp10f(lp), exp10f(ldt), yf, dyf);
+  }
   return ok;
 }
 
@@ -776,28 +798,33 @@ __global__ void __launch_bounds__(256) k_sur_candidates(const DevBlock *__restri
 // The judge over the cells the fused inference accepted (the candidate list
 // of this step): a cell whose increment (recovered from its rate rho dY / dt)
 // the judge refuses goes back to the point-implicit chemistry, and the
-// statistics move it from accepted to fallback.
+// statistics move it from accepted to fallback.  Each warp reads 32
+// candidates at a time and queues the accepted ones in shared memory, judging
+// 32 queued cells at once, so every lane judges a cell (about half of the
+// candidates are accepted).
 template <class C>
-__global__ void __launch_bounds__(256) k_sur_judge(const DevBlock *__restrict__ blks, int b, SurrogateGate g,
-                                                   const int *__restrict__ cand, const int *cand_count,
-                                                   unsigned long long *stats) {
+__global__ void __launch_bounds__(kJudgeCta, 3) k_sur_judge(const DevBlock *__restrict__ blks, int b, SurrogateGate g,
+                                                         const int *__restrict__ cand, const int *cand_count,
+                                                         unsigned long long *stats) {
   constexpr int NS = C::ns;
+  __shared__ int queue[kJudgeCta / 32][64];
   if (g.judge_rel < 0.f) return;
   const DevBlock &B = blks[b];
   const int count = *cand_count;
   const int64_t sz = B.G.size, sz0 = B.Z.size;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
-    const int64_t c = cand[q];
-    const int i = static_cast<int>(c % B.mx), j = static_cast<int>((c / B.mx) % B.my),
-              k = static_cast<int>(c / (static_cast<int64_t>(B.mx) * B.my));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int *wq = queue[warp];
+  int held = 0;  // queued cells of this warp (warp-uniform)
+  auto judge = [&](bool active, int c) {
+    if (!active) return;
+    const int i = c % B.mx, j = (c / B.mx) % B.my, k = c / (B.mx * B.my);
     const int64_t n = B.G.at(i, j, k), nz = B.Z.at(i, j, k);
-    if (!B.chem_quiet[nz]) continue;
     const double rho = B.bv[n], dt = B.dt_local[nz];
-    double Y[NS], dy[NS];
+    float Y[NS], dy[NS];
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
-      Y[s] = B.sv[s * sz + n];
-      dy[s] = B.chem_rate[s * sz0 + nz] * dt / rho;
+      Y[s] = static_cast<float>(B.sv[s * sz + n]);
+      dy[s] = static_cast<float>(B.chem_rate[s * sz0 + nz] * dt / rho);
     }
     if (!judge_accepts<NS>(g, static_cast<float>(B.bv[5 * sz + n]), static_cast<float>(B.bv[4 * sz + n]),
                            static_cast<float>(dt), Y, dy)) {
@@ -805,7 +832,32 @@ __global__ void __launch_bounds__(256) k_sur_judge(const DevBlock *__restrict__ 
       atomicAdd(&stats[0], ~0ull);  // minus one
       atomicAdd(&stats[1], 1ull);
     }
+  };
+  const int warps = gridDim.x * (kJudgeCta / 32);
+  for (int base = (blockIdx.x * (kJudgeCta / 32) + warp) * 32; base < count; base += warps * 32) {
+    const int q = base + lane;
+    int c = 0;
+    bool acc = false;
+    if (q < count) {
+      c = cand[q];
+      const int i = c % B.mx, j = (c / B.mx) % B.my, k = c / (B.mx * B.my);
+      acc = B.chem_quiet[B.Z.at(i, j, k)] != 0;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, acc);
+    if (acc) wq[held + __popc(m & ((1u << lane) - 1u))] = c;
+    held += __popc(m);
+    __syncwarp();
+    if (held >= 32) {
+      const int cell = wq[lane];
+      __syncwarp();
+      if (lane < held - 32) wq[lane] = wq[32 + lane];
+      held -= 32;
+      __syncwarp();
+      judge(true, cell);
+    }
   }
+  __syncwarp();
+  judge(lane < held, lane < held ? wq[lane] : 0);
 }
 
 // EPI fallback for the listed cells of block b (grid-stride over the list).

@@ -413,6 +413,7 @@ void Driver::initialize_computation() {
   s.device = opt.device;
   s.precision = opt.precision;
   s.exact_inner = opt.exact_inner;
+  s.wall_distance = opt.wall_distance;
   plt_out_.reset();  // bound to the engine it copies from
   engine_ = make_engine(s);
   for (int b = 0; b < mesh.n_block; ++b) {

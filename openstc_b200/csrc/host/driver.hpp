@@ -23,6 +23,7 @@ struct DriverOptions {
   bool quiet = false;
   int precision = 0;  // 0 FP64, 1 FP32-bulk / FP64-critical
   bool exact_inner = false;  // multi-block grids computed as one block (ostc_options::exact_inner)
+  int wall_distance = 0;     // ostc_options::wall_distance
 };
 
 class Driver {
