@@ -24,7 +24,8 @@ struct JudgeTables {
   float tb[kMaxReac * kMaxSpec];
   float sf[kMaxReac * kMaxSpec], sb[kMaxReac * kMaxSpec], nu[kMaxReac * kMaxSpec];  // stoichiometry, sb - sf
   float order[kMaxReac];
-  float mw[kMaxSpec], ln_t_low[kMaxSpec], t_mid[kMaxSpec], low[kMaxSpec * 7], high[kMaxSpec * 7];
+  float mw[kMaxSpec], mw_inv[kMaxSpec], t_low[kMaxSpec], ln_t_low[kMaxSpec], t_mid[kMaxSpec];
+  float low[kMaxSpec * 7], high[kMaxSpec * 7];
 };
 
 static __constant__ JudgeTables cJ;
@@ -57,6 +58,8 @@ inline JudgeTables make_judge_tables(const DevParams &p) {
   for (int r = 0; r < kMaxReac; ++r) j.order[r] = static_cast<float>(p.order[r]);
   for (int k = 0; k < kMaxSpec; ++k) {
     j.mw[k] = static_cast<float>(p.mw[k]);
+    j.mw_inv[k] = p.mw[k] > 0 ? static_cast<float>(1.0 / p.mw[k]) : 0.f;
+    j.t_low[k] = static_cast<float>(p.t_low[k]);
     j.ln_t_low[k] = p.t_low[k] > 0 ? static_cast<float>(std::log(p.t_low[k])) : -80.f;
     j.t_mid[k] = static_cast<float>(p.t_mid[k]);
   }
@@ -118,35 +121,36 @@ __device__ inline void epi_increment(double T, double rho, const double *Y, doub
 // coefficients as FP32 factors (q_f = k_f exp(sum_k nu'_k ln c_k)), exponents
 // clamped to the FP32 range, so the loops over species have compile-time trip
 // counts and read uniform constant-bank operands.  Concentrations below 1e-30
-// count as 1e-30 (their products underflow to zero like the exact ones).
+// count as 1e-30 (their products underflow to zero like the exact ones).  The
+// exponentials, logarithms and quotients are the hardware approximations
+// (__expf, __logf, __fdividef: relative errors near 1e-6, against the judge's
+// 25 % tolerance), which have no slow paths for lanes to diverge on.
 template <int NS>
 __device__ __forceinline__ void judge_increment(float T, float p, float dt, const float *Y, float *e) {
   float inv_mw = 0;
 #pragma unroll
-  for (int k = 0; k < NS; ++k) inv_mw += Y[k] / cJ.mw[k];
-  const float rho = p / (8314.462618f * T * inv_mw);
+  for (int k = 0; k < NS; ++k) inv_mw += Y[k] * cJ.mw_inv[k];
+  const float rho = __fdividef(p, 8314.462618f * T * inv_mw);
   float c[NS], lc[NS], g[NS];
-  const float ln_t = logf(T), t_inv = 1.f / T;
+  const float ln_t = __logf(T), t_inv = __fdividef(1.f, T);
 #pragma unroll
   for (int k = 0; k < NS; ++k) {
-    c[k] = rho * Y[k] / cJ.mw[k] * 1e-3f;
-    lc[k] = logf(fmaxf(c[k], 1e-30f));
-    // g_k / RT from the NASA-7 polynomials (frozen below T_low): tt = max(T,
-    // T_low) and ln tt = max(ln T, ln T_low)
-    const float lt = fmaxf(ln_t, cJ.ln_t_low[k]);
-    const float tt = lt == ln_t ? T : expf(lt);
+    c[k] = rho * Y[k] * cJ.mw_inv[k] * 1e-3f;
+    lc[k] = __logf(fmaxf(c[k], 1e-30f));
+    // g_k / RT from the NASA-7 polynomials, frozen below T_low
+    const float tt = fmaxf(T, cJ.t_low[k]), lt = fmaxf(ln_t, cJ.ln_t_low[k]);
     const bool lo = tt < cJ.t_mid[k];
     float a[7];
 #pragma unroll
     for (int m = 0; m < 7; ++m) a[m] = lo ? cJ.low[k * 7 + m] : cJ.high[k * 7 + m];
-    g[k] = a[0] * (1.f - lt) + a[5] / tt - a[6] -
+    g[k] = a[0] * (1.f - lt) + __fdividef(a[5], tt) - a[6] -
            tt * (0.5f * a[1] + tt * (a[2] * (1.f / 6.f) + tt * (a[3] * (1.f / 12.f) + tt * (a[4] * 0.05f))));
   }
   float omega[NS], destruction[NS];
 #pragma unroll
   for (int k = 0; k < NS; ++k) omega[k] = destruction[k] = 0;
   auto rate = [&](float sA, float lnA, float b, float Ea) {
-    return sA * expf(fminf(lnA + b * ln_t - Ea * t_inv, 80.f));
+    return sA * __expf(fminf(lnA + b * ln_t - Ea * t_inv, 80.f));
   };
   const float ln_temp_t = logf(101325.0f / 8314.462618f * 1e-3f) - ln_t;
   const int nr = cP.nr;
@@ -160,19 +164,21 @@ __device__ __forceinline__ void judge_increment(float T, float p, float dt, cons
       for (int k = 0; k < NS; ++k) cc += c[k] * cJ.tb[r * NS + k];
       if (type == 4) {
         kf *= cc;
-      } else if (kf > 0.f) {  // a high-pressure rate that underflows FP32 leaves the rate at zero
-        const float pr = fmaxf(rate(cJ.sA2[r], cJ.lnA2[r], cJ.b2[r], cJ.Ea2[r]) * cc / kf, 1e-30f);
+      } else {
+        // reduced pressure; a high-pressure rate that underflows FP32 leaves
+        // the rate at zero
+        const float pr = fmaxf(__fdividef(rate(cJ.sA2[r], cJ.lnA2[r], cJ.b2[r], cJ.Ea2[r]) * cc, kf), 1e-30f);
         float F = 1.f;
         if (type > 5) {
           const float a = cJ.troe_a[r];
-          float fc = (1 - a) * expf(-T / cJ.troe_t3[r]) + a * expf(-T / cJ.troe_t1[r]);
-          if (type == 7) fc += expf(-cJ.troe_t2[r] / T);
-          const float lfc = log10f(fc), lpr = log10f(pr);
+          float fc = (1 - a) * __expf(__fdividef(-T, cJ.troe_t3[r])) + a * __expf(__fdividef(-T, cJ.troe_t1[r]));
+          if (type == 7) fc += __expf(-cJ.troe_t2[r] * t_inv);
+          const float lfc = __log10f(fc), lpr = __log10f(pr);
           const float cq = -0.4f - 0.67f * lfc, nq = 0.75f - 1.27f * lfc;
-          const float tmp = (lpr + cq) / (nq - 0.14f * (lpr + cq));
-          F = exp10f(lfc / (1.f + tmp * tmp));
+          const float tmp = __fdividef(lpr + cq, nq - 0.14f * (lpr + cq));
+          F = __exp10f(__fdividef(lfc, 1.f + tmp * tmp));
         }
-        kf = kf * pr / (1.f + pr) * F;
+        if (kf > 0.f) kf = kf * __fdividef(pr, 1.f + pr) * F;
       }
     }
     float s1 = 0, s2 = 0, dg = 0;
@@ -182,9 +188,9 @@ __device__ __forceinline__ void judge_increment(float T, float p, float dt, cons
       s2 += cJ.sb[r * NS + k] * lc[k];
       dg += cJ.nu[r * NS + k] * g[k];
     }
-    const float q1 = kf * expf(fminf(s1, 80.f));
-    const float q2 = type != 2 ? kf * expf(fminf(fminf(dg - cJ.order[r] * ln_temp_t, 80.f) + s2, 80.f))
-                               : rate(cJ.sA2[r], cJ.lnA2[r], cJ.b2[r], cJ.Ea2[r]) * expf(fminf(s2, 80.f));
+    const float q1 = kf * __expf(fminf(s1, 80.f));
+    const float q2 = type != 2 ? kf * __expf(fminf(fminf(dg - cJ.order[r] * ln_temp_t, 80.f) + s2, 80.f))
+                               : rate(cJ.sA2[r], cJ.lnA2[r], cJ.b2[r], cJ.Ea2[r]) * __expf(fminf(s2, 80.f));
     const float q = q1 - q2;
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
@@ -192,12 +198,12 @@ __device__ __forceinline__ void judge_increment(float T, float p, float dt, cons
       destruction[k] += cJ.sf[r * NS + k] * q1 + cJ.sb[r * NS + k] * q2;
     }
   }
-  const float f = dt / rho;
+  const float f = __fdividef(dt, rho);
 #pragma unroll
   for (int k = 0; k < NS; ++k) {
     const float w = cJ.mw[k] * 1e3f;
     const float y = fmaxf(Y[k], 1e-30f);
-    e[k] = f * omega[k] * w / (1.f + f * destruction[k] * w / y);
+    e[k] = __fdividef(f * omega[k] * w, 1.f + f * destruction[k] * w * __fdividef(1.f, y));
   }
 }
 
