@@ -325,31 +325,36 @@ __device__ __forceinline__ bool decode(const SurrogateDev &p, const float *o, fl
 
 // ------------------------------------------------------------ fused kernel
 // A persistent kernel, one CTA per SM, that runs the tiles of 128 cells of a
-// block through the network as a software pipeline on mbarriers:
+// block through the network as a software pipeline on mbarriers, with two
+// tiles in flight: tiles alternate between two slots (tile it uses slot
+// it % 2), each with its own 256-column TMEM accumulator, 64 KB activation
+// buffer and 4 KB feature buffer, so that one slot's epilogue runs while the
+// tensor cores work on the other slot's layer.
 //   * warp 17 (one lane) streams the hidden layers' weights through a ring
-//     of kStages shared-memory stages of 32 KB (K = 64), in the order the MMAs
-//     consume them; the first and output layers' weights (8 KB each) stay
-//     resident;
-//   * warp 16 issues the tcgen05 MMAs of global layer g (tile g / 5, layer
-//     g % 5) into accumulator g % 2 (2 x 256 TMEM columns);
-//   * warps 0-15 (TMEM lane quarter w % 4, column group w / 4) run the hidden
-//     epilogues: accumulator + bias -> GELU -> bf16 activations in two steps,
-//     step s covering columns 32 (w / 4) + 128 s; each step's 128 columns are
-//     released to the MMAs of the next layer as soon as all sixteen warps have
-//     written them, so that MMA overlaps the second half of this epilogue;
-//   * warps 18-21 (lane quarters 2, 3, 0, 1) compute the features of the
-//     next tile and decode / gate / apply the outputs of the current one.
-// One activation buffer serves every layer (the epilogue of layer L only
-// starts once the MMAs of layer L, its last readers, have completed), and
-// features alternate between two 4 KB buffers by tile, so no stage waits for
-// the one before it except through the data it needs.  Every wait is bounded: a wait that runs
-// out raises the CTA's abort flag, every role then leaves its loop, the MMAs
-// and copies in flight are drained, and the kernel reports the error.
+//     of kStages shared-memory stages of 16 KB (K = 32), in the order the
+//     MMAs consume them; the first and output layers' weights (8 KB each)
+//     stay resident;
+//   * warp 16 issues the tcgen05 MMAs in the order (pair of tiles, layer,
+//     slot): layer L of tile 2p, layer L of tile 2p + 1, layer L + 1 of
+//     tile 2p, ...;
+//   * warps 0-15 (TMEM lane quarter w % 4, column group w / 4) run the
+//     hidden epilogues in the same order: accumulator + bias -> GELU -> bf16
+//     activations of the slot;
+//   * warps 18-21 (lane quarters 2, 3, 0, 1) compute the features of tile
+//     it + 2 once tile it's first layer has read its slot's feature buffer,
+//     and decode / gate / apply tile it's outputs.
+// Within a slot every stage waits for the one before it (MMA of layer L ->
+// epilogue of layer L -> MMA of layer L + 1 ... -> decode -> first layer of
+// the slot's next tile), so each barrier of a slot completes its phases in
+// that order and a waiter is never more than one phase behind.  Every wait
+// is bounded: a wait that runs out raises the CTA's abort flag, every role
+// then leaves its loop, the MMAs and copies in flight are drained, and the
+// kernel reports the error.
 constexpr int kCells = 128;
 constexpr int kEpiWarps = 16;
 constexpr int kMmaWarp = 16, kLoadWarp = 17, kIoWarp0 = 18;
 constexpr int kThreads = 32 * 22;
-constexpr int kStageChunks = 4;  // weight chunks per ring stage
+constexpr int kStageChunks = 2;  // weight chunks per ring stage
 constexpr int kStages = 4;       // ring stages
 constexpr int kFusedElem = 4;  // largest element count of the fused kernel's conservation gate
 constexpr int kRecheckEvery = 4;  // a cell the gate rejected is evaluated again within this many steps
@@ -357,25 +362,23 @@ constexpr int kRecheckEvery = 4;  // a cell the gate rejected is evaluated again
 // the whole first layer [256 x 16] or the whole output layer [16 x 256],
 // all packed K-major canonical with 16-column tiles.
 constexpr uint32_t kChunkBytes = kSurHidden * 16 * 2;
-constexpr int kTileStages = 3 * 4;  // streamed stages per tile: 3 hidden layers x 4 groups
+constexpr int kLayerStages = kSurHidden / 16 / kStageChunks;  // streamed stages per hidden layer
 constexpr uint32_t kActBytes = 128 * kSurHidden * 2;
 constexpr uint32_t kStageBytes = kStageChunks * kChunkBytes;
 constexpr uint32_t kX0Bytes = 128 * kSurInPad * 2;
-// barriers: full[S], empty[S], feat_full[2], x0_free[2], mma_epi[2], mma_out, acc_free[2], act_ready[2], res,
-// drain.  Each barrier has waiters that are never more than one phase behind
-// its arrivals, which is what parity waits need: the hidden layers' MMAs
-// signal the epilogue through mma_epi (by epilogue index), the output layer's
-// the decode through mma_out (by tile).
-constexpr int kBars = 2 * kStages + 2 + 2 + 2 + 1 + 2 + 2 + 1 + 1;
+// barriers: full[S], empty[S], and per slot feat_full, x0_free, mma_done,
+// epi_done, out_done, out_free; then res, drain.
+constexpr int kBars = 2 * kStages + 6 * 2 + 1 + 1;
 constexpr uint32_t kBiasBytes = (4 * kSurHidden + kSurOutPad) * 4;  // every layer's bias, staged once per CTA
-constexpr uint32_t kSmem = kActBytes + 2 * kX0Bytes + 2 * kChunkBytes + kStages * kStageBytes + kBiasBytes + kBars * 8 + 16;
+constexpr uint32_t kSmem =
+    2 * kActBytes + 2 * kX0Bytes + 2 * kChunkBytes + kStages * kStageBytes + kBiasBytes + kBars * 8 + 16;
 static_assert(kSmem <= 232448, "shared memory of one CTA");
 
-// Source of streamed stage s (0..kTileStages-1) of a tile: K chunks
-// 4 (s % 4) .. 4 (s % 4) + 3 of hidden layer 1 + s / 4, contiguous in its
-// packed weights
+// Source of stage s (0 .. 3 kLayerStages - 1) of hidden layers 1-3: K chunks
+// kStageChunks (s % kLayerStages) onwards of hidden layer 1 + s / kLayerStages,
+// contiguous in its packed weights
 __device__ __forceinline__ const uint8_t *stage_src(const SurrogateDev &P, int s) {
-  return P.w_packed[1 + s / 4] + static_cast<size_t>(s % 4) * kStageBytes;
+  return P.w_packed[1 + s / kLayerStages] + static_cast<size_t>(s % kLayerStages) * kStageBytes;
 }
 
 // Asynchronous bulk copies into shared memory: the stage's mbarrier is told
@@ -554,17 +557,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_sur_infer(const DevBlock *__res
                                                            int *err, const int *__restrict__ cand,
                                                            const int *cand_count, int *phase_ctr) {
   extern __shared__ __align__(128) uint8_t smem[];
-  uint8_t *act = smem;                     // 64 KB
-  uint8_t *x0 = smem + kActBytes;          // 2 x 4 KB, by tile
-  uint8_t *wres = x0 + 2 * kX0Bytes;       // first and output layers' weights, 2 x 8 KB
-  uint8_t *stages = wres + 2 * kChunkBytes;  // kStages x 32 KB
+  uint8_t *act = smem;                       // 2 x 64 KB, by slot
+  uint8_t *x0 = smem + 2 * kActBytes;        // 2 x 4 KB, by slot
+  uint8_t *wres = x0 + 2 * kX0Bytes;         // first and output layers' weights, 2 x 8 KB
+  uint8_t *stages = wres + 2 * kChunkBytes;  // kStages x 16 KB
   float *sbias = reinterpret_cast<float *>(stages + kStages * kStageBytes);
   uint64_t *bars = reinterpret_cast<uint64_t *>(reinterpret_cast<uint8_t *>(sbias) + kBiasBytes);
   uint64_t *full = bars, *empty = full + kStages, *feat_full = empty + kStages, *x0_free = feat_full + 2,
-           *mma_epi = x0_free + 2, *mma_out = mma_epi + 2, *acc_free = mma_out + 1, *act_ready = acc_free + 2,
-           *drain = act_ready + 2, *res_full = drain + 1;
-  static_assert(kBars == 2 * kStages + 2 + 2 + 2 + 1 + 2 + 2 + 1 + 1, "one slot per barrier");
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(res_full + 1);
+           *mma_done = x0_free + 2, *epi_done = mma_done + 2, *out_done = epi_done + 2, *out_free = out_done + 2,
+           *res_full = out_free + 2, *drain = res_full + 1;
+  static_assert(kBars == 2 * kStages + 6 * 2 + 1 + 1, "one slot per barrier");
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(drain + 1);
   volatile int *abort = reinterpret_cast<volatile int *>(tslot + 1);
   const DevBlock &B = blks[b];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -573,9 +576,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_sur_infer(const DevBlock *__res
   // the cell of item idx (past the end: an invalid cell)
   auto cell_of = [&](int64_t idx) -> int64_t { return cand ? (idx < n_items ? cand[idx] : cells) : idx; };
   const int64_t ntiles = (n_items + kCells - 1) / kCells;
-  // this CTA's tiles: blockIdx.x, blockIdx.x + gridDim.x, ...
+  // this CTA's tiles: blockIdx.x, blockIdx.x + gridDim.x, ...; tile it sits in slot it % 2
   const int my_tiles =
       blockIdx.x < ntiles ? static_cast<int>((ntiles - 1 - blockIdx.x) / gridDim.x + 1) : 0;
+  const int n_pairs = (my_tiles + 1) / 2;
 
   if (tid == 0) {
     for (int q = 0; q < kStages; ++q) {
@@ -585,13 +589,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_sur_infer(const DevBlock *__res
     for (int q = 0; q < 2; ++q) {
       tc::mbar_init(&feat_full[q], 4);
       tc::mbar_init(&x0_free[q], 1);
-      tc::mbar_init(&mma_epi[q], 1);
-      tc::mbar_init(&acc_free[q], kEpiWarps);
+      tc::mbar_init(&mma_done[q], 1);
+      tc::mbar_init(&epi_done[q], kEpiWarps);
+      tc::mbar_init(&out_done[q], 1);
+      tc::mbar_init(&out_free[q], 4);
     }
-    for (int q = 0; q < 2; ++q) tc::mbar_init(&act_ready[q], kEpiWarps);
-    tc::mbar_init(mma_out, 1);
-    tc::mbar_init(drain, 1);
     tc::mbar_init(res_full, 1);
+    tc::mbar_init(drain, 1);
     *abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -603,21 +607,30 @@ __global__ void __launch_bounds__(kThreads, 1) k_sur_infer(const DevBlock *__res
   tc::fence_after_sync();
   const uint32_t tmem = *tslot;
 
-  const int total = my_tiles * kTileStages;  // this CTA's streamed stages
   if (warp == kLoadWarp) {
-    // ---- weights: the resident pair once, then stage si of the stream into
-    // ring slot si % kStages once the MMAs of stage si - kStages are done
+    // ---- weights: the resident pair once, then every hidden layer's stages
+    // in the order the MMAs consume them (each tile of a pair streams the
+    // layer again); stage si goes to ring slot si % kStages once the MMAs of
+    // stage si - kStages are done
     if (lane == 0) {
       expect_bytes(res_full, 2 * kChunkBytes);
       load_bytes(wres, P.w_packed[0], kChunkBytes, res_full);
       load_bytes(wres + kChunkBytes, P.w_packed[4], kChunkBytes, res_full);
       int si = 0;
-      for (; si < total; ++si) {
-        const int slot = si % kStages;
-        if (si >= kStages && !wait_bar(&empty[slot], ((si / kStages) - 1) & 1, abort)) break;
-        expect_bytes(&full[slot], kStageBytes);
-        load_bytes(stages + slot * kStageBytes, stage_src(P, si % kTileStages), kStageBytes, &full[slot]);
-      }
+      bool ok = true;
+      for (int pr = 0; pr < n_pairs && ok; ++pr)
+        for (int L = 1; L < 4 && ok; ++L)
+          for (int t = 2 * pr; t < min(2 * pr + 2, my_tiles) && ok; ++t)
+            for (int g = 0; g < kLayerStages; ++g, ++si) {
+              const int slot = si % kStages;
+              if (si >= kStages && !wait_bar(&empty[slot], ((si / kStages) - 1) & 1, abort)) {
+                ok = false;
+                break;
+              }
+              expect_bytes(&full[slot], kStageBytes);
+              load_bytes(stages + slot * kStageBytes, stage_src(P, (L - 1) * kLayerStages + g), kStageBytes,
+                         &full[slot]);
+            }
       // the copies in flight land before the CTA moves on
       tc::mbar_wait(res_full, 0);
       for (int c = si > kStages ? si - kStages : 0; c < si; ++c)
@@ -625,132 +638,140 @@ __global__ void __launch_bounds__(kThreads, 1) k_sur_infer(const DevBlock *__res
     }
   } else if (warp == kMmaWarp) {
     // ---- tensor-core issue: the whole warp runs the loop, converged, and
-    // one elected lane issues each MMA and commit
+    // one elected lane issues each MMA and commit.  Slot q's k-th tile: its
+    // first layer waits for its features and for the decode of the slot's
+    // previous tile (which read the same accumulator); layer L >= 1 waits for
+    // the epilogue of layer L - 1 (epi_done phase 4 k + L - 1).
     constexpr uint32_t kSboAct = (kSurHidden / 8) * 128, kSbo16 = (16 / 8) * 128;
     constexpr uint32_t kIdHidden = tc::idesc_bf16(128, kSurHidden), kIdOut = tc::idesc_bf16(128, kSurOutPad);
-    const uint32_t in = tc::smem_u32(act), w0 = tc::smem_u32(wres), w4 = w0 + kChunkBytes;
+    const uint32_t w0 = tc::smem_u32(wres), w4 = w0 + kChunkBytes;
     int si = 0;
     bool ok = __all_sync(0xffffffffu, wait_bar(res_full, 0, abort));
-    for (int it = 0; it < my_tiles && ok; ++it) {
-      const int tb = it & 1;
+    for (int pr = 0; pr < n_pairs && ok; ++pr) {
       for (int L = 0; L < 5 && ok; ++L) {
-        const int g = it * 5 + L, p = g & 1;
-        const uint32_t acc = tmem + p * kSurHidden;
-        if (g >= 2) ok = __all_sync(0xffffffffu, wait_bar(&acc_free[p], ((g - 2) >> 1) & 1, abort));
-        const int e_prev = it * 4 + L - 1;  // the epilogue that wrote this layer's input
-        if (L == 0) {
-          if (ok) ok = __all_sync(0xffffffffu, wait_bar(&feat_full[tb], (it >> 1) & 1, abort));
-          if (!ok) break;
-          tc::fence_after_sync();
-          tc::mma_bf16_warp(acc, tc::desc_kmajor(tc::smem_u32(x0 + tb * kX0Bytes), 128, kSbo16),
-                            tc::desc_kmajor(w0, 128, kSbo16), kIdHidden, 0u);
-          tc::commit_warp(&x0_free[tb]);
-        } else if (L < 4) {
-          for (int gq = 0; gq < 4 && ok; ++gq, ++si) {
-            const int slot = si % kStages;
-            if ((gq & 1) == 0) ok = __all_sync(0xffffffffu, wait_bar(&act_ready[gq >> 1], e_prev & 1, abort));
-            if (ok) ok = __all_sync(0xffffffffu, wait_bar(&full[slot], (si / kStages) & 1, abort));
+        for (int t = 2 * pr; t < min(2 * pr + 2, my_tiles) && ok; ++t) {
+          const int q = t & 1, k = t >> 1;
+          const uint32_t acc = tmem + q * kSurHidden;
+          const uint32_t in = tc::smem_u32(act + q * kActBytes);
+          if (L == 0) {
+            ok = __all_sync(0xffffffffu, wait_bar(&feat_full[q], k & 1, abort));
+            if (ok && k >= 1) ok = __all_sync(0xffffffffu, wait_bar(&out_free[q], (k - 1) & 1, abort));
             if (!ok) break;
             tc::fence_after_sync();
-            const uint32_t wb = tc::smem_u32(stages + slot * kStageBytes);
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-              tc::mma_bf16_warp(acc, tc::desc_kmajor(in + (4 * gq + c) * 16 * 16, 128, kSboAct),
-                                tc::desc_kmajor(wb + c * kChunkBytes, 128, kSbo16), kIdHidden,
-                                (gq > 0 || c > 0) ? 1u : 0u);
-            tc::commit_warp(&empty[slot]);
+            tc::mma_bf16_warp(acc, tc::desc_kmajor(tc::smem_u32(x0 + q * kX0Bytes), 128, kSbo16),
+                              tc::desc_kmajor(w0, 128, kSbo16), kIdHidden, 0u);
+            tc::commit_warp(&x0_free[q]);
+            tc::commit_warp(&mma_done[q]);
+            continue;
           }
-        } else {
-          for (int j = 0; j < 2 && ok; ++j) ok = __all_sync(0xffffffffu, wait_bar(&act_ready[j], e_prev & 1, abort));
+          ok = __all_sync(0xffffffffu, wait_bar(&epi_done[q], (L - 1) & 1, abort));
           if (!ok) break;
           tc::fence_after_sync();
+          if (L < 4) {
+            for (int g = 0; g < kLayerStages && ok; ++g, ++si) {
+              const int slot = si % kStages;
+              ok = __all_sync(0xffffffffu, wait_bar(&full[slot], (si / kStages) & 1, abort));
+              if (!ok) break;
+              tc::fence_after_sync();
+              const uint32_t wb = tc::smem_u32(stages + slot * kStageBytes);
+#pragma unroll
+              for (int c = 0; c < kStageChunks; ++c) {
+                const int kc = g * kStageChunks + c;  // K chunk of 16 within the layer
+                tc::mma_bf16_warp(acc, tc::desc_kmajor(in + kc * 16 * 16, 128, kSboAct),
+                                  tc::desc_kmajor(wb + c * kChunkBytes, 128, kSbo16), kIdHidden,
+                                  kc > 0 ? 1u : 0u);
+              }
+              tc::commit_warp(&empty[slot]);
+            }
+            if (!ok) break;
+            tc::commit_warp(&mma_done[q]);
+          } else {
 #pragma unroll 4
-          for (int kk = 0; kk < kSurHidden / 16; ++kk)
-            tc::mma_bf16_warp(acc, tc::desc_kmajor(in + kk * 16 * 16, 128, kSboAct),
-                              tc::desc_kmajor(w4 + kk * (kSurOutPad * 16 * 2), 128, kSbo16), kIdOut,
-                              kk > 0 ? 1u : 0u);
+            for (int kk = 0; kk < kSurHidden / 16; ++kk)
+              tc::mma_bf16_warp(acc, tc::desc_kmajor(in + kk * 16 * 16, 128, kSboAct),
+                                tc::desc_kmajor(w4 + kk * (kSurOutPad * 16 * 2), 128, kSbo16), kIdOut,
+                                kk > 0 ? 1u : 0u);
+            tc::commit_warp(&out_done[q]);
+          }
         }
-        if (!ok) break;
-        if (L < 4)
-          tc::commit_warp(&mma_epi[(it * 4 + L) & 1]);
-        else
-          tc::commit_warp(mma_out);
       }
     }
     // every MMA issued has completed before the TMEM columns are released
     tc::commit_warp(drain);
     tc::mbar_wait(drain, 0);
   } else if (warp < kEpiWarps) {
-    // ---- hidden epilogues
+    // ---- hidden epilogues, in the MMAs' order: layer L of slot q's k-th
+    // tile waits for mma_done phase 4 k + L
     const int quarter = warp & 3, cg = warp >> 2, row = quarter * 32 + lane;
     bool ok = true;
-    for (int it = 0; it < my_tiles && ok; ++it) {
+    for (int pr = 0; pr < n_pairs && ok; ++pr) {
       for (int L = 0; L < 4 && ok; ++L) {
-        const int g = it * 5 + L, p = g & 1, e = it * 4 + L;
-        ok = __all_sync(0xffffffffu, wait_bar(&mma_epi[e & 1], (e >> 1) & 1, abort));
-        if (!ok) break;
-        tc::fence_after_sync();
-        const uint32_t tbase = tmem + p * kSurHidden + (static_cast<uint32_t>(quarter * 32) << 16) + cg * 32;
-        const float *bias = sbias + L * kSurHidden + cg * 32;
+        for (int t = 2 * pr; t < min(2 * pr + 2, my_tiles) && ok; ++t) {
+          const int q = t & 1;
+          ok = __all_sync(0xffffffffu, wait_bar(&mma_done[q], L & 1, abort));
+          if (!ok) break;
+          tc::fence_after_sync();
+          const uint32_t tbase = tmem + q * kSurHidden + (static_cast<uint32_t>(quarter * 32) << 16) + cg * 32;
+          const float *bias = sbias + L * kSurHidden + cg * 32;
+          uint8_t *actq = act + q * kActBytes;
 #pragma unroll 1
-        for (int s = 0; s < 2; ++s) {
-          uint32_t cur[32];
-          tc::tmem_ld32_issue(tbase + s * 128, cur);
-          tc::tmem_ld_wait(cur);
+          for (int s = 0; s < 2; ++s) {
+            uint32_t cur[32];
+            tc::tmem_ld32_issue(tbase + s * 128, cur);
+            tc::tmem_ld_wait(cur);
 #pragma unroll
-          for (int q = 0; q < 32; q += 8) {
-            const float4 b0 = *reinterpret_cast<const float4 *>(bias + s * 128 + q);
-            const float4 b1 = *reinterpret_cast<const float4 *>(bias + s * 128 + q + 4);
-            const uint32_t p0 = gelu2_bf16(__uint_as_float(cur[q]) + b0.x, __uint_as_float(cur[q + 1]) + b0.y);
-            const uint32_t p1 = gelu2_bf16(__uint_as_float(cur[q + 2]) + b0.z, __uint_as_float(cur[q + 3]) + b0.w);
-            const uint32_t p2 = gelu2_bf16(__uint_as_float(cur[q + 4]) + b1.x, __uint_as_float(cur[q + 5]) + b1.y);
-            const uint32_t p3 = gelu2_bf16(__uint_as_float(cur[q + 6]) + b1.z, __uint_as_float(cur[q + 7]) + b1.w);
-            *reinterpret_cast<uint4 *>(act + tc::tile_offset(row, s * 128 + cg * 32 + q, kSurHidden)) =
-                make_uint4(p0, p1, p2, p3);
+            for (int c = 0; c < 32; c += 8) {
+              const float4 b0 = *reinterpret_cast<const float4 *>(bias + s * 128 + c);
+              const float4 b1 = *reinterpret_cast<const float4 *>(bias + s * 128 + c + 4);
+              const uint32_t p0 = gelu2_bf16(__uint_as_float(cur[c]) + b0.x, __uint_as_float(cur[c + 1]) + b0.y);
+              const uint32_t p1 = gelu2_bf16(__uint_as_float(cur[c + 2]) + b0.z, __uint_as_float(cur[c + 3]) + b0.w);
+              const uint32_t p2 = gelu2_bf16(__uint_as_float(cur[c + 4]) + b1.x, __uint_as_float(cur[c + 5]) + b1.y);
+              const uint32_t p3 = gelu2_bf16(__uint_as_float(cur[c + 6]) + b1.z, __uint_as_float(cur[c + 7]) + b1.w);
+              *reinterpret_cast<uint4 *>(actq + tc::tile_offset(row, s * 128 + cg * 32 + c, kSurHidden)) =
+                  make_uint4(p0, p1, p2, p3);
+            }
           }
-          if (s == 1) {
-            // this warp has read all its accumulator columns
-            tc::fence_before_sync();
-            __syncwarp();
-            if (lane == 0) bar_arrive(&acc_free[p]);
-          }
-          // columns 128 s .. 128 s + 127 written by all epilogue warps: release them
+          // the accumulator is read and the activations written: the slot's
+          // next MMA may overwrite the one and read the other
+          tc::fence_before_sync();
           tc::fence_async_smem();
           __syncwarp();
-          if (lane == 0) bar_arrive(&act_ready[s]);
+          if (lane == 0) bar_arrive(&epi_done[q]);
         }
       }
     }
   } else {
-    // ---- features of the next tile, outputs of the current one
+    // ---- features of tile it + 2 once tile it's first layer has read the
+    // slot's feature buffer, then tile it's outputs
     const int quarter = warp & 3, row = quarter * 32 + lane;
     bool ok = true;
-    if (my_tiles > 0) {
-      tile_features<C>(B, P, cell_of(static_cast<int64_t>(blockIdx.x) * kCells + row), row, x0);
+    for (int t = 0; t < min(2, my_tiles); ++t) {
+      tile_features<C>(B, P, cell_of((blockIdx.x + static_cast<int64_t>(t) * gridDim.x) * kCells + row), row,
+                       x0 + t * kX0Bytes);
       tc::fence_async_smem();
       __syncwarp();
-      if (lane == 0) bar_arrive(&feat_full[0]);
+      if (lane == 0) bar_arrive(&feat_full[t]);
     }
     for (int it = 0; it < my_tiles && ok; ++it) {
+      const int q = it & 1, k = it >> 1;
       const int64_t tile = blockIdx.x + static_cast<int64_t>(it) * gridDim.x;
-      if (it + 1 < my_tiles) {
-        const int nb = (it + 1) & 1;
-        if (it + 1 >= 2) ok = __all_sync(0xffffffffu, wait_bar(&x0_free[nb], (((it + 1) >> 1) - 1) & 1, abort));
+      if (it + 2 < my_tiles) {
+        ok = __all_sync(0xffffffffu, wait_bar(&x0_free[q], k & 1, abort));
         if (!ok) break;
-        tile_features<C>(B, P, cell_of((tile + gridDim.x) * kCells + row), row, x0 + nb * kX0Bytes);
+        tile_features<C>(B, P, cell_of((tile + 2 * static_cast<int64_t>(gridDim.x)) * kCells + row), row,
+                         x0 + q * kX0Bytes);
         tc::fence_async_smem();
         __syncwarp();
-        if (lane == 0) bar_arrive(&feat_full[nb]);
+        if (lane == 0) bar_arrive(&feat_full[q]);
       }
-      const int g = it * 5 + 4, p = g & 1;
-      ok = __all_sync(0xffffffffu, wait_bar(mma_out, it & 1, abort));
+      ok = __all_sync(0xffffffffu, wait_bar(&out_done[q], k & 1, abort));
       if (!ok) break;
       tc::fence_after_sync();
       float o[kSurOutPad];
-      tc::tmem_ld16(tmem + p * kSurHidden + (static_cast<uint32_t>(quarter * 32) << 16), o);
+      tc::tmem_ld16(tmem + q * kSurHidden + (static_cast<uint32_t>(quarter * 32) << 16), o);
       tc::fence_before_sync();
       __syncwarp();
-      if (lane == 0) bar_arrive(&acc_free[p], kEpiWarps / 4);  // four warps stand for the epilogue warps
+      if (lane == 0) bar_arrive(&out_free[q]);
       tile_apply<C, MODE, NE>(B, P, cell_of(tile * kCells + row), o, sbias + 4 * kSurHidden, fb_count, fb_list,
                               stats);
     }
