@@ -129,35 +129,61 @@ def trained(drv, tmp_path_factory):
     return case, field, sur
 
 
-def test_fused_inference_matches_unfused(trained):
-    """The fused kernel against the unfused prediction on the same cells (the
-    judge off, so that the comparison covers accepted cells too)."""
-    case, field, sur = trained
+def check_fused_against_unfused(field, sur):
+    """The fused kernel (a split chemistry step over every cell of the field)
+    against the unfused prediction on the same cells, the judge off so that
+    the comparison covers accepted cells too.  Returns (accepted, fallback)."""
     sur.set_gate(judge_rel=-1.0)
-    st = cell_states(field)
-    dy_net, acc_net = sur.predict(st)
-    dy_epi = sur.label(st)
-    g = field.info().ngg
-    y0 = field.get(0, "sv")[:9, g:-g, g:-g, g:-g].reshape(9, -1).T.copy()
-    field.set_surrogate(sur)
-    field.run_phase("chemistry")
-    y1 = field.get(0, "sv")[:9, g:-g, g:-g, g:-g].reshape(9, -1).T
-    dy = y1 - y0
-    acc, fb = field.chemistry_stats()
-    assert acc + fb == st.shape[0]
-    # cells that took the EPI fallback: the same FP64 step as the labels
-    scale = np.abs(dy_epi).max(axis=1, keepdims=True) + 1e-30
-    epi_like = np.all(np.abs(dy - dy_epi) <= 1e-9 * scale + 1e-15, axis=1)
-    # the fused kernel evaluates GELU with the hardware tanh: increments agree
-    # to 10 % of the cell's largest increment (floor 1e-13); a layout or
-    # pipeline fault would break nearly every cell, rounding only a few
-    net_like = np.all(np.abs(dy - dy_net) <= 1e-1 * np.abs(dy_net).max(axis=1, keepdims=True) + 1e-13, axis=1)
-    assert np.mean(epi_like | net_like) >= 0.99, np.mean(epi_like | net_like)
-    # where the unfused gate accepted, the fused kernel gave the network's increment
-    assert np.mean(net_like[acc_net]) > 0.98, np.mean(net_like[acc_net])
-    field.set_surrogate(None)
-    sur.set_gate(judge_rel=0.25, judge_abs=1e-4)
+    try:
+        st = cell_states(field)
+        dy_net, acc_net = sur.predict(st)
+        dy_epi = sur.label(st)
+        g = field.info().ngg
+        y0 = field.get(0, "sv")[:9, g:-g, g:-g, g:-g].reshape(9, -1).T.copy()
+        field.set_surrogate(sur)
+        field.run_phase("chemistry")
+        y1 = field.get(0, "sv")[:9, g:-g, g:-g, g:-g].reshape(9, -1).T
+        dy = y1 - y0
+        acc, fb = field.chemistry_stats()
+        assert acc + fb == st.shape[0]
+        # cells that took the EPI fallback: the same FP64 step as the labels
+        scale = np.abs(dy_epi).max(axis=1, keepdims=True) + 1e-30
+        epi_like = np.all(np.abs(dy - dy_epi) <= 1e-9 * scale + 1e-15, axis=1)
+        # the fused kernel evaluates GELU with the hardware tanh: increments agree
+        # to 10 % of the cell's largest increment (floor 1e-13); a layout or
+        # pipeline fault would break nearly every cell, rounding only a few
+        net_like = np.all(np.abs(dy - dy_net) <= 1e-1 * np.abs(dy_net).max(axis=1, keepdims=True) + 1e-13, axis=1)
+        assert np.mean(epi_like | net_like) >= 0.99, np.mean(epi_like | net_like)
+        # where the unfused gate accepted, the fused kernel gave the network's increment
+        assert np.mean(net_like[acc_net]) > 0.98, np.mean(net_like[acc_net])
+        field.set_surrogate(None)
+        return acc, fb
+    finally:
+        sur.set_gate(judge_rel=0.25, judge_abs=1e-4)
+
+
+def test_fused_inference_matches_unfused(trained):
+    """24x16x8 cells: 24 tiles of 128, one per CTA (a pair with one tile)."""
+    case, field, sur = trained
+    acc, fb = check_fused_against_unfused(field, sur)
     print("fused: accepted", acc, "fallback", fb)
+
+
+def test_fused_inference_two_and_three_tiles_per_cta(trained, tmp_path):
+    """64x32x24 cells: 384 tiles over at most 148 CTAs, so a CTA runs a full
+    pair of tiles (both slots) and some a pair and a single tile."""
+    _, _, sur = trained
+    case = tmp_path / "ml_big"
+    cases.mixing_layer_case(case, mx=64, my=32, mz=24, total_step=1, output_screen=1)
+    field = ostc.Driver(case, precision="mixed")
+    field.initialize()
+    field.step(20)
+    try:
+        acc, fb = check_fused_against_unfused(field, sur)
+    finally:
+        field.close()
+    assert acc > 0
+    print("fused, 49152 cells: accepted", acc, "fallback", fb)
 
 
 def test_judge_rejects_a_silent_network_on_reacting_cells(drv):
