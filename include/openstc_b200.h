@@ -174,6 +174,20 @@ int ostc_driver_simulate(ostc_driver *d);
 /* n iterations of the steady loop body, no file output.  *err_max receives
    the last normalised residual (or -1 if none was due). */
 int ostc_driver_step(ostc_driver *d, int n_steps, double *err_max);
+/* No counterpart in the reference, whose loop keeps the state on the device:
+   a host-driven stepping loop.  n_steps iterations of ostc_driver_step, each
+   preceded by the upload of n_fields fields (ostc_field_id) of block `block`
+   from host[k] (counts[k] doubles, the ostc_driver_get_field layout) and
+   followed by their download into the same buffers, so that the host holds
+   each step's result and supplies the next step's input.  The copies run in
+   chunks of chunk_bytes (0: 16 MiB) on two copy streams of their own: the
+   upload of a chunk waits only for the download of the same chunk, so one
+   step's download and the next step's upload overlap.  Page-locked host
+   buffers let the copies run asynchronously.  Only whole state fields
+   (bv, sv, cv and the like); the geometry goes through
+   ostc_driver_set_field.  *err_max as for ostc_driver_step. */
+int ostc_driver_step_io(ostc_driver *d, int n_steps, int block, const int *fields, double *const *host,
+                        const int64_t *counts, int n_fields, int64_t chunk_bytes, double *err_max);
 /* Normalised residuals of rho, |V|, p, T from the last residual step. */
 int ostc_driver_residual(const ostc_driver *d, double res[4]);
 int ostc_driver_run_phase(ostc_driver *d, int phase);

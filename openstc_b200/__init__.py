@@ -132,6 +132,8 @@ def library() -> C.CDLL:
         "ostc_driver_initialize": ([P], C.c_int),
         "ostc_driver_simulate": ([P], C.c_int),
         "ostc_driver_step": ([P, C.c_int, D], C.c_int),
+        "ostc_driver_step_io": ([P, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_void_p), C.POINTER(C.c_int64),
+                                 C.c_int, C.c_int64, D], C.c_int),
         "ostc_driver_residual": ([P, D], C.c_int),
         "ostc_driver_residual_noalloc": ([P, D], C.c_int),
         "ostc_driver_autotune": ([P, C.c_int, C.POINTER(Tuning)], C.c_int),
@@ -287,6 +289,26 @@ class Driver:
     def step(self, n: int = 1) -> float:
         err = C.c_double(-1.0)
         _check(library().ostc_driver_step(self._h, n, C.byref(err)))
+        return err.value
+
+    def step_io(self, n: int, block: int, fields: list[str], arrays: list[np.ndarray], chunk_bytes: int = 0) -> float:
+        """A host-driven stepping loop (ostc_driver_step_io): n steps, each
+        preceded by the upload of the named fields of `block` from `arrays`
+        (float64, C-contiguous, the get_field layout) and followed by their
+        download into the same arrays.  The copies of one step's download and
+        the next step's upload overlap chunk by chunk; page-locked arrays
+        (e.g. from torch's pin_memory) make them asynchronous."""
+        nf = len(fields)
+        if len(arrays) != nf:
+            raise OstcError("one array per field")
+        for a in arrays:
+            if a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise OstcError("arrays must be C-contiguous float64")
+        ids = (C.c_int * nf)(*[FIELD_ID[f] for f in fields])
+        ptrs = (C.c_void_p * nf)(*[a.ctypes.data for a in arrays])
+        counts = (C.c_int64 * nf)(*[a.size for a in arrays])
+        err = C.c_double(-1.0)
+        _check(library().ostc_driver_step_io(self._h, n, block, ids, ptrs, counts, nf, chunk_bytes, C.byref(err)))
         return err.value
 
     def residual(self) -> np.ndarray:

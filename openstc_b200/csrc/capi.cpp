@@ -260,6 +260,32 @@ int ostc_driver_step(ostc_driver *d, int n_steps, double *err_max) {
   });
 }
 
+int ostc_driver_step_io(ostc_driver *d, int n_steps, int block, const int *fields, double *const *host,
+                        const int64_t *counts, int n_fields, int64_t chunk_bytes, double *err_max) {
+  if (!d || n_steps < 0 || n_fields < 0 || (n_fields > 0 && (!fields || !host || !counts)) || chunk_bytes < 0)
+    return fail(OSTC_ERR_INPUT, "bad argument");
+  if (!d->drv.initialized()) return fail(OSTC_ERR_STATE, "initialize first");
+  return guarded([&] {
+    ostc::Engine &E = d->drv.engine();
+    if (block < 0 || block >= static_cast<int>(E.blocks().size())) return fail(OSTC_ERR_INPUT, "block index");
+    std::vector<int> f(fields, fields + n_fields);
+    std::vector<double *> h(host, host + n_fields);
+    for (int k = 0; k < n_fields; ++k) {
+      if (f[k] < 0 || f[k] >= OSTC_N_FIELDS) return fail(OSTC_ERR_INPUT, "field id");
+      if (f[k] == ostc::F_X || f[k] == ostc::F_Y || f[k] == ostc::F_Z || f[k] == ostc::F_JAC ||
+          f[k] == ostc::F_METRIC || f[k] == ostc::F_WALL_DIST)
+        return fail(OSTC_ERR_INPUT, "the geometry is set with ostc_driver_set_field");
+      if (!h[k]) return fail(OSTC_ERR_INPUT, "null host buffer");
+      const int64_t n = E.field_count(block, f[k]);
+      if (n == 0) return fail(OSTC_ERR_INPUT, "field not allocated in this configuration");
+      if (counts[k] != n) return fail(OSTC_ERR_INPUT, "host buffer size does not match the field");
+    }
+    const double e = d->drv.step_io(n_steps, block, f, h, chunk_bytes > 0 ? chunk_bytes : (int64_t(16) << 20));
+    if (err_max) *err_max = e;
+    return static_cast<int>(OSTC_OK);
+  });
+}
+
 int ostc_driver_residual(const ostc_driver *d, double res[4]) {
   if (!d || !res) return fail(OSTC_ERR_INPUT, "null argument");
   for (int l = 0; l < 4; ++l) res[l] = d->drv.res[l];

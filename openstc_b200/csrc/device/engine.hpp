@@ -114,6 +114,19 @@ class Engine {
   // alone (source, flux, implicit increments), eagerly launched `reps`
   // times after one untimed pass; the state is not advanced.
   virtual double time_stages(int reps) = 0;
+
+  // Host-driven stepping loop (Driver::step_io): whole fields of block b
+  // copied in chunks of chunk_bytes on two copy streams of their own.
+  // upload_chunked: every chunk waits for the previous download of the same
+  // chunk (none before the first), then the engine stream waits for all of
+  // them; download_chunked: after everything enqueued on the engine stream,
+  // one event per chunk.  Field k of a call is matched with field k of the
+  // previous call.  sync_copies waits for both copy streams.
+  virtual void upload_chunked(int b, const int *fields, const double *const *host, int n_fields,
+                              int64_t chunk_bytes) = 0;
+  virtual void download_chunked(int b, const int *fields, double *const *host, int n_fields,
+                                int64_t chunk_bytes) = 0;
+  virtual void sync_copies() = 0;
 };
 
 // Largest grid ostc_driver_residual_noalloc accepts, in residual tiles

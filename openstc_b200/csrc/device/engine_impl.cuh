@@ -141,7 +141,79 @@ class EngineT final : public Engine {
     cudaEventDestroy(ev1_);
     for (auto e : out_ev_) cudaEventDestroy(e);
     cudaFree(d_wall2d_);
+    for (auto e : chunk_ev_) cudaEventDestroy(e);
+    if (ev_copy_) cudaEventDestroy(ev_copy_);
+    if (cin_) cudaStreamDestroy(cin_);
+    if (cout_) cudaStreamDestroy(cout_);
     cudaStreamDestroy(stream_);
+  }
+
+  // ---- chunked host transfers of the host-driven stepping loop
+  void copy_streams() {
+    if (cin_) return;
+    cuda_check(cudaStreamCreateWithFlags(&cin_, cudaStreamNonBlocking), "copy stream");
+    cuda_check(cudaStreamCreateWithFlags(&cout_, cudaStreamNonBlocking), "copy stream");
+    cuda_check(cudaEventCreateWithFlags(&ev_copy_, cudaEventDisableTiming), "copy event");
+  }
+
+  // the event of chunk c of the k-th field of a call (created on first use)
+  cudaEvent_t chunk_event(int k, int64_t c) {
+    const size_t slot = static_cast<size_t>(k) * kMaxChunks + static_cast<size_t>(c);
+    if (chunk_ev_.size() <= slot) chunk_ev_.resize(slot + 1, nullptr);
+    if (!chunk_ev_[slot]) cuda_check(cudaEventCreateWithFlags(&chunk_ev_[slot], cudaEventDisableTiming), "chunk event");
+    return chunk_ev_[slot];
+  }
+
+  static int64_t chunk_doubles(int64_t count, int64_t chunk_bytes) {
+    const int64_t per = std::max<int64_t>(1, chunk_bytes / static_cast<int64_t>(sizeof(double)));
+    return std::max<int64_t>(per, (count + kMaxChunks - 1) / kMaxChunks);  // at most kMaxChunks chunks
+  }
+
+  void upload_chunked(int b, const int *fields, const double *const *host, int n_fields,
+                      int64_t chunk_bytes) override {
+    copy_streams();
+    upload_params();
+    // nothing enqueued on the engine stream so far still reads these arrays
+    cuda_check(cudaEventRecord(ev_copy_, stream_), "copy event");
+    cuda_check(cudaStreamWaitEvent(cin_, ev_copy_, 0), "copy wait");
+    for (int k = 0; k < n_fields; ++k) {
+      double *dev = field_ptr(b, fields[k]);
+      const int64_t count = field_count(b, fields[k]);
+      const int64_t per = chunk_doubles(count, chunk_bytes);
+      for (int64_t c = 0, off = 0; off < count; ++c, off += per) {
+        const int64_t n = std::min(per, count - off);
+        if (downloaded_) cuda_check(cudaStreamWaitEvent(cin_, chunk_event(k, c), 0), "chunk wait");
+        cuda_check(cudaMemcpyAsync(dev + off, host[k] + off, sizeof(double) * n, cudaMemcpyHostToDevice, cin_),
+                   "chunk upload");
+      }
+    }
+    cuda_check(cudaEventRecord(ev_copy_, cin_), "copy event");
+    cuda_check(cudaStreamWaitEvent(stream_, ev_copy_, 0), "copy wait");
+  }
+
+  void download_chunked(int b, const int *fields, double *const *host, int n_fields, int64_t chunk_bytes) override {
+    copy_streams();
+    cuda_check(cudaEventRecord(ev_copy_, stream_), "copy event");
+    cuda_check(cudaStreamWaitEvent(cout_, ev_copy_, 0), "copy wait");
+    for (int k = 0; k < n_fields; ++k) {
+      const double *dev = field_ptr(b, fields[k]);
+      const int64_t count = field_count(b, fields[k]);
+      const int64_t per = chunk_doubles(count, chunk_bytes);
+      for (int64_t c = 0, off = 0; off < count; ++c, off += per) {
+        const int64_t n = std::min(per, count - off);
+        cuda_check(cudaMemcpyAsync(host[k] + off, dev + off, sizeof(double) * n, cudaMemcpyDeviceToHost, cout_),
+                   "chunk download");
+        cuda_check(cudaEventRecord(chunk_event(k, c), cout_), "chunk event");
+      }
+    }
+    downloaded_ = true;
+  }
+
+  void sync_copies() override {
+    if (!cin_) return;
+    cuda_check(cudaStreamSynchronize(cout_), "copy sync");
+    cuda_check(cudaStreamSynchronize(cin_), "copy sync");
+    downloaded_ = false;
   }
 
   void set_field(int b, int field, const double *host, int64_t count) override {
@@ -1055,6 +1127,12 @@ class EngineT final : public Engine {
   std::vector<double *> rate_store_;
   cudaEvent_t ev0_{}, ev1_{};
   cudaEvent_t out_ev_[2]{};  // output pipeline slots
+  // chunked host transfers (upload_chunked / download_chunked)
+  static constexpr int64_t kMaxChunks = 64;  // per field
+  cudaStream_t cin_{}, cout_{};
+  cudaEvent_t ev_copy_{};
+  std::vector<cudaEvent_t> chunk_ev_;
+  bool downloaded_ = false;  // chunk events recorded since the last sync_copies
   double *d_wall2d_ = nullptr;  // cf and qw of the 2-D wall post-processing
   int wall_cap_ = 0;
   double last_ms_ = 0;

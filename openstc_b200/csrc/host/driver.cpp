@@ -512,6 +512,29 @@ double Driver::advance(int n) {
   return err;
 }
 
+double Driver::step_io(int n, int block, const std::vector<int> &fields, const std::vector<double *> &host,
+                       int64_t chunk_bytes) {
+  Engine &E = engine();
+  const int screen = parameter.get_int("output_screen");
+  const int nf = static_cast<int>(fields.size());
+  double err = -1;
+  for (int q = 0; q < n; ++q) {
+    E.upload_chunked(block, fields.data(), host.data(), nf, chunk_bytes);
+    ++step;
+    const bool store = step % screen == 0;
+    const bool due = store || step == 1;
+    double raw[4] = {0, 0, 0, 0};
+    last_step_residual = false;
+    E.step(store, due, raw);
+    if (due) err = compute_residual(step, raw);
+    last_step_residual = due;
+    E.download_chunked(block, fields.data(), host.data(), nf, chunk_bytes);
+  }
+  E.sync_copies();
+  E.synchronize();
+  return err;
+}
+
 void Driver::simulate() {
   if (!parameter.get_bool("steady")) throw ParameterError("Not implemented: only steady simulations are supported");
   Engine &E = engine();

@@ -42,6 +42,10 @@ class Driver {
   // Advances n loop iterations (residual cadence of the reference, no file
   // output).  Returns the last err_max or -1 when no residual was due.
   double advance(int n);
+  // advance(n) with each step's fields uploaded before it and downloaded
+  // after it (Engine::upload_chunked / download_chunked)
+  double step_io(int n, int block, const std::vector<int> &fields, const std::vector<double *> &host,
+                 int64_t chunk_bytes);
 
   void write_field(const std::string &path);
 
