@@ -322,12 +322,14 @@ __global__ void k_adam(float *p, const float *g, float *m, float *v, int64_t n, 
 // bf16 copies of a weight [dout x din]: row-major, transposed, and in the
 // tile order of the fused inference kernel (K chunks of 16 columns).
 __global__ void k_pack(const float *w, int dout, int din, uint16_t *wb, uint16_t *wbt, uint8_t *wp) {
+  // wp null: the training GEMMs' copies only
   const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
   if (i >= static_cast<int64_t>(dout) * din) return;
   const int r = static_cast<int>(i / din), k = static_cast<int>(i % din);
   const uint16_t v = bf16(w[i]);
   wb[i] = v;
   wbt[static_cast<int64_t>(k) * dout + r] = v;
+  if (!wp) return;
   const int bk = 16;
   const int c = k / bk, kk = k % bk;
   *reinterpret_cast<uint16_t *>(wp + static_cast<size_t>(c) * dout * bk * 2 + tc::tile_offset(r, kk, bk)) = v;
@@ -590,28 +592,34 @@ double Surrogate::train(int steps, int batch, double lr, int64_t n_train, float 
   if (n_train <= 0 || n_train > n_) n_train = n_;
   ck(cudaSetDevice(device_), "cudaSetDevice");
   ensure_batch(batch);
-  double last = 0;
+  // each step's loss stays on the device until the end: no host
+  // synchronisation between steps
+  double *dloss = nullptr;
+  ck(cudaMalloc(&dloss, sizeof(double) * std::max(1, steps)), "cudaMalloc losses");
   for (int s = 0; s < steps; ++s) {
     k_gather<<<(batch + 255) / 256, 256, 0, stream_>>>(x_, t_, n_train, mix64(seed_ + 0x5151 * (adam_t_ + 1)), batch,
                                                        a_[0], at_[0], tb_);
     forward(batch);
     const double cosine = 0.5 * (1 + std::cos(3.141592653589793 * s / std::max(1, steps)));
-    double loss_host = 0;
-    {
-      // schedule: cosine decay to 5 % of lr
-      const double lr_s = lr * (0.05 + 0.95 * cosine);
-      backward_and_step(batch, lr_s, s);
-      ck(cudaMemcpyAsync(&loss_host, loss_, sizeof(double), cudaMemcpyDeviceToHost, stream_), "loss copy");
-    }
-    // new bf16 weights for the next step
+    // schedule: cosine decay to 5 % of lr
+    const double lr_s = lr * (0.05 + 0.95 * cosine);
+    backward_and_step(batch, lr_s, s);
+    ck(cudaMemcpyAsync(dloss + s, loss_, sizeof(double), cudaMemcpyDeviceToDevice, stream_), "loss copy");
+    // new bf16 weights for the next step's GEMMs (the inference copy once, below)
     for (int l = 0; l < kSurLayers; ++l) {
       const int64_t nw = static_cast<int64_t>(dout_[l]) * din_[l];
-      k_pack<<<(nw + 255) / 256, 256, 0, stream_>>>(w_[l], dout_[l], din_[l], wb_[l], wbt_[l], wpack_[l]);
+      k_pack<<<(nw + 255) / 256, 256, 0, stream_>>>(w_[l], dout_[l], din_[l], wb_[l], wbt_[l], nullptr);
     }
-    ck(cudaStreamSynchronize(stream_), "train step");
-    last = loss_host;
-    if (losses) losses[s] = static_cast<float>(loss_host);
   }
+  pack();
+  std::vector<double> hl(static_cast<size_t>(std::max(1, steps)), 0.0);
+  cudaError_t st = cudaMemcpyAsync(hl.data(), dloss, sizeof(double) * hl.size(), cudaMemcpyDeviceToHost, stream_);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(stream_);
+  cudaFree(dloss);
+  ck(st, "train steps");
+  if (losses)
+    for (int s = 0; s < steps; ++s) losses[s] = static_cast<float>(hl[s]);
+  const double last = steps > 0 ? hl[steps - 1] : 0.0;
   int err = 0;
   d2h(&err, err_, sizeof(int), "err copy");
   if (err) throw std::runtime_error("tensor-core wait timed out during training");
