@@ -78,6 +78,10 @@ struct DevBlock {
   // species enthalpies h_k(T) of each cell, written by k_dq0 for the DPLUR
   // sweeps (layout D, ns components; mixtures under DPLUR only)
   double *h_spec;
+  // FP32-bulk path under DPLUR: the species enthalpies (k_dq0, instead of
+  // h_spec) and the inviscid spectral radii (the x flux pass, beside
+  // inv_spec) in FP32, the precision the sweeps use them in; layout D
+  float *h_spec32, *inv_spec32;
   // chemistry surrogate (layout Z; null when off): cells the surrogate judged
   // chemically quiet take its increment rate rho dY/dt as an explicit source
   unsigned char *chem_quiet;

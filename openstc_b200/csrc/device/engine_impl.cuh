@@ -533,13 +533,26 @@ class EngineT final : public Engine {
       ptr = static_cast<double *>(q);
     }
     B.h_spec = nullptr;
-    if (C::mix != 0 && p.implicit_method == 1) {
+    B.h_spec32 = B.inv_spec32 = nullptr;
+    if (C::mix != 0 && p.implicit_method == 1 && !C::mixed) {
       void *q = nullptr;
       const size_t bytes = sizeof(double) * static_cast<size_t>(B.D.size) * C::ns;
       cuda_check(cudaMalloc(&q, bytes), "cudaMalloc h_spec");
       cuda_check(cudaMemset(q, 0, bytes), "memset h_spec");
       allocations_.push_back(q);
       B.h_spec = static_cast<double *>(q);
+    }
+    if (C::mixed && p.implicit_method == 1) {
+      auto falloc = [&](int n) {
+        void *q = nullptr;
+        const size_t bytes = sizeof(float) * static_cast<size_t>(B.D.size) * n;
+        cuda_check(cudaMalloc(&q, bytes), "cudaMalloc fp32 spectra");
+        cuda_check(cudaMemset(q, 0, bytes), "memset fp32 spectra");
+        allocations_.push_back(q);
+        return static_cast<float *>(q);
+      };
+      if (C::mix != 0) B.h_spec32 = falloc(C::ns);
+      B.inv_spec32 = falloc(3);
     }
     for (auto &f : B.dqf) f = nullptr;
     if (C::mixed && p.implicit_method == 1) {

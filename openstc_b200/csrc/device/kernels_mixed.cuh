@@ -649,6 +649,11 @@ __device__ __forceinline__ void local_time_step_s(const DevBlock &B, const Src &
   B.inv_spec[nd] = s0;
   B.inv_spec[szd + nd] = s1;
   B.inv_spec[2 * szd + nd] = s2;
+  if (B.inv_spec32) {
+    B.inv_spec32[nd] = s0;
+    B.inv_spec32[szd + nd] = s1;
+    B.inv_spec32[2 * szd + nd] = s2;
+  }
   float gamma = 1.4f;
   if constexpr (C::mix != 0) gamma = S.gamma(n);
   const float coeff_1 = fmaxf(gamma, 4.f / 3.f) / S.prim(0, n);
@@ -1029,7 +1034,7 @@ __global__ void __launch_bounds__(kCta, 4) k_sweep_mx(const DevBlock *__restrict
   const fp32::Src32<C> f{B.f32, sz};
   float tot[NV];
   OSTC_UNROLL for (int l = 0; l < NV; ++l) tot[l] = 0;
-  const double *isr = B.inv_spec;
+  const float *isr = B.inv_spec32;  // FP32 values, as k_flux_x computed them
 #pragma unroll 1
   for (int q = 0; q < 6; ++q) {
     const int dir = q < 3 ? q : q - 3;
@@ -1039,7 +1044,7 @@ __global__ void __launch_bounds__(kCta, 4) k_sweep_mx(const DevBlock *__restrict
     if (plus ? id == ext - 1 : id == 0) continue;
     const int64_t gs = dir == 0 ? 1 : (dir == 1 ? sx : sxy), ds = dir == 0 ? 1 : (dir == 1 ? dsx : dsxy);
     const int64_t on = plus ? n + gs : n - gs, od = plus ? nd + ds : nd - ds;
-    const float sr = ldf(isr + dir * szd + od);
+    const float sr = __ldg(isr + dir * szd + od);
     // compute_jacobian_times_dq (src/DPLURHPP.cuh:78-125) at the neighbour,
     // its state from the step's FP32 copy (k_pack32; unchanged until the update)
     const float xi_x = f.metric(3 * dir, on), xi_y = f.metric(3 * dir + 1, on), xi_z = f.metric(3 * dir + 2, on);
@@ -1054,7 +1059,7 @@ __global__ void __launch_bounds__(kCta, 4) k_sweep_mx(const DevBlock *__restrict
       const float t = f.prim(5, on);
       gamma = f.gamma(on);
       OSTC_UNROLL for (int l = 0; l < NS; ++l) {
-        const float hk = ldf(B.h_spec + l * szd + od);
+        const float hk = __ldg(B.h_spec32 + l * szd + od);
         b3 += fp32::kRu * t * cF.mw_inv[l] * d[5 + l];
         b4 += hk * d[5 + l];
         h += f.prim(6 + l, on) * hk;
@@ -1077,7 +1082,8 @@ __global__ void __launch_bounds__(kCta, 4) k_sweep_mx(const DevBlock *__restrict
     OSTC_UNROLL for (int l = 0; l < C::nsc; ++l) tot[5 + l] += sg * (lmd1 * d[5 + l] + f.prim(6 + l, on) * b1);
   }
   const double dt = B.dt_local[nz];
-  const double diag = 1 + dt * (isr[nd] + isr[szd + nd] + isr[2 * szd + nd]);
+  const double diag = 1 + dt * (static_cast<double>(isr[nd]) + static_cast<double>(isr[szd + nd]) +
+                                static_cast<double>(isr[2 * szd + nd]));
   double out[NV];
   if constexpr (C::mix != 2) {
     OSTC_UNROLL for (int l = 0; l < 5 + NS; ++l) out[l] = static_cast<double>(dq0[l * szd + nd]) + dt * tot[l] / diag;

@@ -482,7 +482,11 @@ __global__ void __launch_bounds__(kCta) k_dq0(const DevBlock *__restrict__ blks,
     // T is fixed during the sweeps: evaluate the species enthalpies once
     double hk[NS];
     enthalpy<NS>(B.bv[5 * B.G.size + B.G.at(i, j, k)], hk);
-    OSTC_UNROLL for (int l = 0; l < NS; ++l) B.h_spec[l * szd + nd] = hk[l];
+    if constexpr (C::mixed) {
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) B.h_spec32[l * szd + nd] = static_cast<float>(hk[l]);
+    } else {
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) B.h_spec[l * szd + nd] = hk[l];
+    }
   }
   if constexpr (C::mix != 2) {
     OSTC_UNROLL for (int l = 0; l < 5 + NS; ++l) dq[l] /= diag;
