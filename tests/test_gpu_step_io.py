@@ -50,6 +50,28 @@ def test_step_io_matches_plain_loop(tmp_path, precision, screen, chunk):
         b.close()
 
 
+def test_step_io_second_block_of_two(tmp_path):
+    """A two-block case: the fields of block 1 go up and down, block 0 stays
+    on the device; the result equals the plain loop's."""
+    case = cases.multiblock_case(tmp_path / "mb", mxs=[10, 8], my=12, mz=6, total_step=100, output_screen=50)
+    a = ostc.Driver(case)
+    b = ostc.Driver(case)
+    try:
+        for d in (a, b):
+            d.initialize()
+            d.step(1)
+        bv, sv = pinned_copy(a.get(1, "bv")), pinned_copy(a.get(1, "sv"))
+        a.step_io(4, 1, ["bv", "sv"], [bv, sv], chunk_bytes=2048)
+        b.step(4)
+        for blk in (0, 1):
+            for f in ("bv", "sv"):
+                assert np.array_equal(a.get(blk, f), b.get(blk, f)), (blk, f)
+        assert np.array_equal(bv, b.get(1, "bv").ravel())
+    finally:
+        a.close()
+        b.close()
+
+
 def test_step_io_rejects_bad_arguments(tmp_path):
     case = cases.mixing_layer_case(tmp_path / "ml", mx=8, my=8, mz=4, total_step=10, output_screen=1)
     d = ostc.Driver(case)
