@@ -518,17 +518,26 @@ double Driver::step_io(int n, int block, const std::vector<int> &fields, const s
   const int screen = parameter.get_int("output_screen");
   const int nf = static_cast<int>(fields.size());
   double err = -1;
-  for (int q = 0; q < n; ++q) {
-    E.upload_chunked(block, fields.data(), host.data(), nf, chunk_bytes);
-    ++step;
-    const bool store = step % screen == 0;
-    const bool due = store || step == 1;
-    double raw[4] = {0, 0, 0, 0};
-    last_step_residual = false;
-    E.step(store, due, raw);
-    if (due) err = compute_residual(step, raw);
-    last_step_residual = due;
-    E.download_chunked(block, fields.data(), host.data(), nf, chunk_bytes);
+  try {
+    for (int q = 0; q < n; ++q) {
+      E.upload_chunked(block, fields.data(), host.data(), nf, chunk_bytes);
+      ++step;
+      const bool store = step % screen == 0;
+      const bool due = store || step == 1;
+      double raw[4] = {0, 0, 0, 0};
+      last_step_residual = false;
+      E.step(store, due, raw);
+      if (due) err = compute_residual(step, raw);
+      last_step_residual = due;
+      E.download_chunked(block, fields.data(), host.data(), nf, chunk_bytes);
+    }
+  } catch (...) {
+    // no copy may still touch the caller's buffers once the error reaches it
+    try {
+      E.sync_copies();
+    } catch (...) {
+    }
+    throw;
   }
   E.sync_copies();
   E.synchronize();
