@@ -1137,6 +1137,7 @@ __global__ void __launch_bounds__(kCta) k_props_mx(const DevBlock *__restrict__ 
   const float t = ldf(B.bv + 5 * sz + n);
   if constexpr (C::mix != 0) {
     float cp[NS], Y[NS];
+    const float vel = ldf(B.vel + n);  // read before the first store, which would hold it back
     fp32::thermo<NS, false, true>(t, nullptr, cp);
     float mw_inv = 0, cp_tot = 0, cv = 0;
     OSTC_UNROLL for (int l = 0; l < NS; ++l) {
@@ -1145,7 +1146,7 @@ __global__ void __launch_bounds__(kCta) k_props_mx(const DevBlock *__restrict__ 
       cp_tot += Y[l] * cp[l];
       cv += Y[l] * (cp[l] - cF.ru_mw[l]);
     }
-    const float gamma = cp_tot / cv;
+    const float gamma = __fdividef(cp_tot, cv);
     B.cp[n] = cp_tot;
     B.gamma[n] = gamma;
     const float a = sqrtf(gamma * fp32::kRu * t * mw_inv);
@@ -1156,9 +1157,10 @@ __global__ void __launch_bounds__(kCta) k_props_mx(const DevBlock *__restrict__ 
     OSTC_UNROLL for (int l = 0; l < NS; ++l) {
       X[l] = Y[l] * mw * cF.mw_inv[l];
       const float t_dl = t * cF.lj_inv[l];
-      const float r = 1.f / (t_dl + 0.5f);
-      const float ci = 1.147f * powf(t_dl, -0.145f) + r * r;
-      vis[l] = cF.vis_coeff[l] * st / ci;
+      // the hardware-approximate power and quotients (errors of a few ulp)
+      const float r = __fdividef(1.f, t_dl + 0.5f);
+      const float ci = 1.147f * __powf(t_dl, -0.145f) + r * r;
+      vis[l] = __fdividef(cF.vis_coeff[l] * st, ci);
       rs[l] = rsqrtf(vis[l]);
       sq[l] = vis[l] * rs[l];
     }
@@ -1173,9 +1175,9 @@ __global__ void __launch_bounds__(kCta) k_props_mx(const DevBlock *__restrict__ 
         }
         vt += phi * X[q];
       }
-      viscosity += vis[m] * X[m] / vt;
+      viscosity += __fdividef(vis[m] * X[m], vt);
       const float lambda = vis[m] * (cp[m] + 1.25f * cF.ru_mw[m]);
-      conductivity += lambda * X[m] / (1.065f * vt - 0.065f * X[m]);
+      conductivity += __fdividef(lambda * X[m], 1.065f * vt - 0.065f * X[m]);
     }
     B.mul[n] = viscosity;
     B.cond[n] = conductivity;
@@ -1183,7 +1185,7 @@ __global__ void __launch_bounds__(kCta) k_props_mx(const DevBlock *__restrict__ 
       const float dd = fabsf(X[l] - 1) < 1e-3f ? viscosity / cF.Sc : (1 - Y[l]) * viscosity / ((1 - X[l]) * cF.Sc);
       B.rho_d[l * sz + n] = dd;
     }
-    B.mach[n] = ldf(B.vel + n) / a;
+    B.mach[n] = vel / a;
   } else {
     const float a = sqrtf(1.4f * fp32::kRu / static_cast<float>(kDMwAir) * t);
     B.acoustic[n] = a;
