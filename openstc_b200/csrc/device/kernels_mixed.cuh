@@ -57,6 +57,11 @@ inline MixParams make_mix_params(const DevParams &p) {
 
 namespace fp32 {
 
+// tanh of a non-negative argument from one hardware exponential:
+// 1 - 2 / (e^{2x} + 1) (relative error near 1e-6; 1 where e^{2x} overflows).
+// The SST blending functions F1, F2 take it.
+__device__ __forceinline__ float tanh_pos(float x) { return 1.f - __fdividef(2.f, __expf(2.f * x) + 1.f); }
+
 constexpr float kRu = 8314.462618f;
 
 __device__ __forceinline__ float ldf(const double *p) { return static_cast<float>(__ldg(p)); }
@@ -393,7 +398,7 @@ __device__ __forceinline__ void viscous_face_r(const Src &S, int64_t n, int d, i
       const float CDkomega = fmaxf(1e-20f, 2 * rhom * so2 / omegam * (k_x * o_x + k_y * o_y + k_z * o_z));
       const float param3 = 4 * rhom * so2 * km / (CDkomega * d2);
       const float arg1 = fminf(fmaxf(param1, param2), param3);
-      f1 = tanhf(arg1 * arg1 * arg1 * arg1);
+      f1 = tanh_pos(arg1 * arg1 * arg1 * arg1);
     }
     const float sigma_k = static_cast<float>(sst::sigma_k2) + static_cast<float>(sst::delta_sigma_k) * f1;
     const float sigma_omega =
@@ -457,11 +462,11 @@ __device__ __forceinline__ void sst_source(const DevBlock &B, int64_t n, double 
     const float d2 = dy * dy;
     const float param2 = 500 * ldf(B.mul + n) / (density * d2 * omega);
     const float arg2 = fmaxf(2 * param1, param2);
-    f2 = tanhf(arg2 * arg2);
+    f2 = tanh_pos(arg2 * arg2);
     const float CDkomega = fmaxf(1e-20f, inter_var);
     const float param3 = 4 * density * so2 * tke / (CDkomega * d2);
     const float arg1 = fminf(fmaxf(param1, param2), param3);
-    f1 = tanhf(arg1 * arg1 * arg1 * arg1);
+    f1 = tanh_pos(arg1 * arg1 * arg1 * arg1);
   }
   float mut = 0;
   if (const float den = fmaxf(a1 * omega, vorticity * f2); den > 1e-25f) mut = a1 * rhoK / den;
