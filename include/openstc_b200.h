@@ -231,7 +231,8 @@ typedef struct ostc_surrogate ostc_surrogate;
    dY_EPI,k| / max_k |dY_EPI,k| per sample, over samples with max |dY_EPI| > 1e-6
    (smaller increments change nothing the solver resolves). */
 typedef struct ostc_surrogate_eval {
-  double mean_rel, max_rel; /* over the samples the trust gate accepts */
+  double mean_rel, max_rel; /* over the rel_count samples the trust gate accepts whose EPI
+                               increment reaches 1e-6; both 0 when rel_count is 0 */
   double mean_abs;          /* accepted: mean |dY - dY_EPI| */
   double max_defect;        /* accepted: element defect of the applied (projected) dY, max over elements of
                                |sum_k a_ek dY_k/W_k| / sum_k a_ek Y_k/W_k */
@@ -241,6 +242,7 @@ typedef struct ostc_surrogate_eval {
   double gate_pass;         /* fraction of samples the trust gate accepts */
   long long count;
   long long nonfinite;      /* samples whose (rejected) prediction was not finite */
+  long long rel_count;      /* accepted samples with max |dY_EPI| > 1e-6 */
 } ostc_surrogate_eval;
 
 /* Mechanism and device from the driver (9-species finite-rate case). */

@@ -43,7 +43,7 @@ class SurrogateEval(C.Structure):
     _fields_ = [("mean_rel", C.c_double), ("max_rel", C.c_double), ("mean_abs", C.c_double),
                 ("max_defect", C.c_double), ("mean_defect", C.c_double), ("median_rel_all", C.c_double),
                 ("p90_rel_all", C.c_double), ("gate_pass", C.c_double), ("count", C.c_longlong),
-                ("nonfinite", C.c_longlong)]
+                ("nonfinite", C.c_longlong), ("rel_count", C.c_longlong)]
 
 
 class SurrogateGate(C.Structure):
@@ -439,7 +439,11 @@ class Surrogate:
     def evaluate(self, begin: int, count: int) -> dict:
         e = SurrogateEval()
         _check(library().ostc_surrogate_evaluate(self._h, begin, count, C.byref(e)))
-        return {f: getattr(e, f) for f, _ in SurrogateEval._fields_}
+        out = {f: getattr(e, f) for f, _ in SurrogateEval._fields_}
+        if e.rel_count == 0:
+            # no accepted sample has a resolvable increment: no relative error to report
+            out["mean_rel"] = out["max_rel"] = None
+        return out
 
     def label(self, states: np.ndarray) -> np.ndarray:
         s = np.ascontiguousarray(states, dtype=np.float64)

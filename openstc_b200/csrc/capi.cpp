@@ -501,6 +501,7 @@ int ostc_surrogate_evaluate(ostc_surrogate *s, long long begin, long long count,
     out->gate_pass = e.gate_pass;
     out->count = e.count;
     out->nonfinite = e.nonfinite;
+    out->rel_count = e.rel_count;
     return OSTC_OK;
   });
 }

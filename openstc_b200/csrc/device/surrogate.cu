@@ -836,6 +836,7 @@ SurrogateEval Surrogate::evaluate(int64_t begin, int64_t count) {
   }
   e.gate_pass = static_cast<double>(n_acc) / static_cast<double>(count);
   e.mean_rel = rel_n ? rel_sum / rel_n : 0;
+  e.rel_count = rel_n;
   if (n_acc) {
     e.mean_abs /= n_acc;
     e.mean_defect /= n_acc;

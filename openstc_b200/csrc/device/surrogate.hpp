@@ -61,11 +61,13 @@ struct SurrogateDev {
 // 1e-6); the defect is that of the prediction the solver would apply (after
 // the element projection), relative to the element totals.
 struct SurrogateEval {
-  double mean_rel, max_rel, mean_abs;  // the samples the trust gate accepts
+  double mean_rel, max_rel;            // the rel_count accepted samples with a resolvable increment
+  double mean_abs;                     // the samples the trust gate accepts
   double max_defect, mean_defect;      // accepted samples
   double median_rel_all, p90_rel_all;  // every sample
   double gate_pass;                    // fraction accepted
   int64_t count, nonfinite;            // samples; predictions that were not finite
+  int64_t rel_count;                   // accepted samples whose EPI increment reaches the floor
 };
 
 class Surrogate {

@@ -64,3 +64,42 @@ def test_layouts_follow_reference_ghosts(case_factory):
     assert d.layout("chem_jac") == (0, 81)  # EPI Jacobian, no ghosts
     assert d.layout("bv_last") == (0, 4)
     assert d.field_shape(0, "metric") == (9, 10, 14, 16)
+
+
+STRUCTS = {
+    "ostc_options": ostc.Options, "ostc_info": ostc.Info, "ostc_params": ostc.Params, "ostc_bc": ostc.Bc,
+    "ostc_inner": ostc.Inner, "ostc_surrogate_eval": ostc.SurrogateEval,
+    "ostc_surrogate_gate": ostc.SurrogateGate, "ostc_tuning": ostc.Tuning,
+}
+
+
+def test_ctypes_structures_match_header(tmp_path):
+    """Every ctypes mirror of a C-ABI struct has the header's size, field
+    names, offsets and field sizes (compiled with the host C compiler)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "openstc_b200.h"', "int main(void) {",
+             '  printf("OSTC_MAX_SPEC %d\\n", OSTC_MAX_SPEC);', '  printf("OSTC_MAX_REAC %d\\n", OSTC_MAX_REAC);']
+    for cname, cls in STRUCTS.items():
+        lines.append(f'  printf("{cname} %zu\\n", sizeof({cname}));')
+        for f, _ in cls._fields_:
+            lines.append(f'  printf("{cname}.{f} %zu %zu\\n", offsetof({cname}, {f}), '
+                         f"sizeof((({cname} *)0)->{f}));")
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", "-Wall", "-Werror", "-I", str(ROOT / "include"), str(src), "-o", str(exe)],
+                   check=True)
+    got = dict(line.split(" ", 1) for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                               text=True).stdout.splitlines())
+    assert int(got["OSTC_MAX_SPEC"]) == ostc.MAX_SPEC and int(got["OSTC_MAX_REAC"]) == ostc.MAX_REAC
+    for cname, cls in STRUCTS.items():
+        assert int(got[cname]) == ctypes.sizeof(cls), cname
+        for f, _ in cls._fields_:
+            off, size = map(int, got[f"{cname}.{f}"].split())
+            desc = getattr(cls, f)
+            assert (desc.offset, desc.size) == (off, size), (cname, f)
