@@ -194,7 +194,8 @@ def ramp_case(case: str | Path, mx: int = 256, my: int = 128, total_step: int = 
         (0, mx - 1, my - 1, my - 1, 0, 0, 3),
     ]])
     write_setup(case, setup_files(
-        dimension=2, total_step=total_step, output_file=output_file or total_step, output_screen=output_screen,
+        dimension=2, total_step=total_step, output_file=total_step if output_file is None else output_file,
+        output_screen=output_screen,
         cfl=0.5, implicit_method=0, dplur_inner_step=3, species=False, reaction=False, turbulence=False,
         inflows=[dict(name="freestream", label=5, temperature=220.0, mach=3.0, pressure=2500.0, u=1.0, v=0.0,
                       w=0.0)],

@@ -204,6 +204,9 @@ Driver::Driver(const std::string &dir, const DriverOptions &o) : case_dir(dir), 
   mix = species ? (reaction ? 2 : 1) : 0;
   if (rans && parameter.get_int("RANS_model") != 2)
     throw ParameterError("only the k-omega SST model (RANS_model = 2) is implemented");
+  // the step loops take step % output_screen and step % output_file
+  for (const char *key : {"output_screen", "output_file"})
+    if (parameter.get_int(key) < 1) throw ParameterError(std::string(key) + " must be a positive number of steps");
 
   // initialize_basic_variables, src/Initialize.cuh:37-55: the default inflow
   // is always constructed first, which defines rho_inf / v_inf / p_inf.

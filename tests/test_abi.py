@@ -36,6 +36,14 @@ def test_device_calls_need_initialize(case_factory):
         d.step(1)
 
 
+@pytest.mark.parametrize("key", ["output_screen", "output_file"])
+def test_step_intervals_must_be_positive(tmp_path, key):
+    kw = {"output_screen": 1, "output_file": 2, key: 0}
+    case = cases.ramp_case(tmp_path / "ramp", mx=16, my=12, total_step=2, **kw)
+    with pytest.raises(ostc.OstcError, match=key + " must be a positive number of steps"):
+        ostc.Driver(case)
+
+
 def test_ramp_case_description(case_factory):
     case = case_factory("ramp", cases.ramp_case, mx=16, my=12, total_step=2, output_screen=1)
     d = ostc.Driver(case)
