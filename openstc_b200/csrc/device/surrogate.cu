@@ -65,6 +65,17 @@ void ck(cudaError_t e, const char *what) {
   if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
 }
 
+// A temporary device array, freed when it leaves scope (an exception from a
+// failed check included; cudaFree waits for the work still using it).
+template <class T>
+struct DevTemp {
+  T *p = nullptr;
+  DevTemp(size_t count, const char *what) { ck(cudaMalloc(&p, count * sizeof(T)), what); }
+  ~DevTemp() { cudaFree(p); }
+  DevTemp(const DevTemp &) = delete;
+  DevTemp &operator=(const DevTemp &) = delete;
+};
+
 __host__ __device__ inline uint64_t mix64(uint64_t x) {
   x += 0x9E3779B97F4A7C15ull;
   x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -449,14 +460,12 @@ void Surrogate::generate(int64_t n, uint64_t seed, const DevBlock *field, double
   k_label<<<(n + 127) / 128, 128, smem, stream_>>>(states_, labels_, n);
   ck(cudaGetLastError(), "label launch");
   // normalisation from the data
-  double *acc = nullptr;
-  ck(cudaMalloc(&acc, (2 * kSurIn + kSurOut) * sizeof(double)), "cudaMalloc stats");
-  ck(cudaMemsetAsync(acc, 0, (2 * kSurIn + kSurOut) * sizeof(double), stream_), "memset stats");
-  k_stats<<<1184, 256, 0, stream_>>>(states_, labels_, n, acc);
+  DevTemp<double> acc(2 * kSurIn + kSurOut, "cudaMalloc stats");
+  ck(cudaMemsetAsync(acc.p, 0, (2 * kSurIn + kSurOut) * sizeof(double), stream_), "memset stats");
+  k_stats<<<1184, 256, 0, stream_>>>(states_, labels_, n, acc.p);
   double h[2 * kSurIn + kSurOut];
-  ck(cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, stream_), "stats copy");
+  ck(cudaMemcpyAsync(h, acc.p, sizeof(h), cudaMemcpyDeviceToHost, stream_), "stats copy");
   ck(cudaStreamSynchronize(stream_), "generate");
-  cudaFree(acc);
   Norm nm{};
   for (int q = 0; q < kSurIn; ++q) {
     const double mu = h[q] / n, var = std::max(h[kSurIn + q] / n - mu * mu, 1e-12);
@@ -594,8 +603,8 @@ double Surrogate::train(int steps, int batch, double lr, int64_t n_train, float 
   ensure_batch(batch);
   // each step's loss stays on the device until the end: no host
   // synchronisation between steps
-  double *dloss = nullptr;
-  ck(cudaMalloc(&dloss, sizeof(double) * std::max(1, steps)), "cudaMalloc losses");
+  DevTemp<double> dloss_buf(static_cast<size_t>(std::max(1, steps)), "cudaMalloc losses");
+  double *dloss = dloss_buf.p;
   for (int s = 0; s < steps; ++s) {
     k_gather<<<(batch + 255) / 256, 256, 0, stream_>>>(x_, t_, n_train, mix64(seed_ + 0x5151 * (adam_t_ + 1)), batch,
                                                        a_[0], at_[0], tb_);
@@ -615,7 +624,6 @@ double Surrogate::train(int steps, int batch, double lr, int64_t n_train, float 
   std::vector<double> hl(static_cast<size_t>(std::max(1, steps)), 0.0);
   cudaError_t st = cudaMemcpyAsync(hl.data(), dloss, sizeof(double) * hl.size(), cudaMemcpyDeviceToHost, stream_);
   if (st == cudaSuccess) st = cudaStreamSynchronize(stream_);
-  cudaFree(dloss);
   ck(st, "train steps");
   if (losses)
     for (int s = 0; s < steps; ++s) losses[s] = static_cast<float>(hl[s]);
@@ -669,9 +677,8 @@ void Surrogate::features(const double *states_dev, int64_t n, uint16_t *x_dev, f
 void Surrogate::label_host(const double *states, int64_t n, double *dy) {
   ck(cudaSetDevice(device_), "cudaSetDevice");
   upload_chem();
-  double *s = nullptr, *d = nullptr;
-  ck(cudaMalloc(&s, n * kSurIn * 8), "label alloc");
-  ck(cudaMalloc(&d, n * NS * 8), "label alloc");
+  DevTemp<double> s_buf(n * kSurIn, "label alloc"), d_buf(n * NS, "label alloc");
+  double *s = s_buf.p, *d = d_buf.p;
   ck(cudaMemcpyAsync(s, states, n * kSurIn * 8, cudaMemcpyHostToDevice, stream_), "label upload");
   const size_t smem = label_smem(chem_);
   ck(cudaFuncSetAttribute(k_label, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)), "smem");
@@ -679,8 +686,6 @@ void Surrogate::label_host(const double *states, int64_t n, double *dy) {
   ck(cudaGetLastError(), "label");
   ck(cudaMemcpyAsync(dy, d, n * NS * 8, cudaMemcpyDeviceToHost, stream_), "label download");
   ck(cudaStreamSynchronize(stream_), "label");
-  cudaFree(s);
-  cudaFree(d);
 }
 
 namespace {
@@ -704,12 +709,11 @@ void Surrogate::predict_host(const double *states, int64_t n, double *dy, int *a
   ck(cudaSetDevice(device_), "cudaSetDevice");
   const int batch = static_cast<int>((n + 127) / 128 * 128);
   ensure_batch(batch);
-  double *s = nullptr, *d = nullptr;
-  int *acc = nullptr;
-  ck(cudaMalloc(&s, static_cast<size_t>(batch) * kSurIn * 8), "predict alloc");
+  DevTemp<double> s_buf(static_cast<size_t>(batch) * kSurIn, "predict alloc"), d_buf(n * NS, "predict alloc");
+  DevTemp<int> acc_buf(n, "predict alloc");
+  double *s = s_buf.p, *d = d_buf.p;
+  int *acc = acc_buf.p;
   ck(cudaMemsetAsync(s, 0, static_cast<size_t>(batch) * kSurIn * 8, stream_), "predict memset");
-  ck(cudaMalloc(&d, n * NS * 8), "predict alloc");
-  ck(cudaMalloc(&acc, n * sizeof(int)), "predict alloc");
   ck(cudaMemcpyAsync(s, states, n * kSurIn * 8, cudaMemcpyHostToDevice, stream_), "predict upload");
   features(s, n, a_[0], nullptr, nullptr);
   ck(cudaMemsetAsync(a_[0] + n * kSurInPad, 0, (batch - n) * kSurInPad * 2, stream_), "pad rows");
@@ -722,9 +726,6 @@ void Surrogate::predict_host(const double *states, int64_t n, double *dy, int *a
   ck(cudaMemcpyAsync(dy, d, n * NS * 8, cudaMemcpyDeviceToHost, stream_), "predict download");
   ck(cudaMemcpyAsync(accepted, acc, n * sizeof(int), cudaMemcpyDeviceToHost, stream_), "predict download");
   ck(cudaStreamSynchronize(stream_), "predict");
-  cudaFree(s);
-  cudaFree(d);
-  cudaFree(acc);
 }
 
 double Surrogate::grad_host(const double *states, const double *dy, int64_t n, std::vector<std::vector<float>> &grads) {
@@ -732,9 +733,8 @@ double Surrogate::grad_host(const double *states, const double *dy, int64_t n, s
   if (n % 128) throw std::runtime_error("gradient batch must be a multiple of 128");
   const int batch = static_cast<int>(n);
   ensure_batch(batch);
-  double *s = nullptr, *d = nullptr;
-  ck(cudaMalloc(&s, n * kSurIn * 8), "grad alloc");
-  ck(cudaMalloc(&d, n * NS * 8), "grad alloc");
+  DevTemp<double> s_buf(n * kSurIn, "grad alloc"), d_buf(n * NS, "grad alloc");
+  double *s = s_buf.p, *d = d_buf.p;
   ck(cudaMemcpyAsync(s, states, n * kSurIn * 8, cudaMemcpyHostToDevice, stream_), "grad upload");
   ck(cudaMemcpyAsync(d, dy, n * NS * 8, cudaMemcpyHostToDevice, stream_), "grad upload");
   features(s, n, a_[0], tb_, d);
@@ -769,8 +769,6 @@ double Surrogate::grad_host(const double *states, const double *dy, int64_t n, s
   double loss = 0;
   ck(cudaMemcpyAsync(&loss, loss_, sizeof(double), cudaMemcpyDeviceToHost, stream_), "loss");
   ck(cudaStreamSynchronize(stream_), "grad");
-  cudaFree(s);
-  cudaFree(d);
   return loss;
 }
 
