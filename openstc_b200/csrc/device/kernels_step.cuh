@@ -973,30 +973,48 @@ struct DevBc {
   double t_wall;
 };
 
-// compute_total_energy, src/FieldOperation.cuh:15-35
+// compute_total_energy, src/FieldOperation.cuh:15-35: rho E of a cell from
+// its primitives and the species' rho Y; speed = |V|
+template <class C>
+__device__ __forceinline__ double total_energy_of(double rho, double u, double v, double w, double p, double t,
+                                                  const double *rho_y, double &speed) {
+  constexpr int NS = C::ns;
+  const double vel = u * u + v * v + w * w;
+  // the reference stores this product in cv before adding the enthalpies
+  double e = __dmul_rn(0.5 * rho, vel);
+  if constexpr (C::mix != 0) {
+    double h[NS];
+    enthalpy<NS>(t, h);
+    OSTC_UNROLL for (int l = 0; l < NS; l++) e += h[l] * rho_y[l];
+    e -= p;
+  } else {
+    e += p / (kDGammaAir - 1);
+  }
+  speed = sqrt(vel);
+  return e;
+}
+
 template <class C>
 __device__ __forceinline__ void total_energy(const DevBlock &B, int64_t n) {
   constexpr int NS = C::ns;
   const int64_t sz = B.G.size;
-  const double u = B.bv[sz + n], v = B.bv[2 * sz + n], w = B.bv[3 * sz + n];
-  const double vel = u * u + v * v + w * w;
-  // the reference stores this product in cv before adding the enthalpies
-  double e = __dmul_rn(0.5 * B.bv[n], vel);
-  if constexpr (C::mix != 0) {
-    double h[NS];
-    enthalpy<NS>(B.bv[5 * sz + n], h);
-    OSTC_UNROLL for (int l = 0; l < NS; l++) e += h[l] * B.cv[(5 + l) * sz + n];
-    e -= B.bv[4 * sz + n];
-  } else {
-    e += B.bv[4 * sz + n] / (kDGammaAir - 1);
-  }
-  B.cv[4 * sz + n] = e;
-  B.vel[n] = sqrt(vel);
+  double rho_y[NS > 0 ? NS : 1];
+  if constexpr (C::mix != 0)
+    OSTC_UNROLL for (int l = 0; l < NS; l++) rho_y[l] = B.cv[(5 + l) * sz + n];
+  double speed;
+  B.cv[4 * sz + n] = total_energy_of<C>(B.bv[n], B.bv[sz + n], B.bv[2 * sz + n], B.bv[3 * sz + n],
+                                        B.bv[4 * sz + n], B.bv[5 * sz + n], rho_y, speed);
+  B.vel[n] = speed;
 }
 
+// Each branch reads what it needs before its first store: the compiler cannot
+// tell the arrays apart, so a load written after a store would wait for that
+// store, one memory round trip per variable.  The arithmetic is the
+// reference's, in its order.
 template <class C>
 __global__ void k_bc(const DevBlock *__restrict__ blks, const DevBc *__restrict__ bcs, int face) {
   constexpr int NS = C::ns, NSC = C::nsc;
+  constexpr int NS1 = NS > 0 ? NS : 1, NSC1 = NSC > 0 ? NSC : 1;
   const DevBc &f = bcs[face];
   const int e0 = f.end[0] - f.start[0] + 1, e1 = f.end[1] - f.start[1] + 1, e2 = f.end[2] - f.start[2] + 1;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1011,11 +1029,15 @@ __global__ void k_bc(const DevBlock *__restrict__ blks, const DevBc *__restrict_
   const int64_t n = B.G.at(i, j, k);
   double *bv = B.bv, *sv = B.sv, *cv = B.cv;
   if (f.type == 6) {  // apply_outflow
+    double b[6], s[NSC1], mut_n = 0;
+    OSTC_UNROLL for (int l = 0; l < 6; ++l) b[l] = bv[l * sz + n];
+    OSTC_UNROLL for (int l = 0; l < NSC; ++l) s[l] = sv[l * sz + n];
+    if constexpr (C::turb) mut_n = B.mut[n];
     for (int g = 1; g <= ngg; ++g) {
       const int64_t gn = n + g * step;
-      for (int l = 0; l < 6; ++l) bv[l * sz + gn] = bv[l * sz + n];
-      for (int l = 0; l < NSC; ++l) sv[l * sz + gn] = sv[l * sz + n];
-      if constexpr (C::turb) B.mut[gn] = B.mut[n];
+      OSTC_UNROLL for (int l = 0; l < 6; ++l) bv[l * sz + gn] = b[l];
+      OSTC_UNROLL for (int l = 0; l < NSC; ++l) sv[l * sz + gn] = s[l];
+      if constexpr (C::turb) B.mut[gn] = mut_n;
     }
   } else if (f.type == 5) {  // apply_inflow
     for (int g = 1; g <= ngg; ++g) {
@@ -1033,59 +1055,81 @@ __global__ void k_bc(const DevBlock *__restrict__ blks, const DevBc *__restrict_
     const int64_t in = n - step;
     const double *mr = B.metric + 3 * f.face * sz;
     double k_x = mr[n], k_y = mr[sz + n], k_z = mr[2 * sz + n];
+    double bi[6], si[NSC1];
+    OSTC_UNROLL for (int l = 0; l < 6; ++l) bi[l] = bv[l * sz + in];
+    OSTC_UNROLL for (int l = 0; l < NSC; ++l) si[l] = sv[l * sz + in];
+    const double e_in = cv[4 * sz + in];
     const double k_magnitude = sqrt(k_x * k_x + k_y * k_y + k_z * k_z);
     k_x /= k_magnitude;
     k_y /= k_magnitude;
     k_z /= k_magnitude;
-    const double u1 = bv[sz + in], v1 = bv[2 * sz + in], w1 = bv[3 * sz + in];
+    const double u1 = bi[1], v1 = bi[2], w1 = bi[3];
     double u_k = k_x * u1 + k_y * v1 + k_z * w1;
     const double u_t = u1 - k_x * u_k, v_t = v1 - k_y * u_k, w_t = w1 - k_z * u_k;
+    const double rho = bi[0];  // the face takes the interior density
     bv[sz + n] = u_t;
     bv[2 * sz + n] = v_t;
     bv[3 * sz + n] = w_t;
     B.vel[n] = sqrt(u_t * u_t + v_t * v_t + w_t * w_t);
-    bv[n] = bv[in];
-    bv[4 * sz + n] = bv[4 * sz + in];
-    bv[5 * sz + n] = bv[5 * sz + in];
-    for (int l = 0; l < NSC; ++l) sv[l * sz + n] = sv[l * sz + in];
-    const double rho = bv[n];
+    bv[n] = rho;
+    bv[4 * sz + n] = bi[4];
+    bv[5 * sz + n] = bi[5];
+    OSTC_UNROLL for (int l = 0; l < NSC; ++l) sv[l * sz + n] = si[l];
     cv[n] = rho;
-    cv[sz + n] = rho * bv[sz + n];
-    cv[2 * sz + n] = rho * bv[2 * sz + n];
-    cv[3 * sz + n] = rho * bv[3 * sz + n];
-    cv[4 * sz + n] = cv[4 * sz + in] - 0.5 * bv[in] * (u1 * u1 + v1 * v1 + w1 * w1) +
-                     0.5 * rho * (u_t * u_t + v_t * v_t + w_t * w_t);
-    for (int l = 0; l < NSC; ++l) cv[(5 + l) * sz + n] = rho * sv[l * sz + n];
+    cv[sz + n] = rho * u_t;
+    cv[2 * sz + n] = rho * v_t;
+    cv[3 * sz + n] = rho * w_t;
+    cv[4 * sz + n] = e_in - 0.5 * rho * (u1 * u1 + v1 * v1 + w1 * w1) + 0.5 * rho * (u_t * u_t + v_t * v_t + w_t * w_t);
+    OSTC_UNROLL for (int l = 0; l < NSC; ++l) cv[(5 + l) * sz + n] = rho * si[l];
     for (int g = 1; g <= ngg; ++g) {
       const int64_t gn = n + g * step, ig = n - g * step;
-      bv[gn] = bv[ig];
-      const double u = bv[sz + ig], v = bv[2 * sz + ig], w = bv[3 * sz + ig];
+      double bg[6], sg[NSC1], mut_g = 0;
+      OSTC_UNROLL for (int l = 0; l < 6; ++l) bg[l] = bv[l * sz + ig];
+      OSTC_UNROLL for (int l = 0; l < NSC; ++l) sg[l] = sv[l * sz + ig];
+      if constexpr (C::turb) mut_g = B.mut[ig];
+      const double u = bg[1], v = bg[2], w = bg[3];
       u_k = k_x * u + k_y * v + k_z * w;
       const double ug = u - 2 * u_k * k_x, vg = v - 2 * u_k * k_y, wg = w - 2 * u_k * k_z;
+      bv[gn] = bg[0];
       bv[sz + gn] = ug;
       bv[2 * sz + gn] = vg;
       bv[3 * sz + gn] = wg;
       B.vel[gn] = sqrt(ug * ug + vg * vg + wg * wg);
-      bv[4 * sz + gn] = bv[4 * sz + ig];
-      bv[5 * sz + gn] = bv[5 * sz + ig];
-      for (int l = 0; l < NSC; ++l) sv[l * sz + gn] = sv[l * sz + ig];
-      if constexpr (C::turb) B.mut[gn] = B.mut[ig];
+      bv[4 * sz + gn] = bg[4];
+      bv[5 * sz + gn] = bg[5];
+      OSTC_UNROLL for (int l = 0; l < NSC; ++l) sv[l * sz + gn] = sg[l];
+      if constexpr (C::turb) B.mut[gn] = mut_g;
     }
   } else if (f.type == 2) {  // apply_wall
     const int64_t in = n - step;
+    const double t_in = bv[5 * sz + in], p = bv[4 * sz + in];
+    double s_in[NSC1];
+    OSTC_UNROLL for (int l = 0; l < NSC; ++l) s_in[l] = sv[l * sz + in];
+    double dy = 0;
+    if constexpr (C::turb) dy = B.wall_dist[in];
     double t_wall = f.t_wall;
-    if (!f.isothermal) t_wall = bv[5 * sz + in];
-    const double p = bv[4 * sz + in];
+    if (!f.isothermal) t_wall = t_in;
     double mw = kDMwAir;
     if constexpr (C::mix != 0) {
       mw = 0;
-      OSTC_UNROLL for (int l = 0; l < NS; ++l) {
-        sv[l * sz + n] = sv[l * sz + in];
-        mw += sv[l * sz + n] / cP.mw[l];
-      }
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) mw += s_in[l] / cP.mw[l];
       mw = 1 / mw;
     }
     const double rho_wall = p * mw / (t_wall * kDR_u);
+    double rho_y[NS1];
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) rho_y[l] = s_in[l] * rho_wall;
+    double speed;
+    const double e_wall = total_energy_of<C>(rho_wall, 0.0, 0.0, 0.0, p, t_wall, rho_y, speed);
+    double omega = 0;
+    if constexpr (C::turb) {
+      double mu_wall;
+      if constexpr (C::mix != 0)
+        mu_wall = mixture_viscosity<NS>(t_wall, mw, s_in);
+      else
+        mu_wall = sutherland(t_wall);
+      omega = dy > 1e-25 ? 60 * mu_wall / (rho_wall * sst::beta_1 * dy * dy) : s_in[NS + 1];
+    }
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) sv[l * sz + n] = s_in[l];
     bv[n] = rho_wall;
     bv[sz + n] = 0;
     bv[2 * sz + n] = 0;
@@ -1096,31 +1140,21 @@ __global__ void k_bc(const DevBlock *__restrict__ blks, const DevBc *__restrict_
     cv[sz + n] = 0;
     cv[2 * sz + n] = 0;
     cv[3 * sz + n] = 0;
-    OSTC_UNROLL for (int l = 0; l < NS; ++l) cv[(l + 5) * sz + n] = sv[l * sz + n] * rho_wall;
-    total_energy<C>(B, n);
+    OSTC_UNROLL for (int l = 0; l < NS; ++l) cv[(l + 5) * sz + n] = rho_y[l];
+    cv[4 * sz + n] = e_wall;
+    B.vel[n] = speed;
     if constexpr (C::turb) {
-      double mu_wall;
-      if constexpr (C::mix != 0) {
-        double Y[NS];
-        OSTC_UNROLL for (int l = 0; l < NS; ++l) Y[l] = sv[l * sz + n];
-        mu_wall = mixture_viscosity<NS>(t_wall, mw, Y);
-      } else {
-        mu_wall = sutherland(t_wall);
-      }
-      const double dy = B.wall_dist[in];
       sv[NS * sz + n] = 0;
       cv[(NS + 5) * sz + n] = 0;
-      if (dy > 1e-25) {
-        sv[(NS + 1) * sz + n] = 60 * mu_wall / (rho_wall * sst::beta_1 * dy * dy);
-      } else {
-        sv[(NS + 1) * sz + n] = sv[(NS + 1) * sz + in];
-      }
-      cv[(NS + 6) * sz + n] = rho_wall * sv[(NS + 1) * sz + n];
+      sv[(NS + 1) * sz + n] = omega;
+      cv[(NS + 6) * sz + n] = rho_wall * omega;
     }
     for (int g = 1; g <= ngg; ++g) {
       const int64_t ig = n - g * step, gn = n + g * step;
       const double u_i = bv[sz + ig], v_i = bv[2 * sz + ig], w_i = bv[3 * sz + ig];
       const double p_i = bv[4 * sz + ig], t_i = bv[5 * sz + ig];
+      double y_i[NS1];
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) y_i[l] = sv[l * sz + ig];
       double t_g = t_i;
       if (f.isothermal) {
         t_g = 2 * t_wall - t_i;
@@ -1128,13 +1162,11 @@ __global__ void k_bc(const DevBlock *__restrict__ blks, const DevBc *__restrict_
       }
       if constexpr (C::mix != 0) {
         mw = 0;
-        OSTC_UNROLL for (int l = 0; l < NS; ++l) {
-          sv[l * sz + gn] = sv[l * sz + ig];
-          mw += sv[l * sz + gn] / cP.mw[l];
-        }
+        OSTC_UNROLL for (int l = 0; l < NS; ++l) mw += y_i[l] / cP.mw[l];
         mw = 1 / mw;
       }
       const double rho_g = p_i * mw / (t_g * kDR_u);
+      OSTC_UNROLL for (int l = 0; l < NS; ++l) sv[l * sz + gn] = y_i[l];
       bv[gn] = rho_g;
       bv[sz + gn] = -u_i;
       bv[2 * sz + gn] = -v_i;
@@ -1143,7 +1175,7 @@ __global__ void k_bc(const DevBlock *__restrict__ blks, const DevBc *__restrict_
       bv[5 * sz + gn] = t_g;
       if constexpr (C::turb) {
         sv[NS * sz + gn] = 0;
-        sv[(NS + 1) * sz + gn] = sv[(NS + 1) * sz + n];
+        sv[(NS + 1) * sz + gn] = omega;
         B.mut[gn] = 0;
       }
     }
@@ -1257,15 +1289,19 @@ __global__ void k_kcopy(const DevBlock *__restrict__ blks, int b) {
   if (t >= ex * ey) return;
   const int i = t % ex - g, j = t / ex - g;
   const int64_t sz = B.G.size, n0 = B.G.at(i, j, 0);
+  // the plane's values read once, before the stores
+  double pb[6], ps[C::nsc > 0 ? C::nsc : 1];
+  OSTC_UNROLL for (int l = 0; l < 6; ++l) pb[l] = B.bv[l * sz + n0];
+  OSTC_UNROLL for (int l = 0; l < C::nsc; ++l) ps[l] = B.sv[l * sz + n0];
   for (int k = 1; k <= g; ++k) {
     const int64_t np = n0 + k * B.G.sxy, nm = n0 - k * B.G.sxy;
-    for (int l = 0; l < 6; ++l) {
-      B.bv[l * sz + np] = B.bv[l * sz + n0];
-      B.bv[l * sz + nm] = B.bv[l * sz + n0];
+    OSTC_UNROLL for (int l = 0; l < 6; ++l) {
+      B.bv[l * sz + np] = pb[l];
+      B.bv[l * sz + nm] = pb[l];
     }
     OSTC_UNROLL for (int l = 0; l < C::nsc; ++l) {
-      B.sv[l * sz + np] = B.sv[l * sz + n0];
-      B.sv[l * sz + nm] = B.sv[l * sz + n0];
+      B.sv[l * sz + np] = ps[l];
+      B.sv[l * sz + nm] = ps[l];
     }
   }
 }
