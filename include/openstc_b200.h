@@ -306,9 +306,11 @@ int ostc_driver_chemistry_stats(ostc_driver *d, long long *accepted, long long *
    launches each block separately with fixed 2-D thread blocks,
    src/Driver.cu:205-216).  schedule: the order in which the blocks of a
    multi-block grid share each launch (0 block order, 1 largest block first);
-   flux_variant: the variant of the FP32-bulk flux passes (resident CTAs per SM
-   and cells each thread marches over; 0 on the FP64 path).  No choice changes
-   a result. */
+   flux_variant: on the FP32-bulk path the variant of the flux passes
+   (resident CTAs per SM and cells each thread marches over, 0-3); on the
+   FP64 path 0 the column kernel (each face evaluated once) or 1 the per-cell
+   kernel (each face evaluated by both of its cells, no barriers).  No choice
+   changes a result. */
 typedef struct ostc_tuning {
   int schedule, flux_variant;
   int candidates;     /* pairs timed */

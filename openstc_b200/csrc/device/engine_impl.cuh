@@ -698,8 +698,12 @@ class EngineT final : public Engine {
         case 2: launch_flux_passes<kFluxVariant[2].min_blocks, kFluxVariant[2].march>(); break;
         default: launch_flux_passes<kFluxVariant[3].min_blocks, kFluxVariant[3].march>(); break;
       }
-    } else
+    } else if (flux_variant_ == 1) {
+      // the per-cell form: each face evaluated by both of its cells, no barriers
+      k_flux<C><<<grid(tiles0_), block3(), flux_smem_, stream_>>>(d_blocks_, tiles0_);
+    } else {
       k_flux_col<C><<<grid(col_tiles_), kFluxThreads, col_smem_, stream_>>>(d_blocks_, col_tiles_);
+    }
   }
 
   template <int MINB, int MARCH>
@@ -1076,7 +1080,8 @@ class EngineT final : public Engine {
       }
   }
 
-  int flux_variants() const override { return C::mixed ? kFluxVariants : 1; }
+  // FP64: 0 the column kernel (faces once), 1 the per-cell kernel
+  int flux_variants() const override { return C::mixed ? kFluxVariants : 2; }
 
   double time_stages(int reps) override {
     upload_params();

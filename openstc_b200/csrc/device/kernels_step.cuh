@@ -911,6 +911,7 @@ __global__ void __launch_bounds__(kCta) k_props(const DevBlock *__restrict__ blk
   const DevBlock &B = blks[b];
   const int64_t n = B.G.at(i, j, k), sz = B.G.size;
   const double t = B.bv[5 * sz + n];
+  const double speed = B.vel[n];  // read before the first store, which would hold it back
   if constexpr (C::mix != 0) {
     double cp[NS], Y[NS];
     heat_capacity<NS>(t, cp);
@@ -949,7 +950,7 @@ __global__ void __launch_bounds__(kCta) k_props(const DevBlock *__restrict__ blk
       }
       B.rho_d[l * sz + n] = d;
     }
-    B.mach[n] = B.vel[n] / a;
+    B.mach[n] = speed / a;
   } else {
     constexpr double c_temp = kDGammaAir * kDR_u / kDMwAir;
     constexpr double cp = kDGammaAir * kDR_u / kDMwAir / (kDGammaAir - 1);
@@ -958,7 +959,7 @@ __global__ void __launch_bounds__(kCta) k_props(const DevBlock *__restrict__ blk
     const double mul = sutherland(t);
     B.mul[n] = mul;
     B.cond[n] = mul * cp / cP.Pr;
-    B.mach[n] = B.vel[n] / a;
+    B.mach[n] = speed / a;
   }
 }
 

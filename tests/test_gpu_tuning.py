@@ -1,7 +1,7 @@
 """The launch autotuner (ostc_driver_autotune): every tuning it chooses from
-(the order of the blocks in each launch x the variant of the FP32-bulk flux
-passes) computes the same fields bit for bit, and the choice it records is
-applied again by a later driver on the same case."""
+(the order of the blocks in each launch x the variant of the flux kernels)
+computes the same fields bit for bit, and the choice it records is applied
+again by a later driver on the same case."""
 import numpy as np
 import pytest
 
@@ -13,17 +13,17 @@ pytestmark = pytest.mark.gpu
 MXS, MY, MZ = [12, 9, 10], 12, 6
 
 
-def run(case, precision, schedule, variant, steps=3):
+def run(case, precision, schedule, variant, steps=3, fields=("bv", "sv", "dq")):
     d = ostc.Driver(case, precision=precision)
     d.initialize()
     d.set_tuning(schedule, variant)
     err = [d.step(1) for _ in range(steps)]
-    out = {f: [d.get(b, f) for b in range(d.info().n_block)] for f in ("bv", "sv", "dq")}
+    out = {f: [d.get(b, f) for b in range(d.info().n_block)] for f in fields}
     d.close()
     return out, err
 
 
-@pytest.mark.parametrize("precision,variants", [("fp64", 1), ("mixed", 4)])
+@pytest.mark.parametrize("precision,variants", [("fp64", 2), ("mixed", 4)])
 def test_every_tuning_gives_the_same_fields(case_factory, precision, variants):
     case = case_factory("tuning_blocks", cases.multiblock_case, mxs=MXS, my=MY, mz=MZ, total_step=3,
                         output_screen=1)
@@ -62,3 +62,15 @@ def test_autotune_records_its_choice(case_factory, tmp_path):
     with pytest.raises(ostc.OstcError, match="no such flux variant"):
         d.set_tuning(0, 9)
     d.close()
+
+
+def test_fp64_flux_forms_agree_on_the_ramp(case_factory):
+    """The column and the per-cell FP64 flux kernels on the 2-D ramp (a wall,
+    an inflow, an outflow and a symmetry face): the same fields bit for bit."""
+    case = case_factory("tuning_ramp", cases.ramp_case, mx=40, my=24, total_step=5, output_screen=1)
+    fields = ("bv", "dq", "dt_local")
+    ref, ref_err = run(case, "fp64", 0, 0, steps=5, fields=fields)
+    got, err = run(case, "fp64", 0, 1, steps=5, fields=fields)
+    assert err == ref_err
+    for f in ref:
+        assert np.array_equal(got[f][0], ref[f][0], equal_nan=True), f
