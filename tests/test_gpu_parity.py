@@ -22,6 +22,13 @@ pytestmark = pytest.mark.gpu
 from fixture_cases import FIXTURES
 
 CASES = {n: (fn, kw) for n, (fn, kw, _) in FIXTURES.items()}
+# The mixing layer whose j = 0 face is an isothermal wall: the wall boundary
+# with species and SST, checked against the oracle at initialisation only (no
+# reference-program fixture).  Its first update leaves k or omega negative in
+# the whole wall row, and limit_flow's turbulence branch then averages
+# neighbours that other threads overwrite (the reference's own race), so the
+# later phases depend on scheduling there.
+ORACLE_CASES = dict(CASES, ml_wall=(cases.mixing_layer_case, dict(mx=16, my=12, mz=6, wall_j0=True)))
 FIXTURE_RUNS = [(n, k) for n, (_, _, steps) in FIXTURES.items() for k in steps]
 
 STATE = ["bv", "sv", "cv", "vel", "acoustic", "mach", "mul", "conductivity", "mut", "turb_cond", "rho_d", "gamma",
@@ -29,7 +36,7 @@ STATE = ["bv", "sv", "cv", "vel", "acoustic", "mach", "mul", "conductivity", "mu
 
 
 def make_case(case_factory, name, steps=10):
-    fn, kw = CASES[name]
+    fn, kw = ORACLE_CASES[name]
     return case_factory(name, fn, **dict(kw, total_step=steps, output_screen=1, output_file=steps))
 
 
@@ -58,7 +65,7 @@ def compare(gpu, orc, fields, tol, ghosts=True):
     return worst
 
 
-@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("name", list(ORACLE_CASES))
 def test_initialization_matches_oracle(case_factory, name):
     gpu, orc = pair(make_case(case_factory, name))
     compare(gpu, orc, STATE, 1e-12)
