@@ -111,3 +111,44 @@ def test_ctypes_structures_match_header(tmp_path):
             off, size = map(int, got[f"{cname}.{f}"].split())
             desc = getattr(cls, f)
             assert (desc.offset, desc.size) == (off, size), (cname, f)
+
+
+def test_device_entry_points_refuse_an_uninitialised_driver(case_factory):
+    """Before ostc_driver_initialize every entry point that needs the device
+    returns OSTC_ERR_STATE ("initialize first") and touches nothing; with a
+    null driver each returns OSTC_ERR_INPUT.  Host only: no GPU is needed."""
+    case = case_factory("ramp", cases.ramp_case, mx=16, my=12, total_step=2, output_screen=1)
+    d = ostc.Driver(case)
+    lib = ostc.library()
+    x = np.zeros(16)
+    dp = x.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    fields = (ctypes.c_int * 1)(0)
+    hosts = (ctypes.c_void_p * 1)(x.ctypes.data)
+    counts = (ctypes.c_int64 * 1)(16)
+    ll = ctypes.c_longlong()
+    buf = ctypes.create_string_buffer(64)
+    calls = {
+        "ostc_driver_simulate": (),
+        "ostc_driver_step": (1, dp),
+        "ostc_driver_step_io": (1, 0, fields, hosts, counts, 1, 0, dp),
+        "ostc_driver_autotune": (1, None),
+        "ostc_driver_set_tuning": (0, 0),
+        "ostc_driver_residual_noalloc": (dp,),
+        "ostc_driver_run_phase": (0,),
+        "ostc_driver_get_field": (0, 0, dp, 16),
+        "ostc_driver_set_field": (0, 0, dp, 16),
+        "ostc_driver_write_plt": (b"never_written.plt",),
+        "ostc_driver_launches_per_step": (0, 0),
+        "ostc_driver_last_step_ms": (dp,),
+        "ostc_driver_profile_step": (buf, 64),
+        "ostc_driver_set_surrogate": (None,),
+        "ostc_driver_chemistry_stats": (ctypes.byref(ll), ctypes.byref(ll), ctypes.byref(ll)),
+    }
+    for name, args in calls.items():
+        fn = getattr(lib, name)
+        assert fn(d._h, *args) == -3, name  # OSTC_ERR_STATE
+        assert "initialize first" in lib.ostc_last_error().decode(), name
+        assert fn(None, *args) == -1, name  # OSTC_ERR_INPUT
+    assert not np.any(x)
+    assert lib.ostc_driver_stream(d._h) is None
+    d.close()
