@@ -152,3 +152,31 @@ def test_device_entry_points_refuse_an_uninitialised_driver(case_factory):
     assert not np.any(x)
     assert lib.ostc_driver_stream(d._h) is None
     d.close()
+
+
+def test_surrogate_entry_points_refuse_a_null_handle():
+    lib = ostc.library()
+    f = (ctypes.c_float * 16)()
+    x = np.zeros(16)
+    p = x.ctypes.data
+    gate = ostc.SurrogateGate()
+    ev = ostc.SurrogateEval()
+    dbl = ctypes.c_double()
+    calls = {
+        "ostc_surrogate_generate": (None, 16, 1, 0.5),
+        "ostc_surrogate_train": (1, 128, 1e-3, 0, None),
+        "ostc_surrogate_evaluate": (0, 1, ctypes.byref(ev)),
+        "ostc_surrogate_label": (p, 1, p),
+        "ostc_surrogate_predict": (p, 1, p, p),
+        "ostc_surrogate_gradients": (p, p, 128, f, ctypes.byref(dbl)),
+        "ostc_surrogate_get_params": (f,),
+        "ostc_surrogate_set_params": (f,),
+        "ostc_surrogate_normalisation": (f, f, f, f),
+        "ostc_surrogate_save": (b"never_written.bin",),
+        "ostc_surrogate_load": (b"never_read.bin",),
+        "ostc_surrogate_get_gate": (ctypes.byref(gate),),
+        "ostc_surrogate_set_gate": (ctypes.byref(gate),),
+    }
+    for name, args in calls.items():
+        assert getattr(lib, name)(None, *args) == -1, name  # OSTC_ERR_INPUT
+    assert lib.ostc_surrogate_param_count() > 0
