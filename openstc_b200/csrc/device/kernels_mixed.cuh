@@ -671,163 +671,6 @@ __device__ __forceinline__ void local_time_step_s(const DevBlock &B, const Src &
   B.dt_local[B.Z.at(i, j, k)] = cF.cfl / (s0 + s1 + s2 + srv);
 }
 
-template <class C>
-__device__ __forceinline__ void local_time_step_mx(const DevBlock &B, int i, int j, int k, int64_t n, int64_t nd) {
-  local_time_step_s<C>(B, fp32::Src64{B}, i, j, k, n, nd);
-}
-
-// Inviscid + viscous flux differences in FP32 (accumulated in FP32 and added
-// to the FP64 source terms), then the local time step.
-template <class C>
-__global__ void __launch_bounds__(kCta, 4) k_flux_mx(const DevBlock *__restrict__ blks, Tiles T) {
-  constexpr int NV = C::nv;
-  extern __shared__ float sfm[];
-  int b, i, j, k;
-  if (!tile_cell<kTX, kTY, kTZ>(T, b, i, j, k, blks)) return;
-  const DevBlock &B = blks[b];
-  const int tid = threadIdx.x + kTX * (threadIdx.y + kTY * threadIdx.z);
-  float *fm = sfm + tid;
-  const int64_t n = B.G.at(i, j, k), nd = B.D.at(i, j, k), szd = B.D.size;
-  const int64_t sx = B.G.sx, sxy = B.G.sxy;
-  const bool three_d = B.mz > 1;
-  float acc[NV];
-  OSTC_UNROLL for (int l = 0; l < NV; ++l) acc[l] = 0;
-  const int n_face = three_d ? 6 : 4;
-#pragma unroll 1
-  for (int f = 0; f < n_face; ++f) {
-    const int d = f >> 1;
-    const int64_t s = d == 0 ? 1 : (d == 1 ? sx : sxy);
-    float t[NV];
-    fp32::inviscid_face<C>(B, (f & 1) ? n : n - s, d, s, t);
-    if ((f & 1) == 0) {
-      OSTC_UNROLL for (int l = 0; l < NV; ++l) fm[l * kCta] = t[l];
-    } else {
-      OSTC_UNROLL for (int l = 0; l < NV; ++l) acc[l] -= t[l] - fm[l * kCta];
-    }
-  }
-  if (cP.viscous_order != 0) {
-#pragma unroll 1
-    for (int f = 0; f < n_face; ++f) {
-      const int d = f >> 1;
-      const int64_t s = d == 0 ? 1 : (d == 1 ? sx : sxy);
-      float t[NV];
-      fp32::viscous_face<C>(B, (f & 1) ? n : n - s, d, s, t);
-      if ((f & 1) == 0) {
-        OSTC_UNROLL for (int l = 0; l < NV; ++l) fm[l * kCta] = t[l];
-      } else {
-        OSTC_UNROLL for (int l = 0; l < NV; ++l) acc[l] += t[l] - fm[l * kCta];
-      }
-    }
-  }
-  OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq[l * szd + nd] += static_cast<double>(acc[l]);
-  local_time_step_mx<C>(B, i, j, k, n, nd);
-}
-
-// k_flux_mx_col (below): the same flux differences with every face evaluated
-// once, on the columns of k_flux_col (kernels_step.cuh).  Each face value is
-// the one k_flux_mx computes for it, and the per-cell sums run in the same
-// order, so the result is bit-identical.
-
-// One face type (VISC 0: inviscid, 1: viscous) of plane k of a column: every
-// face into shared memory (one inlined face evaluation, looped over the
-// thread's faces), then each cell's differences in the order x, y, z,
-// subtracted (inviscid) or added (viscous).
-template <class C, int VISC>
-__device__ __forceinline__ void col_faces(const DevBlock &B, int i0, int j0, int k, bool first, bool cell,
-                                          float *sm, float *acc) {
-  constexpr int NV = C::nv;
-  using S = ColSmem<NV>;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
-  const int i = i0 + lane, j = j0 + warp;
-  const int64_t sx = B.G.sx, sxy = B.G.sxy;
-  const bool three_d = B.mz > 1;
-  float *zs = sm + S::zs + VISC * NV * kCta;
-  const int ntask = cell ? (three_d ? (first ? 4 : 3) : 2) : (warp == kTY ? 2 : 0);
-#pragma unroll 1
-  for (int q = 0; q < ntask; ++q) {
-    int64_t nl = 0, s = 1;
-    int d = 0, off = 0, stride = kCta;
-    bool valid = true;
-    if (cell) {
-      const int64_t n = B.G.at(i, j, k);
-      const int task = (q >= 2 && !first) ? q + 1 : q;  // x, y, low z (first plane), high z
-      if (task == 0) {
-        nl = n; d = 0; s = 1; off = S::xs + warp * (kTX + 1) + lane + 1; stride = kTY * (kTX + 1);
-      } else if (task == 1) {
-        nl = n; d = 1; s = sx; off = S::ys + (warp + 1) * kTX + lane; stride = (kTY + 1) * kTX;
-      } else if (task == 2) {
-        nl = n - sxy; d = 2; s = sxy; off = static_cast<int>(zs - sm) + tid;
-      } else {
-        nl = n; d = 2; s = sxy; off = S::zp + tid;
-      }
-    } else if (q == 0) {  // low-i faces of the column's rows
-      valid = lane < kTY && j0 + lane < B.my && i0 < B.mx;
-      if (valid) nl = B.G.at(i0, j0 + lane, k) - 1;
-      d = 0; s = 1; off = S::xs + lane * (kTX + 1); stride = kTY * (kTX + 1);
-    } else {  // low-j faces of the column's i
-      valid = i < B.mx && j0 < B.my;
-      if (valid) nl = B.G.at(i, j0, k) - sx;
-      d = 1; s = sx; off = S::ys + lane; stride = (kTY + 1) * kTX;
-    }
-    if (!valid) continue;
-    float t[NV];
-    if constexpr (VISC == 0)
-      fp32::inviscid_face<C>(B, nl, d, s, t);
-    else
-      fp32::viscous_face<C>(B, nl, d, s, t);
-    OSTC_UNROLL for (int l = 0; l < NV; ++l) sm[off + l * stride] = t[l];
-  }
-  __syncthreads();
-  if (cell) {
-    const float *xs = sm + S::xs + warp * (kTX + 1) + lane, *ys = sm + S::ys + warp * kTX + lane;
-    OSTC_UNROLL for (int l = 0; l < NV; ++l) {
-      const float dx = xs[l * kTY * (kTX + 1) + 1] - xs[l * kTY * (kTX + 1)];
-      const float dy = ys[l * (kTY + 1) * kTX + kTX] - ys[l * (kTY + 1) * kTX];
-      if constexpr (VISC == 0) {
-        acc[l] -= dx;
-        acc[l] -= dy;
-      } else {
-        acc[l] += dx;
-        acc[l] += dy;
-      }
-      if (three_d) {
-        const float zp = sm[S::zp + l * kCta + tid];
-        const float dz = zp - zs[l * kCta + tid];
-        zs[l * kCta + tid] = zp;
-        if constexpr (VISC == 0)
-          acc[l] -= dz;
-        else
-          acc[l] += dz;
-      }
-    }
-  }
-  __syncthreads();
-}
-
-template <class C>
-__global__ void __launch_bounds__(kFluxThreads, 4) k_flux_mx_col(const DevBlock *__restrict__ blks, Tiles T) {
-  constexpr int NV = C::nv;
-  __shared__ float sm[ColSmem<NV>::size];
-  int b, i0, j0, k0;
-  col_tile(T, b, i0, j0, k0);
-  const DevBlock &B = blks[b];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int i = i0 + lane, j = j0 + warp;
-  const bool cell = warp < kTY && i < B.mx && j < B.my;
-  const int64_t szd = B.D.size;
-  const int k1 = min(k0 + kFluxKC, B.mz);
-  for (int k = k0; k < k1; ++k) {
-    float acc[NV];
-    OSTC_UNROLL for (int l = 0; l < NV; ++l) acc[l] = 0;
-    col_faces<C, 0>(B, i0, j0, k, k == k0, cell, sm, acc);
-    if (cP.viscous_order != 0) col_faces<C, 1>(B, i0, j0, k, k == k0, cell, sm, acc);
-    if (!cell) continue;
-    const int64_t n = B.G.at(i, j, k), nd = B.D.at(i, j, k);
-    OSTC_UNROLL for (int l = 0; l < NV; ++l) B.dq[l * szd + nd] += static_cast<double>(acc[l]);
-    local_time_step_mx<C>(B, i, j, k, n, nd);
-  }
-}
-
 // ----------------------------------------------------- direction passes
 // The flux differences as three passes, one per direction d: every face
 // along d is evaluated once, inviscid and viscous together, as
